@@ -1,0 +1,473 @@
+"""Benchmark of the flat TurboQuant FastScan search on B200.
+
+Workload (default): 1,000,000 x 1536 database, 4-bit codes, TQ+ calibrated on
+10,000 rows, 10,000 queries, k = 10 — vectors drawn (seeded) from a Gaussian
+with power-law variances lambda_i ~ i^-0.8, a Haar-random rotation and L2
+normalization (vectorcache_b200.synthetic.power_law_torch). One step = one
+search of the whole query batch against the index.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). Multi-GPU (torchrun, one rank per GPU): every
+rank holds its own 1M-vector shard (weak scaling), all ranks search the same
+queries, and the per-shard top-k lists are exchanged with one NCCL all-gather
+and merged (score desc, id asc) — the only collective of the path.
+
+--impl reference times the reference's own CPU implementation
+(oracle/_ref/libtqref.so: encode + repack + search_flat compiled in place from
+the reference sources) on this host's cores, on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "QPS at fixed Recall@10 (1Mx1536 4-bit, k=10)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=1_000_000, help="vectors per GPU shard")
+    p.add_argument("--nq", type=int, default=10_000)
+    p.add_argument("--dim", type=int, default=1536)
+    p.add_argument("--bits", type=int, default=4)
+    p.add_argument("--k", type=int, default=10)
+    p.add_argument("--calib", type=int, default=10_000)
+    p.add_argument("--recall-queries", type=int, default=1000)
+    p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def load_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the scan kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "scan_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        return json.loads(f.read_text())
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.tmp.flush()
+        rows = []
+        for line in Path(self.tmp.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def merge_shards(world, scores, ids, k):
+    """All-gather every rank's top-k and merge: score desc, equal scores by lower id."""
+    import torch
+    import torch.distributed as dist
+
+    if world == 1:
+        return scores, ids
+    gs = [torch.empty_like(scores) for _ in range(world)]
+    gi = [torch.empty_like(ids) for _ in range(world)]
+    dist.all_gather(gs, scores)
+    dist.all_gather(gi, ids)
+    s = torch.cat(gs, dim=1)
+    i = torch.cat(gi, dim=1)
+    order = torch.argsort(i, dim=1, stable=True)
+    s, i = torch.gather(s, 1, order), torch.gather(i, 1, order)
+    order = torch.argsort(s, dim=1, descending=True, stable=True)
+    return torch.gather(s, 1, order)[:, :k], torch.gather(i, 1, order)[:, :k]
+
+
+def exact_topk(db, q, k):
+    """Exact inner-product top-k on the device in fp32 (no TF32)."""
+    import torch
+
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        best_s = None
+        best_i = None
+        chunk = 262144
+        for s0 in range(0, db.shape[0], chunk):
+            sc = q @ db[s0:s0 + chunk].T
+            ts, ti = torch.topk(sc, min(k, sc.shape[1]), dim=1)
+            ti = ti + s0
+            if best_s is None:
+                best_s, best_i = ts, ti
+            else:
+                cs = torch.cat([best_s, ts], 1)
+                ci = torch.cat([best_i, ti], 1)
+                top = torch.topk(cs, k, dim=1)
+                best_s, best_i = top.values, torch.gather(ci, 1, top.indices)
+        return best_i
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def recall_at(approx_ids, exact_ids, t):
+    a = approx_ids[:, :t]
+    e = exact_ids[:, :t]
+    hits = sum(len(set(a[r].tolist()) & set(e[r].tolist())) for r in range(a.shape[0]))
+    return hits / (t * a.shape[0])
+
+
+def cpu_reference_run(db_host, q_host, calib_host, bits, k, sample_queries, steps, warmup):
+    """Times the reference's own CPU search_flat (all host cores) on the same
+    index; returns (qps_list, threads, build_seconds)."""
+    from oracle.oracle import Reference, ReferenceIndex
+
+    ref = Reference()
+    threads = ref.max_threads()
+    t0 = time.perf_counter()
+    idx = ReferenceIndex(ref, db_host, bits, calib_rows=calib_host)
+    build_s = time.perf_counter() - t0
+    qps = []
+    nq = q_host.shape[0]
+    for step in range(warmup + steps):
+        s0 = (step * sample_queries) % max(1, nq - sample_queries + 1)
+        qs = q_host[s0:s0 + sample_queries]
+        t = time.perf_counter()
+        idx.search(qs, k)
+        dt = time.perf_counter() - t
+        if step >= warmup:
+            qps.append(qs.shape[0] / dt)
+    idx.close()
+    return qps, threads, build_s
+
+
+def make_data(args, rank, device):
+    import torch
+
+    from vectorcache_b200.synthetic import power_law_torch
+
+    db = power_law_torch(args.n, args.dim, seed=1000 + rank, device=device)
+    q = power_law_torch(args.nq, args.dim, seed=7, device=device)
+    torch.cuda.synchronize()
+    return db, q
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import torch
+
+    device = torch.device("cuda", 0) if torch.cuda.is_available() else None
+    if device is not None:
+        db, q = make_data(args, 0, device)
+        db_h, q_h = db.cpu().numpy(), q.cpu().numpy()
+        del db, q
+    else:
+        from vectorcache_b200.synthetic import power_law
+
+        db_h, q_h = power_law(args.n, args.dim, 1000), power_law(args.nq, args.dim, 7)
+    calib = db_h[: args.calib]
+    qps, threads, build_s = cpu_reference_run(db_h, q_h, calib, args.bits, args.k, args.cpu_queries,
+                                              args.steps, args.warmup)
+    value = statistics.mean(qps)
+    sample = (f"{args.cpu_queries} queries per step against the full {args.n}x{args.dim} {args.bits}-bit "
+              f"TQ+ index built by the reference's encode/repack ({build_s:.1f}s); avx2_perm0 backend")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.cpu_queries / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"flat TurboQuant search {args.n}x{args.dim} {args.bits}-bit TQ+, k={args.k}",
+                   "n": args.n, "dim": args.dim, "bits": args.bits, "k": args.k, "nq": args.nq,
+                   "queries_per_step": args.cpu_queries},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import vectorcache_b200 as vcb
+
+    device = torch.device("cuda", local)
+    db, q = make_data(args, rank, device)
+    index = vcb.TurboQuantIndex(args.dim, args.bits, device=local)
+    idx_stream = torch.cuda.ExternalStream(index.stream(), device=device)
+
+    # Build: calibrate on the first rows, stage, encode (timed as encode vectors/s).
+    index.calibrate_device(db[: args.calib])
+    index.add_device(db)
+    index.set_profiling(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(idx_stream)
+    index.prepare()
+    ev1.record(idx_stream)
+    ev1.synchronize()
+    prof_build = index.read_profile()
+    encode_ms = ev0.elapsed_time(ev1)
+    encode_vps = args.n / (encode_ms / 1e3)
+
+    k = args.k
+    # An explicit stream: NULL would mean the index's own (non-blocking) stream.
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    d_scores = torch.empty((args.nq, k), dtype=torch.float32, device=device)
+    d_ids = torch.empty((args.nq, k), dtype=torch.int64, device=device)
+
+    def step():
+        index.search_device(q, k, d_scores, d_ids, stream=stream)
+        if world > 1:
+            off = torch.as_tensor(rank * args.n, device=device)
+            return merge_shards(world, d_scores, d_ids + off, k)
+        return d_scores, d_ids
+
+    # Recall@10 of the returned top-k against exact fp32 inner-product top-k.
+    nr = min(args.recall_queries, args.nq)
+    step()
+    torch.cuda.synchronize()
+    exact = exact_topk(db, q[:nr], 10)
+    recall10 = recall_at(d_ids[:nr].cpu().numpy(), exact.cpu().numpy(), min(10, k))
+    del exact
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    index.read_profile()  # reset counters
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    elapsed_ms = max_over_ranks(world, t0.elapsed_time(t1))
+    prof = index.read_profile()
+    clocks = clk.summary()
+
+    queries_scanned = args.nq * args.steps * world  # one query against one 1M-vector shard = one unit
+    value = queries_scanned / (elapsed_ms / 1e3)
+
+    # End to end through the public host-buffer API: pinned host queries in,
+    # host top-k out, copies inside the timed region.
+    q_host = q.cpu().pin_memory()
+    out_s = np.empty(args.nq * k, np.float32)
+    out_i = np.empty(args.nq * k, np.uint64)
+    import ctypes as C
+
+    lib = vcb.load_library()
+    ke = C.c_size_t(0)
+
+    def host_step():
+        rc = lib.tq_index_search(index._h, C.c_void_p(q_host.data_ptr()), args.nq, k,
+                                 out_s.ctypes.data_as(C.c_void_p), out_i.ctypes.data_as(C.c_void_p), C.byref(ke))
+        if rc != 0:
+            raise RuntimeError(lib.tq_last_error().decode())
+        if world > 1:
+            s = torch.from_numpy(out_s).view(args.nq, k).to(device)
+            i = torch.from_numpy(out_i.view(np.int64)).view(args.nq, k).to(device) + rank * args.n
+            ms, mi = merge_shards(world, s, i, k)
+            ms.cpu(), mi.cpu()
+
+    for _ in range(max(1, args.warmup)):
+        host_step()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(idx_stream)
+    for _ in range(args.steps):
+        host_step()
+    e1.record(idx_stream)
+    e1.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
+    e2e_value = args.nq * args.steps * world / (e2e_ms / 1e3)
+
+    # Roofline of the dominant kernel (scan): algorithmic bytes per launch over
+    # its mean event-timed duration.
+    peak, peak_kind = load_peaks()
+    scan_launches = max(1, prof["scan_launches"])
+    scan_ms_avg = prof["scan_ms"] / scan_launches
+    bytes_per_launch = prof["scan_stream_bytes"] / scan_launches
+    achieved = bytes_per_launch / (scan_ms_avg / 1e3) / 1e9
+    traffic = load_traffic()
+    tr = None
+    if traffic and traffic.get("n") and traffic.get("dram_bytes_per_launch"):
+        # Captured on a smaller case; DRAM traffic scales with the vectors streamed.
+        tr = traffic["dram_bytes_per_launch"] * (args.n / traffic["n"]) * (args.nq / traffic.get("nq", args.nq))
+    nbg = args.dim // (8 // args.bits)
+    lookups = 2.0 * args.nq * args.n * nbg
+    total_kernel_ms = prof["prep_ms"] + prof["scan_ms"] + prof["merge_ms"]
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            db_h = db.cpu().numpy()
+            q_h = q.cpu().numpy()
+            del db
+            torch.cuda.empty_cache()
+            qps, threads, build_s = cpu_reference_run(db_h, q_h, db_h[: args.calib], args.bits, k,
+                                                      args.cpu_queries, 2, 1)
+            cpu_base = {"value": statistics.mean(qps), "unit": "queries/s", "cores": threads, "kind": "reference",
+                        "sample": f"{args.cpu_queries} queries x 2 timed steps against the same "
+                                  f"{args.n}x{args.dim} {args.bits}-bit TQ+ data, index built by the "
+                                  f"reference's own encode/repack on the host ({build_s:.1f}s), avx2_perm0"}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu_base = {"value": None, "unit": "queries/s", "cores": os.cpu_count(), "kind": "reference",
+                        "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {
+                "workload": f"flat TurboQuant search {args.n}x{args.dim} {args.bits}-bit TQ+, k={k}, "
+                            f"{args.nq} queries per step",
+                "n_per_gpu": args.n, "dim": args.dim, "bits": args.bits, "k": k, "nq": args.nq,
+                "calibration_rows": args.calib, "recall_at_10": recall10,
+                "recall_queries": nr, "l2": "inputs larger than L2 (codes %.0f MB per shard)"
+                                           % (args.n * (nbg + 4) / 1e6),
+                "parallelism": f"shard{world}" if world > 1 else "single",
+                "encode_vectors_per_s": encode_vps, "encode_ms": encode_ms,
+                "kernel_ms_per_step": {"prep": prof["prep_ms"] / args.steps, "scan": prof["scan_ms"] / args.steps,
+                                       "merge": prof["merge_ms"] / args.steps},
+                "nibble_lookups_per_s": lookups * args.steps / (prof["scan_ms"] / 1e3) if prof["scan_ms"] else None,
+                "encode_kernel_ms": prof_build["encode_ms"],
+            },
+            "roofline": {"kernel": "scan_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": tr,
+                         "bytes_per_launch": bytes_per_launch, "ms_per_launch": scan_ms_avg,
+                         "share_of_kernel_time": prof["scan_ms"] / total_kernel_ms if total_kernel_ms else None},
+            "cpu_baseline": cpu_base,
+            "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * args.dim * 4,
+                    "d2h_bytes_per_step": args.nq * k * 12},
+            "gpu_launches": prof["prep_launches"] + prof["scan_launches"] + prof["merge_launches"],
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    index.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if world > 1 and rank != 0:
+            return
+        if not (ROOT / "oracle" / "_ref" / "libtqref.so").exists():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtqref.so was not built"}))
+            return
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

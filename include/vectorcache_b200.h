@@ -1,0 +1,163 @@
+/*
+ * vectorcache_b200 — C ABI of the B200 (sm_100a) TurboQuant flat index.
+ *
+ * Drop-in boundary for the flat TurboQuant encode + FastScan search path of
+ * nishadtardalkar/vectorcache. The reference exposes this path as C++ only:
+ * the free functions fit_calibration / encode / repack / prepare_queries /
+ * score_prepared / search_flat and the GPU class gpu::FlatIndex. Each entry
+ * point below names the reference interface it replaces (paths inside the
+ * reference project).
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a nonzero TQ_ERR_* code on
+ *     failure; tq_last_error() returns the calling thread's last message.
+ *     Nothing throws across this boundary.
+ *   - Host pointers belong to the caller. Device memory belongs to the library,
+ *     except for the *_device entry points, whose buffers the caller owns
+ *     (16-byte aligned, on the index's device).
+ *   - A handle is used by one host thread at a time. Work is queued on the
+ *     index's own CUDA stream unless a `stream` (cudaStream_t) is passed.
+ *   - Validation follows the reference: dim a positive multiple of 8 and
+ *     <= 16384, bits in {2, 3, 4}; search returns k_eff = min(k, n) results
+ *     per query, scores descending, equal scores ordered by lower id.
+ */
+#ifndef VECTORCACHE_B200_H
+#define VECTORCACHE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TQ_OK = 0,
+  TQ_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  TQ_ERR_STATE = 2,            /* std::runtime_error: wrong call order */
+  TQ_ERR_CUDA = 3,             /* CUDA runtime error */
+  TQ_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed or over the HBM budget */
+  TQ_ERR_UNSUPPORTED = 5       /* valid for the reference, not for this device path */
+};
+
+typedef struct tq_index tq_index;
+
+/* Last error message of the calling thread ("" if none). */
+const char* tq_last_error(void);
+
+/* Library version string. */
+const char* tq_version(void);
+
+/* ---- host-side tables (same values as the reference's setup code) -------- */
+
+/* Lloyd-Max codebook for Beta((dim-1)/2, (dim-1)/2).
+ * Replaces vectorcache::codebook (src/quantize/codebook.cpp:203).
+ * boundaries: 2^bits - 1 floats, centroids: 2^bits floats. */
+int tq_codebook(size_t bits, size_t dim, float* boundaries, float* centroids);
+
+/* Rotation tables: signs[dim] (+-1) and perm[dim].
+ * Replaces vectorcache::Rotation::signs/perm (src/transform/rotation.cpp:139-160). */
+int tq_rotation_tables(size_t dim, float* signs, uint32_t* perm);
+
+/* ---- index lifecycle ------------------------------------------------------- */
+
+/* Create an empty flat index on CUDA device `device`. flags: reserved, pass 0.
+ * Replaces gpu::FlatIndex::FlatIndex(dim, bits)
+ * (include/vectorcache/gpu/flat_index.hpp:19, src/gpu/flat_index.cpp:82). */
+int tq_index_create(size_t dim, size_t bits, uint32_t flags, int device, tq_index** out);
+
+int tq_index_destroy(tq_index* h);
+
+/* Optional TQ+ calibration from n >= 2 sample rows (host memory). Must precede
+ * prepare(). Replaces vectorcache::fit_calibration (src/encode/encode.cpp:327). */
+int tq_index_calibrate(tq_index* h, const float* sample, size_t n);
+int tq_index_calibrate_device(tq_index* h, const float* d_sample, size_t n, void* stream);
+
+/* Append n rows. Before prepare() rows are staged on the device and encoded by
+ * prepare(); after prepare() they are encoded and appended immediately.
+ * Replaces gpu::FlatIndex::add (src/gpu/flat_index.cpp:134) and
+ * vectorcache::encode (src/encode/encode.cpp:294). */
+int tq_index_add(tq_index* h, const float* vectors, size_t n);
+int tq_index_add_device(tq_index* h, const float* d_vectors, size_t n, void* stream);
+
+/* Encode staged rows and build the scan layout.
+ * Replaces gpu::FlatIndex::prepare (src/gpu/flat_index.cpp:147) and
+ * vectorcache::repack (src/pack/pack.cpp:366). */
+int tq_index_prepare(tq_index* h);
+
+/* Top-k search. scores/ids hold nq * k entries; rows are written with stride
+ * *k_eff = min(k, size). 1 <= k <= 256.
+ * Replaces gpu::FlatIndex::search (src/gpu/flat_index.cpp:220) and
+ * vectorcache::search_flat (src/search/search.cpp:1293). */
+int tq_index_search(tq_index* h, const float* queries, size_t nq, size_t k, float* scores,
+                    uint64_t* ids, size_t* k_eff);
+/* Same with caller-owned device buffers, queued on `stream` (NULL: the
+ * index's stream); returns without synchronizing. */
+int tq_index_search_device(tq_index* h, const float* d_queries, size_t nq, size_t k,
+                           float* d_scores, uint64_t* d_ids, size_t* k_eff, void* stream);
+
+/* Block until the index's queued work is done. */
+int tq_index_synchronize(tq_index* h);
+
+/* ---- introspection (parity exports) --------------------------------------- */
+
+int tq_index_info(const tq_index* h, size_t* dim, size_t* bits, size_t* n, int* prepared,
+                  int* calibrated);
+
+/* Row-major byte-group codes, n * (dim / (8 / bits)) bytes; first code of a
+ * byte in the high bits (codes_flat_from_packed, src/pack/pack.cpp:352). */
+int tq_index_export_codes_flat(tq_index* h, uint8_t* out);
+
+/* Bit-plane rows exactly as vectorcache::encode writes them:
+ * n * bits * dim / 8 bytes (src/encode/encode.cpp:147-153). */
+int tq_index_export_packed(tq_index* h, uint8_t* out);
+
+/* Per-vector alpha = ||v|| / <u, x_hat> (encode.cpp:32-37). */
+int tq_index_export_alpha(tq_index* h, float* out);
+
+/* TQ+ shift / scale (dim floats each); TQ_ERR_STATE if not calibrated. */
+int tq_index_export_calibration(tq_index* h, float* shift, float* scale);
+
+/* Query-side state of prepare_queries (src/search/search.cpp:762):
+ * q_rot (nq*dim), bias_corr (nq), LUT bytes (nq * nbg * 32), LUT scale and
+ * bias (nq each). Any output pointer may be NULL. */
+int tq_index_prepare_queries(tq_index* h, const float* queries, size_t nq, float* q_rot,
+                             float* bias_corr, uint8_t* luts, float* lut_scale, float* lut_bias);
+
+/* Dense scores of every (query, vector): integer LUT sums over all groups
+ * (nq * n uint32) and the float scores the scan ranks (nq * n floats).
+ * Either output may be NULL. */
+int tq_index_dense_scores(tq_index* h, const float* queries, size_t nq, uint32_t* int_scores,
+                          float* scores);
+
+/* Number of vectors whose alpha (or queries whose TQ+ bias) needed the exact
+ * sequential replay since the index was created. */
+int tq_index_replay_count(const tq_index* h, uint64_t* count);
+
+/* ---- measurement (no counterpart in the reference, which times with
+ *      std::chrono around whole calls: tools/gpu-bench.cpp:155-190) ---------- */
+
+/* The index's own CUDA stream (a cudaStream_t), for callers that time or
+ * order work around the host-buffer entry points. */
+int tq_index_get_stream(tq_index* h, void** stream);
+
+/* Per-kernel device time, recorded with CUDA events around every launch
+ * while profiling is enabled. Reading the profile synchronizes the index and
+ * resets it. scan_stream_bytes counts the bytes one streaming of the codes +
+ * alpha per query group moves: sum over scan launches of
+ * query_groups * n * (n_byte_groups + 4). */
+typedef struct tq_profile {
+  double prep_ms, scan_ms, merge_ms, encode_ms;
+  uint64_t prep_launches, scan_launches, merge_launches, encode_launches;
+  uint64_t scan_stream_bytes;
+  uint64_t scan_queries;
+} tq_profile;
+
+int tq_index_set_profiling(tq_index* h, int enabled);
+int tq_index_read_profile(tq_index* h, tq_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VECTORCACHE_B200_H */

@@ -1,0 +1,219 @@
+"""Test infrastructure only — ctypes loaders for the two CPU checkers.
+
+* `Oracle`   — oracle/_build/libtqoracle.so, the plain-C restatement of the
+               reference's flat TurboQuant arithmetic (tq_oracle.c).
+* `Reference` — oracle/_ref/libtqref.so, the reference's own CPU code compiled
+               in place by oracle/Makefile (only where the reference tree was
+               available at build time).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arms use this module, and only as the checker or the timed CPU baseline; the
+product library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libtqoracle.so"
+REF_SO = HERE / "_ref" / "libtqref.so"
+REF_TREE = Path(os.environ.get("VCB_REFERENCE_TREE", "/root/reference"))
+
+_SZ = C.c_size_t
+_P = C.c_void_p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def build(reference: bool = True) -> None:
+    """Compile the C oracle, and the reference in place when its tree exists."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if reference and REF_TREE.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_TREE}", f"-j{os.cpu_count() or 4}"],
+                       check=True)
+
+
+def nbg_of(bits: int, dim: int) -> int:
+    return dim // (8 // bits)
+
+
+class _Common:
+    prefix = ""
+
+    def __init__(self, path: Path):
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (python -c 'import oracle.oracle as o; o.build()')")
+        self.lib = C.CDLL(str(path))
+
+    def fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def codebook(self, bits, dim):
+        b = np.zeros(15, np.float32)
+        c = np.zeros(16, np.float32)
+        assert self.fn("codebook")(_SZ(bits), _SZ(dim), _p(b), _p(c)) == 0
+        L = 1 << bits
+        return b[: L - 1].copy(), c[:L].copy()
+
+    def rotation(self, dim):
+        s = np.zeros(dim, np.float32)
+        p = np.zeros(dim, np.uint32)
+        assert self.fn("rotation")(_SZ(dim), _p(s), _p(p)) == 0
+        return s, p
+
+    def fit_calibration(self, x, bits):
+        x = np.ascontiguousarray(x, np.float32)
+        n, dim = x.shape
+        sh = np.zeros(dim, np.float32)
+        sc = np.zeros(dim, np.float32)
+        assert self.fn("fit_calibration")(_p(x), _SZ(n), _SZ(dim), _SZ(bits), _p(sh), _p(sc)) == 0
+        return sh, sc
+
+    def encode(self, x, bits, shift=None, scale=None):
+        x = np.ascontiguousarray(x, np.float32)
+        n, dim = x.shape
+        packed = np.zeros((n, bits * dim // 8), np.uint8)
+        alpha = np.zeros(n, np.float32)
+        rc = self.fn("encode")(_p(x), _SZ(n), _SZ(dim), _SZ(bits), _p(shift), _p(scale), _p(packed), _p(alpha))
+        assert rc == 0
+        return packed, alpha
+
+    def codes_flat(self, packed, bits, dim):
+        packed = np.ascontiguousarray(packed, np.uint8)
+        n = packed.shape[0]
+        out = np.zeros((n, nbg_of(bits, dim)), np.uint8)
+        assert self.fn("codes_flat")(_p(packed), _SZ(n), _SZ(bits), _SZ(dim), _p(out)) == 0
+        return out
+
+    def prepare_queries(self, q, bits, shift=None, scale=None):
+        q = np.ascontiguousarray(q, np.float32)
+        nq, dim = q.shape
+        nbg = nbg_of(bits, dim)
+        out = {
+            "q_rot": np.zeros((nq, dim), np.float32),
+            "bias_corr": np.zeros(nq, np.float32),
+            "luts": np.zeros((nq, nbg * 32), np.uint8),
+            "lut_scale": np.zeros(nq, np.float32),
+            "lut_bias": np.zeros(nq, np.float32),
+        }
+        rc = self.fn("prepare_queries")(_p(q), _SZ(nq), _SZ(dim), _SZ(bits), _p(shift), _p(scale),
+                                       _p(out["q_rot"]), _p(out["bias_corr"]), _p(out["luts"]),
+                                       _p(out["lut_scale"]), _p(out["lut_bias"]))
+        assert rc == 0
+        return out
+
+
+class Oracle(_Common):
+    prefix = "tqo_"
+
+    def __init__(self, path: Path = ORACLE_SO):
+        super().__init__(path)
+        self.lib.tqo_beta_cdf_aa.restype = C.c_double
+        self.lib.tqo_beta_cdf_aa.argtypes = [C.c_double, C.c_double]
+        self.lib.tqo_topk.restype = _SZ
+        self.lib.tqo_search_flat.restype = _SZ
+
+    def beta_cdf_aa(self, a, t):
+        return self.lib.tqo_beta_cdf_aa(a, t)
+
+    def int_scores(self, luts, codes_flat):
+        luts = np.ascontiguousarray(luts, np.uint8)
+        codes_flat = np.ascontiguousarray(codes_flat, np.uint8)
+        nq, n, nbg = luts.shape[0], codes_flat.shape[0], codes_flat.shape[1]
+        out = np.zeros((nq, n), np.uint32)
+        self.lib.tqo_int_scores(_p(luts), _SZ(nq), _p(codes_flat), _SZ(n), _SZ(nbg), _p(out))
+        return out
+
+    def float_scores(self, prep, codes_flat, alpha):
+        codes_flat = np.ascontiguousarray(codes_flat, np.uint8)
+        alpha = np.ascontiguousarray(alpha, np.float32)
+        nq, n, nbg = prep["luts"].shape[0], codes_flat.shape[0], codes_flat.shape[1]
+        out = np.zeros((nq, n), np.float32)
+        self.lib.tqo_float_scores(_p(prep["luts"]), _p(prep["lut_scale"]), _p(prep["lut_bias"]),
+                                  _p(prep["bias_corr"]), _SZ(nq), _p(codes_flat), _p(alpha), _SZ(n),
+                                  _SZ(nbg), _p(out))
+        return out
+
+    def topk(self, scores, k):
+        scores = np.ascontiguousarray(scores, np.float32)
+        nq, n = scores.shape
+        s = np.zeros(max(nq * k, 1), np.float32)
+        i = np.zeros(max(nq * k, 1), np.uint64)
+        ke = self.lib.tqo_topk(_p(scores), _SZ(nq), _SZ(n), _SZ(k), _p(s), _p(i))
+        return s[: nq * ke].reshape(nq, ke), i[: nq * ke].reshape(nq, ke)
+
+    def search_flat(self, q, bits, packed, alpha, k, shift=None, scale=None):
+        q = np.ascontiguousarray(q, np.float32)
+        nq, dim = q.shape
+        n = packed.shape[0]
+        s = np.zeros(max(nq * k, 1), np.float32)
+        i = np.zeros(max(nq * k, 1), np.uint64)
+        ke = self.lib.tqo_search_flat(_p(q), _SZ(nq), _SZ(dim), _SZ(bits), _p(shift), _p(scale),
+                                      _p(np.ascontiguousarray(packed)), _p(np.ascontiguousarray(alpha)),
+                                      _SZ(n), _SZ(k), _p(s), _p(i))
+        return s[: nq * ke].reshape(nq, ke), i[: nq * ke].reshape(nq, ke)
+
+
+class Reference(_Common):
+    prefix = "tqref_"
+
+    def __init__(self, path: Path = REF_SO):
+        super().__init__(path)
+        self.lib.tqref_last_error.restype = C.c_char_p
+        self.lib.tqref_beta_cdf_aa.restype = C.c_double
+        self.lib.tqref_beta_cdf_aa.argtypes = [C.c_double, C.c_double]
+
+    def beta_cdf_aa(self, a, t):
+        return self.lib.tqref_beta_cdf_aa(a, t)
+
+    def max_threads(self) -> int:
+        return int(self.lib.tqref_max_threads())
+
+    def set_threads(self, n: int) -> None:
+        self.lib.tqref_set_threads(C.c_int(n))
+
+
+class ReferenceIndex:
+    """The reference's flat CPU path (fit_calibration + encode + repack at
+    creation, search_flat per query batch) under the pinned AVX2 backend."""
+
+    def __init__(self, ref: Reference, x, bits, calib_rows=None, native_backend=False):
+        self.ref = ref
+        x = np.ascontiguousarray(x, np.float32)
+        self.n, self.dim = x.shape
+        self.bits = bits
+        h = _P()
+        cal = None if calib_rows is None else np.ascontiguousarray(calib_rows, np.float32)
+        rc = ref.lib.tqref_index_create(_p(x), _SZ(self.n), _SZ(self.dim), _SZ(bits), _p(cal),
+                                        _SZ(0 if cal is None else cal.shape[0]), C.c_int(int(native_backend)),
+                                        C.byref(h))
+        if rc != 0:
+            raise RuntimeError(ref.lib.tqref_last_error().decode())
+        self.h = h
+
+    def search(self, q, k):
+        q = np.ascontiguousarray(q, np.float32)
+        nq = q.shape[0]
+        s = np.zeros(max(nq * k, 1), np.float32)
+        i = np.zeros(max(nq * k, 1), np.uint64)
+        ke = _SZ(0)
+        rc = self.ref.lib.tqref_index_search(self.h, _p(q), _SZ(nq), _SZ(k), _p(s), _p(i), C.byref(ke))
+        if rc != 0:
+            raise RuntimeError(self.ref.lib.tqref_last_error().decode())
+        kk = ke.value
+        return s[: nq * kk].reshape(nq, kk), i[: nq * kk].reshape(nq, kk)
+
+    def close(self):
+        if self.h:
+            self.ref.lib.tqref_index_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

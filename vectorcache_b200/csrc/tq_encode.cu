@@ -1,0 +1,406 @@
+// Encode path on sm_100a: norm -> rotation -> (TQ+) -> Lloyd-Max code ->
+// alpha -> row-major codes, then the relayout into the scan layout.
+//
+// Follows the reference's encode (src/encode/encode.cpp:112-231, :294-307) and
+// pack (src/pack/pack.cpp:70-131) arithmetic bit for bit; see tq_device.cuh for
+// the rounding contract.
+#include "tq_kernels.h"
+#include "tq_device.cuh"
+
+namespace vcb {
+namespace {
+
+// Encodes four rows per warp iteration (the norm phase uses all 32 lanes as
+// 4 rows x 8 chains); the rotation/quantize phase then walks the four rows
+// with the whole warp. Shared memory: perm|sign table, TQ+ tables, one staged
+// input row per warp.
+template <int R>
+__global__ void __launch_bounds__(256) encode_rows_kernel(EncodeArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int dim = a.dim;
+  uint32_t* s_perm = reinterpret_cast<uint32_t*>(smem);
+  float* s_shift = reinterpret_cast<float*>(s_perm + dim);
+  float* s_scale = s_shift + (a.tqplus ? dim : 0);
+  float* s_inv_scale = s_scale + (a.tqplus ? dim : 0);
+  float* s_bnd = s_inv_scale + (a.tqplus ? dim : 0);
+  float* s_cen = s_bnd + 16;
+  float* s_rows = s_cen + 16;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* xrow = s_rows + static_cast<size_t>(warp) * dim;
+
+  for (int i = threadIdx.x; i < dim; i += blockDim.x) {
+    s_perm[i] = a.perm_sign[i];
+    if (a.tqplus) {
+      s_shift[i] = a.shift[i];
+      s_scale[i] = a.scale[i];
+      s_inv_scale[i] = a.inv_scale[i];
+    }
+  }
+  if (threadIdx.x < 16) {
+    s_bnd[threadIdx.x] = threadIdx.x < 15 ? a.boundaries[threadIdx.x] : 0.f;
+    s_cen[threadIdx.x] = a.centroids[threadIdx.x];
+  }
+  __syncthreads();
+
+  const int cpb = 8 / a.bits;                 // codes per byte group
+  const int field = (a.bits == 3) ? 4 : a.bits;  // bits per code inside the byte
+  const int lanes_per_word = 4 * cpb;         // lanes whose codes fill one u32 of codes_flat
+  const int nc = (dim + 3) / 4;               // terms per inner-product chain
+
+  const long long warps_total = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+  for (long long quad = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + warp;
+       quad * 4 < a.n; quad += warps_total) {
+    const long long v_lane = quad * 4 + (lane >> 3);
+    const bool lane_valid = v_lane < a.n;
+    const float nrm_lane =
+        warp_norm4(a.x + (lane_valid ? v_lane : 0) * static_cast<long long>(dim), dim, lane_valid, lane);
+
+    for (int j = 0; j < 4; ++j) {
+      const long long v = quad * 4 + j;
+      const float nrm = __shfl_sync(full_mask(), nrm_lane, 8 * j);
+      if (v >= a.n) break;
+      const float* src = a.x + v * static_cast<long long>(dim);
+      __syncwarp();
+      for (int i = lane * 4; i < dim; i += kWarp * 4) {
+        *reinterpret_cast<float4*>(xrow + i) = __ldg(reinterpret_cast<const float4*>(src + i));
+      }
+      __syncwarp();
+      const float inv = (nrm > kMinInputNorm) ? __fdiv_rn(1.f, nrm) : 0.f;
+      float y[R];
+      warp_rotate<R>(xrow, s_perm, dim, a.block, inv, a.inv_sqrt_block, y, lane);
+
+      // Quantize, inner-product estimate, codes_flat words.
+      double est = 0.0, mag = 0.0;
+      uint8_t* flat_row = a.out_flat + v * static_cast<long long>(a.flat_stride);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + kWarp * r;
+        unsigned code = 0;
+        if (i < dim) {
+          double term;
+          if (a.tqplus) {
+            const float c = __fmul_rn(__fadd_rn(y[r], s_shift[i]), s_scale[i]);
+            code = quantize_code(c, s_bnd, a.bits);
+            const double back = __dsub_rn(
+                __dmul_rn(static_cast<double>(s_cen[code]), static_cast<double>(s_inv_scale[i])),
+                static_cast<double>(s_shift[i]));
+            term = __dmul_rn(static_cast<double>(y[r]), back);
+          } else {
+            code = quantize_code(y[r], s_bnd, a.bits);
+            term = __dmul_rn(static_cast<double>(y[r]), static_cast<double>(s_cen[code]));
+          }
+          est = __dadd_rn(est, term);
+          mag = __dadd_rn(mag, fabs(term));
+        }
+        // Row-major byte groups: codes_per_byte codes per byte, first code in
+        // the high bits (pack.cpp:70-131). OR-reduce over the lanes of a word.
+        const int e = lane % lanes_per_word;
+        uint32_t word = code << (8 * (e / cpb) + field * (cpb - 1 - e % cpb));
+        for (int o = 1; o < lanes_per_word; o <<= 1) word |= __shfl_xor_sync(full_mask(), word, o);
+        const int byte_off = (kWarp * r) / cpb + 4 * (lane / lanes_per_word);
+        if (e == 0 && kWarp * r + lane < dim) {
+          *reinterpret_cast<uint32_t*>(flat_row + byte_off) = word;
+        }
+      }
+      est = warp_sum_d(est);
+      mag = warp_sum_d(mag);
+
+      float alpha = 0.f;
+      bool above = false;
+      float inner_f = 0.f;
+      if (decide_float_of_sum(est, mag, nc + 2 + R + 6, kDegenerateInner, &above, &inner_f)) {
+        alpha = above ? __fdiv_rn(nrm, inner_f) : 0.f;
+      } else {
+        // Exact replay of the reference's four sequential double chains
+        // (chain i % 4, one fused multiply-add per term; encode.cpp:117-156).
+        // The staged input row is no longer needed: park y there.
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = lane + kWarp * r;
+          if (i < dim) xrow[i] = y[r];
+        }
+        __syncwarp();
+        double ch = 0.0;
+        if (lane < 4) {
+#pragma unroll 1
+          for (int i = lane; i < dim; i += 4) {
+            const float yv = xrow[i];
+            if (a.tqplus) {
+              const float c = __fmul_rn(__fadd_rn(yv, s_shift[i]), s_scale[i]);
+              const unsigned code = quantize_code(c, s_bnd, a.bits);
+              const double back = __dsub_rn(__dmul_rn(static_cast<double>(s_cen[code]),
+                                                      static_cast<double>(s_inv_scale[i])),
+                                            static_cast<double>(s_shift[i]));
+              ch = __fma_rn(static_cast<double>(yv), back, ch);
+            } else {
+              const unsigned code = quantize_code(yv, s_bnd, a.bits);
+              ch = __fma_rn(static_cast<double>(yv), static_cast<double>(s_cen[code]), ch);
+            }
+          }
+        }
+        const double c0 = __shfl_sync(full_mask(), ch, 0), c1 = __shfl_sync(full_mask(), ch, 1);
+        const double c2 = __shfl_sync(full_mask(), ch, 2), c3 = __shfl_sync(full_mask(), ch, 3);
+        const double inner = __dadd_rn(__dadd_rn(c0, c1), __dadd_rn(c2, c3));
+        alpha = inner > kDegenerateInner ? __fdiv_rn(nrm, __double2float_rn(inner)) : 0.f;
+        if (lane == 0 && a.replay_count) atomicAdd(a.replay_count, 1ull);
+      }
+      if (lane == 0) a.out_alpha[v] = alpha;
+    }
+  }
+}
+
+// codes_flat rows (stride flat_stride) -> scan layout words. One CTA converts
+// 128 consecutive vectors x 32 byte groups through shared memory so both the
+// reads and the word writes are coalesced. Vectors below `keep_below` belong to
+// an earlier add() and keep their existing nibbles.
+__global__ void __launch_bounds__(256) relayout_kernel(RelayoutArgs a) {
+  __shared__ uint32_t tile[128][9];  // 128 vectors x 32 bytes (+1 word pad)
+  const long long v0 = a.first_vector + static_cast<long long>(blockIdx.x) * 128;
+  const int g0 = blockIdx.y * 32;
+  for (int t = threadIdx.x; t < 128 * 8; t += blockDim.x) {
+    const int vr = t >> 3, wcol = t & 7;
+    const long long v = v0 + vr;
+    uint32_t w = 0;
+    if (v >= a.src_first && v < a.src_first + a.src_n) {
+      w = *reinterpret_cast<const uint32_t*>(a.flat + (v - a.src_first) * a.flat_stride + g0 + 4 * wcol);
+    }
+    tile[vr][wcol] = w;
+  }
+  __syncthreads();
+  const int q = threadIdx.x & 31;  // quad inside the 128-vector strip
+  const int cpb = 8 / a.bits;
+  for (int gi = threadIdx.x >> 5; gi < 32; gi += blockDim.x >> 5) {
+    const int g = g0 + gi;
+    if (g >= a.nbg) break;
+    uint32_t word = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t byte = (tile[4 * q + j][gi >> 2] >> (8 * (gi & 3))) & 0xffu;
+      word |= (byte & 0xfu) << (4 * j);          // second half of the group's codes
+      word |= (byte >> 4) << (16 + 4 * j);       // first half
+    }
+    const long long vq = v0 + 4 * q;  // first vector of this quad
+    if (vq >= a.n_total) continue;
+    const long long tile_idx = vq / kTileVectors;
+    const int wq = static_cast<int>((vq % kTileVectors) / 4);
+    uint32_t* dst = a.codes + (tile_idx * a.nbg + g) * kTileWords + wq;
+    if (vq < a.keep_below) {
+      // Merge with the nibbles of vectors that were encoded by an earlier add().
+      uint32_t keep = 0;
+      for (int j = 0; j < 4; ++j) {
+        if (vq + j < a.keep_below) keep |= (0xfu << (4 * j)) | (0xfu << (16 + 4 * j));
+      }
+      word = (*dst & keep) | (word & ~keep);
+    }
+    *dst = word;
+    (void)cpb;
+  }
+}
+
+// Scan layout -> codes_flat rows (introspection and parity export).
+__global__ void export_flat_kernel(const uint32_t* __restrict__ codes, long long n, int nbg,
+                                   uint8_t* __restrict__ out) {
+  const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= n * nbg) return;
+  const long long v = idx / nbg;
+  const int g = static_cast<int>(idx % nbg);
+  const long long tile = v / kTileVectors;
+  const int wq = static_cast<int>((v % kTileVectors) / 4), j = static_cast<int>(v & 3);
+  const uint32_t w = codes[(tile * nbg + g) * kTileWords + wq];
+  const uint32_t lo = (w >> (4 * j)) & 0xfu, hi = (w >> (16 + 4 * j)) & 0xfu;
+  out[idx] = static_cast<uint8_t>((hi << 4) | lo);
+}
+
+// Rotated (and normalized) rows, transposed to dim x n, for the TQ+ fit.
+template <int R>
+__global__ void __launch_bounds__(256) rotate_rows_t_kernel(RotateArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int dim = a.dim;
+  uint32_t* s_perm = reinterpret_cast<uint32_t*>(smem);
+  float* s_rows = reinterpret_cast<float*>(s_perm + dim);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* xrow = s_rows + static_cast<size_t>(warp) * dim;
+  for (int i = threadIdx.x; i < dim; i += blockDim.x) s_perm[i] = a.perm_sign[i];
+  __syncthreads();
+  const long long warps_total = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+  for (long long quad = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + warp;
+       quad * 4 < a.n; quad += warps_total) {
+    const long long v_lane = quad * 4 + (lane >> 3);
+    const bool lane_valid = v_lane < a.n;
+    const float nrm_lane =
+        warp_norm4(a.x + (lane_valid ? v_lane : 0) * static_cast<long long>(dim), dim, lane_valid, lane);
+    for (int j = 0; j < 4; ++j) {
+      const long long v = quad * 4 + j;
+      const float nrm = __shfl_sync(full_mask(), nrm_lane, 8 * j);
+      if (v >= a.n) break;
+      const float* src = a.x + v * static_cast<long long>(dim);
+      __syncwarp();
+      for (int i = lane * 4; i < dim; i += kWarp * 4) {
+        *reinterpret_cast<float4*>(xrow + i) = __ldg(reinterpret_cast<const float4*>(src + i));
+      }
+      __syncwarp();
+      const float inv = (nrm > kMinInputNorm) ? __fdiv_rn(1.f, nrm) : 0.f;
+      float y[R];
+      warp_rotate<R>(xrow, s_perm, dim, a.block, inv, a.inv_sqrt_block, y, lane);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + kWarp * r;
+        if (i < dim) a.out_t[static_cast<long long>(i) * a.n + v] = y[r];
+      }
+    }
+  }
+}
+
+// Per-dimension order statistics of the rotated sample (radix select on the
+// f32 total-order key, encode.cpp:60-69, :262-276). One CTA per dimension
+// selects the lo-th and hi-th smallest keys.
+__device__ __forceinline__ uint32_t f32_order_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float f32_from_order_key(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void __launch_bounds__(256) order_stats_kernel(const float* __restrict__ yt, long long n,
+                                                          long long lo_rank, long long hi_rank,
+                                                          float* __restrict__ q_lo,
+                                                          float* __restrict__ q_hi) {
+  __shared__ unsigned int hist[2][256];
+  __shared__ uint32_t prefix[2];
+  __shared__ long long rank[2];
+  const float* col = yt + static_cast<long long>(blockIdx.x) * n;
+  if (threadIdx.x < 2) {
+    prefix[threadIdx.x] = 0;
+    rank[threadIdx.x] = threadIdx.x == 0 ? lo_rank : hi_rank;
+  }
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int b = threadIdx.x; b < 512; b += blockDim.x) hist[b >> 8][b & 255] = 0;
+    __syncthreads();
+    const uint32_t hmask = (shift == 24) ? 0u : (0xffffffffu << (shift + 8));
+    const uint32_t p0 = prefix[0], p1 = prefix[1];
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t k = f32_order_key(col[i]);
+      const uint32_t d = (k >> shift) & 255u;
+      if ((k & hmask) == (p0 & hmask)) atomicAdd(&hist[0][d], 1u);
+      if ((k & hmask) == (p1 & hmask)) atomicAdd(&hist[1][d], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int s = threadIdx.x;
+      long long r = rank[s];
+      uint32_t d = 0;
+      for (; d < 256; ++d) {
+        if (r < static_cast<long long>(hist[s][d])) break;
+        r -= hist[s][d];
+      }
+      rank[s] = r;
+      prefix[s] |= d << shift;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    q_lo[blockIdx.x] = f32_from_order_key(prefix[0]);
+    q_hi[blockIdx.x] = f32_from_order_key(prefix[1]);
+  }
+}
+
+int rows_template(int dim) {
+  const int need = (dim + kWarp - 1) / kWarp;
+  const int options[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
+  for (int r : options) {
+    if (r >= need) return r;
+  }
+  return -1;
+}
+
+int grid_for_quads(long long n, int sms) {
+  const long long quads = (n + 3) / 4;
+  long long ctas = (quads + 7) / 8;
+  const long long cap = static_cast<long long>(sms) * 8;
+  if (ctas > cap) ctas = cap;
+  return static_cast<int>(ctas < 1 ? 1 : ctas);
+}
+
+}  // namespace
+
+size_t encode_smem_bytes(int dim, bool tqplus) {
+  return static_cast<size_t>(dim) * 4 * (tqplus ? 4 : 1) + 32 * 4 + static_cast<size_t>(8) * dim * 4;
+}
+
+bool encode_dim_supported(int dim) { return rows_template(dim) > 0; }
+
+#define VCB_ROWS_CASES(X) X(1) X(2) X(3) X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64)
+
+cudaError_t launch_encode(const EncodeArgs& a, int sms, cudaStream_t stream) {
+  if (a.n == 0) return cudaSuccess;
+  const int r = rows_template(a.dim);
+  const size_t smem = encode_smem_bytes(a.dim, a.tqplus);
+  const int grid = grid_for_quads(a.n, sms);
+  switch (r) {
+#define VCB_CASE(RR)                                                                          \
+  case RR: {                                                                                  \
+    cudaError_t e = cudaFuncSetAttribute(encode_rows_kernel<RR>,                              \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                         static_cast<int>(smem));                             \
+    if (e != cudaSuccess) return e;                                                           \
+    encode_rows_kernel<RR><<<grid, 256, smem, stream>>>(a);                                   \
+    return cudaGetLastError();                                                                \
+  }
+    VCB_ROWS_CASES(VCB_CASE)
+#undef VCB_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_relayout(const RelayoutArgs& a, cudaStream_t stream) {
+  const long long first = (a.keep_below / 128) * 128;
+  const long long strips = (a.n_total - first + 127) / 128;
+  if (strips <= 0) return cudaSuccess;
+  RelayoutArgs b = a;
+  b.first_vector = first;
+  dim3 grid(static_cast<unsigned>(strips), static_cast<unsigned>((a.nbg + 31) / 32));
+  relayout_kernel<<<grid, 256, 0, stream>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_flat(const uint32_t* codes, long long n, int nbg, uint8_t* out,
+                               cudaStream_t stream) {
+  const long long total = n * nbg;
+  if (total == 0) return cudaSuccess;
+  export_flat_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(codes, n, nbg, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotate_rows_t(const RotateArgs& a, int sms, cudaStream_t stream) {
+  if (a.n == 0) return cudaSuccess;
+  const int r = rows_template(a.dim);
+  const size_t smem = static_cast<size_t>(a.dim) * 4 + static_cast<size_t>(8) * a.dim * 4;
+  const int grid = grid_for_quads(a.n, sms);
+  switch (r) {
+#define VCB_CASE(RR)                                                                          \
+  case RR: {                                                                                  \
+    cudaError_t e = cudaFuncSetAttribute(rotate_rows_t_kernel<RR>,                            \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                         static_cast<int>(smem));                             \
+    if (e != cudaSuccess) return e;                                                           \
+    rotate_rows_t_kernel<RR><<<grid, 256, smem, stream>>>(a);                                 \
+    return cudaGetLastError();                                                                \
+  }
+    VCB_ROWS_CASES(VCB_CASE)
+#undef VCB_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_order_stats(const float* yt, long long n, int dim, long long lo_rank,
+                               long long hi_rank, float* q_lo, float* q_hi, cudaStream_t stream) {
+  order_stats_kernel<<<dim, 256, 0, stream>>>(yt, n, lo_rank, hi_rank, q_lo, q_hi);
+  return cudaGetLastError();
+}
+
+}  // namespace vcb

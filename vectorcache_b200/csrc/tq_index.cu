@@ -1,0 +1,802 @@
+// Host side of the flat TurboQuant index and its C ABI (include/vectorcache_b200.h).
+//
+// The index owns its device memory and one CUDA stream. Lifecycle mirrors the
+// reference's gpu::FlatIndex (src/gpu/flat_index.cpp:82-242) and the flat free
+// functions (encode.cpp, pack.cpp, search.cpp): calibrate (optional TQ+) ->
+// add -> prepare -> search.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/vectorcache_b200.h"
+#include "tq_host_math.h"
+#include "tq_kernels.h"
+
+namespace vcb {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  const int code = (e == cudaErrorMemoryAllocation) ? TQ_ERR_OUT_OF_MEMORY : TQ_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return TQ_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return TQ_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return TQ_ERR_INVALID_ARGUMENT;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return TQ_ERR_CUDA;
+  }
+}
+
+// Grow-only device allocation.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+
+  void* reserve(size_t bytes) {
+    if (bytes <= bytes_ && ptr_) return ptr_;
+    release();
+    if (bytes == 0) bytes = 16;
+    check(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    bytes_ = bytes;
+    return ptr_;
+  }
+  void release() {
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  void swap(DeviceBuffer& o) noexcept {
+    std::swap(ptr_, o.ptr_);
+    std::swap(bytes_, o.bytes_);
+  }
+  void* get() const { return ptr_; }
+  size_t bytes() const { return bytes_; }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr_);
+  }
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    check(cudaGetDevice(&prev_), "cudaGetDevice");
+    if (prev_ != device) check(cudaSetDevice(device), "cudaSetDevice");
+    restore_ = prev_ != device;
+  }
+  ~DeviceGuard() {
+    if (restore_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0;
+  bool restore_ = false;
+};
+
+size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+}  // namespace vcb
+
+struct tq_index {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  size_t dim = 0, bits = 0, nbg = 0, block = 0;
+  float inv_sqrt_block = 0.f;
+  vcb::Codebook cb;
+  bool calibrated = false;
+  std::vector<float> shift, scale;
+  bool prepared = false;
+  size_t n = 0;          // encoded vectors
+  size_t staged_n = 0;   // rows waiting for prepare()
+  size_t cap = 0;        // layout capacity in vectors (multiple of kScanBlockVectors)
+
+  vcb::DeviceBuffer d_perm_sign, d_bnd, d_cen, d_shift, d_scale, d_inv_scale;
+  vcb::DeviceBuffer d_codes, d_alpha, d_staged, d_flat, d_counter;
+  // search scratch
+  vcb::DeviceBuffer d_queries, d_luts, d_qf, d_cand_s, d_cand_i, d_out_s, d_out_i, d_qrot;
+
+  // Optional per-launch timing (tq_index_set_profiling).
+  enum Kind { kPrep = 0, kScan = 1, kMerge = 2, kEncode = 3 };
+  struct Timed {
+    int kind;
+    cudaEvent_t start, stop;
+  };
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<Timed> timed_launches;
+  uint64_t launches[4] = {0, 0, 0, 0};
+  uint64_t scan_stream_bytes = 0, scan_queries = 0;
+
+  ~tq_index() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    for (auto& t : timed_launches) {
+      cudaEventDestroy(t.start);
+      cudaEventDestroy(t.stop);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
+  }
+
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    vcb::check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+  }
+
+  // Runs one kernel launch, bracketed by events when profiling is on.
+  template <typename F>
+  void launch(int kind, cudaStream_t s, const char* what, F&& fn) {
+    ++launches[kind];
+    if (!profiling) {
+      vcb::check(fn(), what);
+      return;
+    }
+    Timed t{kind, take_event(), take_event()};
+    vcb::check(cudaEventRecord(t.start, s), "cudaEventRecord");
+    vcb::check(fn(), what);
+    vcb::check(cudaEventRecord(t.stop, s), "cudaEventRecord");
+    timed_launches.push_back(t);
+  }
+
+  void sync() { vcb::check(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+
+  cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
+
+  size_t flat_stride() const { return vcb::round_up(nbg, 32); }
+
+  void upload(void* dst, const void* src, size_t bytes) {
+    vcb::check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+  }
+
+  // Grow the scan layout and alpha buffers to hold `want` vectors.
+  void ensure_capacity(size_t want) {
+    if (want <= cap) return;
+    size_t new_cap = std::max(want, cap + cap / 2);
+    new_cap = vcb::round_up(new_cap, vcb::kScanBlockVectors);
+    const size_t code_bytes = (new_cap / vcb::kTileVectors) * nbg * vcb::kTileWords * 4;
+    vcb::DeviceBuffer codes, alpha;
+    codes.reserve(code_bytes);
+    alpha.reserve(new_cap * 4);
+    vcb::check(cudaMemsetAsync(codes.get(), 0, code_bytes, stream), "cudaMemsetAsync");
+    vcb::check(cudaMemsetAsync(alpha.get(), 0, new_cap * 4, stream), "cudaMemsetAsync");
+    if (cap > 0) {
+      // Tiles are self-contained, so the old layout is a prefix of the new one.
+      const size_t old_code_bytes = (cap / vcb::kTileVectors) * nbg * vcb::kTileWords * 4;
+      vcb::check(cudaMemcpyAsync(codes.get(), d_codes.get(), old_code_bytes, cudaMemcpyDeviceToDevice, stream),
+                 "cudaMemcpyAsync D2D");
+      vcb::check(cudaMemcpyAsync(alpha.get(), d_alpha.get(), cap * 4, cudaMemcpyDeviceToDevice, stream),
+                 "cudaMemcpyAsync D2D");
+    }
+    sync();
+    codes.swap(d_codes);
+    alpha.swap(d_alpha);
+    cap = new_cap;
+  }
+
+  // Encode `count` rows at device pointer x and append them after the current n.
+  void encode_append(const float* x, size_t count, cudaStream_t s) {
+    if (count == 0) return;
+    ensure_capacity(n + count);
+    const size_t stride = flat_stride();
+    const size_t chunk = std::max<size_t>(1, std::min<size_t>(count, (size_t{512} << 20) / stride));
+    d_flat.reserve(chunk * stride);
+    for (size_t done = 0; done < count; done += chunk) {
+      const size_t m = std::min(chunk, count - done);
+      vcb::EncodeArgs a{};
+      a.x = x + done * dim;
+      a.n = static_cast<long long>(m);
+      a.dim = static_cast<int>(dim);
+      a.bits = static_cast<int>(bits);
+      a.block = static_cast<int>(block);
+      a.inv_sqrt_block = inv_sqrt_block;
+      a.perm_sign = d_perm_sign.as<uint32_t>();
+      a.boundaries = d_bnd.as<float>();
+      a.centroids = d_cen.as<float>();
+      a.tqplus = calibrated;
+      a.shift = d_shift.as<float>();
+      a.scale = d_scale.as<float>();
+      a.inv_scale = d_inv_scale.as<float>();
+      a.out_flat = d_flat.as<uint8_t>();
+      a.flat_stride = static_cast<int>(stride);
+      a.out_alpha = d_alpha.as<float>() + n + done;
+      a.replay_count = d_counter.as<unsigned long long>();
+      launch(kEncode, s, "encode kernel", [&] { return vcb::launch_encode(a, sms, s); });
+      vcb::RelayoutArgs r{};
+      r.flat = d_flat.as<uint8_t>();
+      r.src_first = static_cast<long long>(n + done);
+      r.src_n = static_cast<long long>(m);
+      r.flat_stride = static_cast<int>(stride);
+      r.keep_below = static_cast<long long>(n + done);
+      r.n_total = static_cast<long long>(n + done + m);
+      r.nbg = static_cast<int>(nbg);
+      r.bits = static_cast<int>(bits);
+      r.codes = d_codes.as<uint32_t>();
+      launch(kEncode, s, "relayout kernel", [&] { return vcb::launch_relayout(r, s); });
+    }
+    n += count;
+  }
+
+  // LUTs and per-query constants for nq device rows.
+  void prep_queries(const float* d_q, size_t nq, cudaStream_t s, float* q_rot_out) {
+    d_luts.reserve(nq * nbg * 32);
+    d_qf.reserve(nq * 4 * sizeof(float));
+    float* qf = d_qf.as<float>();
+    vcb::QueryPrepArgs a{};
+    a.q = d_q;
+    a.nq = static_cast<long long>(nq);
+    a.dim = static_cast<int>(dim);
+    a.bits = static_cast<int>(bits);
+    a.block = static_cast<int>(block);
+    a.nbg = static_cast<int>(nbg);
+    a.inv_sqrt_block = inv_sqrt_block;
+    a.perm_sign = d_perm_sign.as<uint32_t>();
+    a.centroids = d_cen.as<float>();
+    a.tqplus = calibrated;
+    a.shift = d_shift.as<float>();
+    a.scale = d_scale.as<float>();
+    a.luts = d_luts.as<uint8_t>();
+    a.lut_scale = qf;
+    a.lut_bias = qf + nq;
+    a.bias_corr = qf + 2 * nq;
+    a.fa_init = qf + 3 * nq;
+    a.q_rot = q_rot_out;
+    a.replay_count = d_counter.as<unsigned long long>();
+    launch(kPrep, s, "query prep kernel", [&] { return vcb::launch_query_prep(a, sms, s); });
+  }
+
+  // Full device search of nq rows at d_q into d_scores/d_ids (stride k_eff).
+  void search_device(const float* d_q, size_t nq, size_t k, float* d_scores, uint64_t* d_ids,
+                     size_t k_eff, cudaStream_t s) {
+    if (nq == 0 || k_eff == 0) return;
+    // Bound the scratch per pass: LUTs + candidate lists.
+    const size_t max_pass = 1 << 16;
+    for (size_t q0 = 0; q0 < nq; q0 += max_pass) {
+      const size_t m = std::min(max_pass, nq - q0);
+      prep_queries(d_q + q0 * dim, m, s, nullptr);
+      vcb::ScanPlan plan;
+      if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
+                          static_cast<int>(k_eff), sms, &plan)) {
+        vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
+      }
+      const size_t lists = static_cast<size_t>(plan.n_ranges) * 8;
+      d_cand_s.reserve(m * lists * k_eff * 4);
+      d_cand_i.reserve(m * lists * k_eff * 4);
+      const float* qf = d_qf.as<float>();
+      vcb::ScanArgs a{};
+      a.codes = d_codes.as<uint32_t>();
+      a.alpha = d_alpha.as<float>();
+      a.luts = d_luts.as<uint8_t>();
+      a.lut_scale = qf;
+      a.fa_init = qf + 3 * m;
+      a.n = static_cast<long long>(n);
+      a.nbg = static_cast<int>(nbg);
+      a.nq = static_cast<long long>(m);
+      a.k = static_cast<int>(k_eff);
+      a.q_per_cta = plan.q_per_cta;
+      a.range_vectors = plan.range_vectors;
+      a.n_ranges = plan.n_ranges;
+      a.lut_chunk_groups = plan.lut_chunk_groups;
+      a.cand_score = d_cand_s.as<float>();
+      a.cand_id = d_cand_i.as<uint32_t>();
+      launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
+      scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
+      scan_queries += m;
+      vcb::MergeArgs mg{};
+      mg.cand_score = a.cand_score;
+      mg.cand_id = a.cand_id;
+      mg.nq = static_cast<long long>(m);
+      mg.n_lists = static_cast<int>(lists);
+      mg.k = static_cast<int>(k_eff);
+      mg.k_out = static_cast<int>(k_eff);
+      mg.out_score = d_scores + q0 * k_eff;
+      mg.out_id = d_ids + q0 * k_eff;
+      launch(kMerge, s, "merge kernel", [&] { return vcb::launch_merge(mg, s); });
+    }
+    (void)k;
+  }
+};
+
+namespace {
+
+void require(bool ok, int code, const char* msg) {
+  if (!ok) vcb::fail(code, msg);
+}
+
+void check_aligned(const void* p, const char* what) {
+  if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
+    vcb::fail(TQ_ERR_INVALID_ARGUMENT, std::string(what) + " must be 16-byte aligned");
+  }
+}
+
+void do_calibrate(tq_index* h, const float* d_sample, size_t n, cudaStream_t s) {
+  require(n >= 2, TQ_ERR_INVALID_ARGUMENT, "calibration needs at least 2 rows");
+  require(!h->prepared && h->n == 0, TQ_ERR_STATE, "calibrate must precede prepare()");
+  vcb::DeviceBuffer yt, qlo;
+  yt.reserve(n * h->dim * sizeof(float));
+  qlo.reserve(2 * h->dim * sizeof(float));
+  vcb::RotateArgs r{};
+  r.x = d_sample;
+  r.n = static_cast<long long>(n);
+  r.dim = static_cast<int>(h->dim);
+  r.block = static_cast<int>(h->block);
+  r.inv_sqrt_block = h->inv_sqrt_block;
+  r.perm_sign = h->d_perm_sign.as<uint32_t>();
+  r.out_t = yt.as<float>();
+  vcb::check(vcb::launch_rotate_rows_t(r, h->sms, s), "rotate kernel");
+  const vcb::TqplusAnchor anc = vcb::tqplus_anchor(n, h->bits, h->dim);
+  vcb::check(vcb::launch_order_stats(yt.as<float>(), static_cast<long long>(n), static_cast<int>(h->dim),
+                                     static_cast<long long>(anc.lo_idx),
+                                     static_cast<long long>(anc.hi_idx), qlo.as<float>(),
+                                     qlo.as<float>() + h->dim, s),
+             "order statistics kernel");
+  std::vector<float> q(2 * h->dim);
+  vcb::check(cudaMemcpyAsync(q.data(), qlo.get(), q.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  // Shift and scale per dimension (encode.cpp:277-283).
+  h->shift.assign(h->dim, 0.f);
+  h->scale.assign(h->dim, 1.f);
+  for (size_t d = 0; d < h->dim; ++d) {
+    const float q_lo = q[d], q_hi = q[h->dim + d];
+    const float span = q_hi - q_lo;
+    if (!(span > 1e-12f) || !(anc.qc_span > 0.f)) continue;
+    const float sc = anc.qc_span / span;
+    h->scale[d] = sc;
+    h->shift[d] = anc.qc_lo / sc - q_lo;
+  }
+  std::vector<float> inv(h->dim);
+  for (size_t d = 0; d < h->dim; ++d) inv[d] = 1.f / h->scale[d];
+  h->d_shift.reserve(h->dim * 4);
+  h->d_scale.reserve(h->dim * 4);
+  h->d_inv_scale.reserve(h->dim * 4);
+  h->upload(h->d_shift.get(), h->shift.data(), h->dim * 4);
+  h->upload(h->d_scale.get(), h->scale.data(), h->dim * 4);
+  h->upload(h->d_inv_scale.get(), inv.data(), h->dim * 4);
+  h->sync();
+  h->calibrated = true;
+}
+
+void do_add_device(tq_index* h, const float* d_x, size_t n, cudaStream_t s) {
+  if (n == 0) return;
+  check_aligned(d_x, "vectors");
+  if (h->prepared) {
+    h->encode_append(d_x, n, s);
+    return;
+  }
+  // Stage on the device until prepare(), like gpu::FlatIndex::add.
+  const size_t need = (h->staged_n + n) * h->dim * sizeof(float);
+  if (need > h->d_staged.bytes()) {
+    vcb::DeviceBuffer grown;
+    grown.reserve(std::max(need, h->d_staged.bytes() + h->d_staged.bytes() / 2));
+    if (h->staged_n) {
+      vcb::check(cudaMemcpyAsync(grown.get(), h->d_staged.get(), h->staged_n * h->dim * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, s),
+                 "cudaMemcpyAsync D2D");
+    }
+    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    grown.swap(h->d_staged);
+  }
+  vcb::check(cudaMemcpyAsync(h->d_staged.as<float>() + h->staged_n * h->dim, d_x, n * h->dim * sizeof(float),
+                             cudaMemcpyDeviceToDevice, s),
+             "cudaMemcpyAsync D2D");
+  h->staged_n += n;
+}
+
+// Bit-plane rows from row-major byte-group codes (encode.cpp:147-153).
+void flat_to_planes(const uint8_t* flat, size_t n, size_t bits, size_t dim, uint8_t* out) {
+  const size_t cpb = 8 / bits, field = (bits == 3) ? 4 : bits, nbg = dim / cpb, bpp = dim / 8;
+  std::memset(out, 0, n * bits * bpp);
+  for (size_t v = 0; v < n; ++v) {
+    const uint8_t* row = flat + v * nbg;
+    uint8_t* o = out + v * bits * bpp;
+    for (size_t j = 0; j < dim; ++j) {
+      const size_t g = j / cpb, sh = (cpb - 1 - j % cpb) * field;
+      const unsigned code = (row[g] >> sh) & ((1u << field) - 1u);
+      for (size_t p = 0; p < bits; ++p) {
+        o[p * bpp + j / 8] |= static_cast<uint8_t>(((code >> p) & 1u) << (7 - j % 8));
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tq_last_error(void) { return vcb::g_last_error.c_str(); }
+
+const char* tq_version(void) { return "vectorcache_b200 0.1.0 (sm_100a)"; }
+
+int tq_codebook(size_t bits, size_t dim, float* boundaries, float* centroids) {
+  return vcb::guarded([&] {
+    require(vcb::bits_supported(bits), TQ_ERR_INVALID_ARGUMENT, "bits must be 2, 3, or 4");
+    require(dim >= 2, TQ_ERR_INVALID_ARGUMENT, "dim must be >= 2");
+    const vcb::Codebook& cb = vcb::codebook(bits, dim);
+    std::memcpy(boundaries, cb.boundaries.data(), cb.boundaries.size() * 4);
+    std::memcpy(centroids, cb.centroids.data(), cb.centroids.size() * 4);
+  });
+}
+
+int tq_rotation_tables(size_t dim, float* signs, uint32_t* perm) {
+  return vcb::guarded([&] {
+    require(vcb::dim_supported(dim), TQ_ERR_INVALID_ARGUMENT,
+            "dim must be a positive multiple of 8, <= 16384");
+    const vcb::RotationTables t = vcb::make_rotation(dim);
+    std::memcpy(signs, t.signs.data(), dim * 4);
+    std::memcpy(perm, t.perm.data(), dim * 4);
+  });
+}
+
+int tq_index_create(size_t dim, size_t bits, uint32_t flags, int device, tq_index** out) {
+  return vcb::guarded([&] {
+    require(out != nullptr, TQ_ERR_INVALID_ARGUMENT, "out must not be NULL");
+    *out = nullptr;
+    require(vcb::dim_supported(dim), TQ_ERR_INVALID_ARGUMENT,
+            "dim must be a positive multiple of 8, <= 16384");
+    require(vcb::bits_supported(bits), TQ_ERR_INVALID_ARGUMENT, "bits must be 2, 3, or 4");
+    require(flags == 0, TQ_ERR_INVALID_ARGUMENT, "flags must be 0");
+    require(vcb::encode_dim_supported(static_cast<int>(dim)), TQ_ERR_UNSUPPORTED,
+            "dim > 2048 is not supported by the device kernels yet");
+    int count = 0;
+    vcb::check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    require(device >= 0 && device < count, TQ_ERR_INVALID_ARGUMENT, "no such CUDA device");
+    vcb::DeviceGuard g(device);
+    auto h = std::make_unique<tq_index>();
+    h->device = device;
+    vcb::check(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+    vcb::check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    h->dim = dim;
+    h->bits = bits;
+    h->nbg = vcb::byte_groups(bits, dim);
+    h->block = vcb::wht_block(dim);
+    h->inv_sqrt_block = 1.f / std::sqrt(static_cast<float>(h->block));
+    h->cb = vcb::codebook(bits, dim);
+    const vcb::RotationTables rot = vcb::make_rotation(dim);
+    std::vector<uint32_t> ps(dim);
+    for (size_t i = 0; i < dim; ++i) ps[i] = rot.perm[i] | (rot.signs[i] < 0.f ? 0x80000000u : 0u);
+    std::vector<float> bnd(16, 0.f), cen(16, 0.f);
+    std::copy(h->cb.boundaries.begin(), h->cb.boundaries.end(), bnd.begin());
+    std::copy(h->cb.centroids.begin(), h->cb.centroids.end(), cen.begin());
+    h->d_perm_sign.reserve(dim * 4);
+    h->d_bnd.reserve(64);
+    h->d_cen.reserve(64);
+    h->d_counter.reserve(8);
+    h->upload(h->d_perm_sign.get(), ps.data(), dim * 4);
+    h->upload(h->d_bnd.get(), bnd.data(), 64);
+    h->upload(h->d_cen.get(), cen.data(), 64);
+    vcb::check(cudaMemsetAsync(h->d_counter.get(), 0, 8, h->stream), "cudaMemsetAsync");
+    h->sync();
+    *out = h.release();
+  });
+}
+
+int tq_index_destroy(tq_index* h) {
+  return vcb::guarded([&] {
+    if (!h) return;
+    vcb::DeviceGuard g(h->device);
+    delete h;
+  });
+}
+
+int tq_index_calibrate(tq_index* h, const float* sample, size_t n) {
+  return vcb::guarded([&] {
+    require(h && sample, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(n >= 2, TQ_ERR_INVALID_ARGUMENT, "calibration needs at least 2 rows");
+    vcb::DeviceGuard g(h->device);
+    vcb::DeviceBuffer d;
+    d.reserve(n * h->dim * 4);
+    h->upload(d.get(), sample, n * h->dim * 4);
+    do_calibrate(h, d.as<float>(), n, h->stream);
+  });
+}
+
+int tq_index_calibrate_device(tq_index* h, const float* d_sample, size_t n, void* stream) {
+  return vcb::guarded([&] {
+    require(h && d_sample, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    check_aligned(d_sample, "sample");
+    vcb::DeviceGuard g(h->device);
+    do_calibrate(h, d_sample, n, h->pick(stream));
+  });
+}
+
+int tq_index_add(tq_index* h, const float* vectors, size_t n) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    if (n == 0) return;
+    require(vectors != nullptr, TQ_ERR_INVALID_ARGUMENT, "null vectors");
+    vcb::DeviceGuard g(h->device);
+    vcb::DeviceBuffer d;
+    d.reserve(n * h->dim * 4);
+    h->upload(d.get(), vectors, n * h->dim * 4);
+    do_add_device(h, d.as<float>(), n, h->stream);
+    h->sync();
+  });
+}
+
+int tq_index_add_device(tq_index* h, const float* d_vectors, size_t n, void* stream) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    if (n == 0) return;
+    require(d_vectors != nullptr, TQ_ERR_INVALID_ARGUMENT, "null vectors");
+    vcb::DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    if (s != h->stream) vcb::check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    do_add_device(h, d_vectors, n, s);
+    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  });
+}
+
+int tq_index_prepare(tq_index* h) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    if (h->prepared) return;
+    require(h->staged_n > 0, TQ_ERR_STATE, "prepare with empty index");
+    vcb::DeviceGuard g(h->device);
+    h->encode_append(h->d_staged.as<float>(), h->staged_n, h->stream);
+    h->sync();
+    h->staged_n = 0;
+    h->d_staged.release();
+    h->d_flat.release();
+    h->prepared = true;
+  });
+}
+
+int tq_index_search_device(tq_index* h, const float* d_queries, size_t nq, size_t k, float* d_scores,
+                           uint64_t* d_ids, size_t* k_eff, void* stream) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    require(h->prepared, TQ_ERR_STATE, "search before prepare");
+    require(k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be <= 256");
+    const size_t ke = std::min(k, h->n);
+    if (k_eff) *k_eff = ke;
+    if (nq == 0 || ke == 0) return;
+    require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    check_aligned(d_queries, "queries");
+    vcb::DeviceGuard g(h->device);
+    h->search_device(d_queries, nq, k, d_scores, d_ids, ke, h->pick(stream));
+  });
+}
+
+int tq_index_search(tq_index* h, const float* queries, size_t nq, size_t k, float* scores,
+                    uint64_t* ids, size_t* k_eff) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    require(h->prepared, TQ_ERR_STATE, "search before prepare");
+    require(k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be <= 256");
+    const size_t ke = std::min(k, h->n);
+    if (k_eff) *k_eff = ke;
+    if (nq == 0 || ke == 0) return;
+    require(queries && scores && ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    vcb::DeviceGuard g(h->device);
+    h->d_queries.reserve(nq * h->dim * 4);
+    h->d_out_s.reserve(nq * ke * 4);
+    h->d_out_i.reserve(nq * ke * 8);
+    h->upload(h->d_queries.get(), queries, nq * h->dim * 4);
+    h->search_device(h->d_queries.as<float>(), nq, k, h->d_out_s.as<float>(), h->d_out_i.as<uint64_t>(),
+                     ke, h->stream);
+    vcb::check(cudaMemcpyAsync(scores, h->d_out_s.get(), nq * ke * 4, cudaMemcpyDeviceToHost, h->stream),
+               "D2H");
+    vcb::check(cudaMemcpyAsync(ids, h->d_out_i.get(), nq * ke * 8, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_index_synchronize(tq_index* h) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    vcb::DeviceGuard g(h->device);
+    h->sync();
+  });
+}
+
+int tq_index_info(const tq_index* h, size_t* dim, size_t* bits, size_t* n, int* prepared, int* calibrated) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    if (dim) *dim = h->dim;
+    if (bits) *bits = h->bits;
+    if (n) *n = h->n + h->staged_n;
+    if (prepared) *prepared = h->prepared ? 1 : 0;
+    if (calibrated) *calibrated = h->calibrated ? 1 : 0;
+  });
+}
+
+int tq_index_export_codes_flat(tq_index* h, uint8_t* out) {
+  return vcb::guarded([&] {
+    require(h && out, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(h->prepared, TQ_ERR_STATE, "export before prepare");
+    vcb::DeviceGuard g(h->device);
+    vcb::DeviceBuffer d;
+    d.reserve(h->n * h->nbg);
+    vcb::check(vcb::launch_export_flat(h->d_codes.as<uint32_t>(), static_cast<long long>(h->n),
+                                       static_cast<int>(h->nbg), d.as<uint8_t>(), h->stream),
+               "export kernel");
+    vcb::check(cudaMemcpyAsync(out, d.get(), h->n * h->nbg, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_index_export_packed(tq_index* h, uint8_t* out) {
+  return vcb::guarded([&] {
+    require(h && out, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint8_t> flat(h->n * h->nbg);
+    const int rc = tq_index_export_codes_flat(h, flat.data());
+    if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+    flat_to_planes(flat.data(), h->n, h->bits, h->dim, out);
+  });
+}
+
+int tq_index_export_alpha(tq_index* h, float* out) {
+  return vcb::guarded([&] {
+    require(h && out, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(h->prepared, TQ_ERR_STATE, "export before prepare");
+    vcb::DeviceGuard g(h->device);
+    vcb::check(cudaMemcpyAsync(out, h->d_alpha.get(), h->n * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_index_export_calibration(tq_index* h, float* shift, float* scale) {
+  return vcb::guarded([&] {
+    require(h && shift && scale, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(h->calibrated, TQ_ERR_STATE, "index is not calibrated");
+    std::memcpy(shift, h->shift.data(), h->dim * 4);
+    std::memcpy(scale, h->scale.data(), h->dim * 4);
+  });
+}
+
+int tq_index_prepare_queries(tq_index* h, const float* queries, size_t nq, float* q_rot, float* bias_corr,
+                             uint8_t* luts, float* lut_scale, float* lut_bias) {
+  return vcb::guarded([&] {
+    require(h && queries, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    if (nq == 0) return;
+    vcb::DeviceGuard g(h->device);
+    h->d_queries.reserve(nq * h->dim * 4);
+    h->d_qrot.reserve(nq * h->dim * 4);
+    h->upload(h->d_queries.get(), queries, nq * h->dim * 4);
+    h->prep_queries(h->d_queries.as<float>(), nq, h->stream, h->d_qrot.as<float>());
+    const float* qf = h->d_qf.as<float>();
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+      if (dst) vcb::check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    };
+    d2h(q_rot, h->d_qrot.get(), nq * h->dim * 4);
+    d2h(luts, h->d_luts.get(), nq * h->nbg * 32);
+    d2h(lut_scale, qf, nq * 4);
+    d2h(lut_bias, qf + nq, nq * 4);
+    d2h(bias_corr, qf + 2 * nq, nq * 4);
+    h->sync();
+  });
+}
+
+int tq_index_dense_scores(tq_index* h, const float* queries, size_t nq, uint32_t* int_scores, float* scores) {
+  return vcb::guarded([&] {
+    require(h && queries, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(h->prepared, TQ_ERR_STATE, "scores before prepare");
+    if (nq == 0 || h->n == 0) return;
+    vcb::DeviceGuard g(h->device);
+    h->d_queries.reserve(nq * h->dim * 4);
+    h->upload(h->d_queries.get(), queries, nq * h->dim * 4);
+    h->prep_queries(h->d_queries.as<float>(), nq, h->stream, nullptr);
+    vcb::DeviceBuffer di, ds;
+    di.reserve(nq * h->n * 4);
+    ds.reserve(nq * h->n * 4);
+    const float* qf = h->d_qf.as<float>();
+    vcb::check(vcb::launch_dense_scores(h->d_codes.as<uint32_t>(), h->d_alpha.as<float>(),
+                                        h->d_luts.as<uint8_t>(), qf, qf + 3 * nq, static_cast<long long>(h->n),
+                                        static_cast<int>(h->nbg), static_cast<long long>(nq),
+                                        di.as<uint32_t>(), ds.as<float>(), h->stream),
+               "dense scores kernel");
+    if (int_scores) {
+      vcb::check(cudaMemcpyAsync(int_scores, di.get(), nq * h->n * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    }
+    if (scores) {
+      vcb::check(cudaMemcpyAsync(scores, ds.get(), nq * h->n * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    }
+    h->sync();
+  });
+}
+
+int tq_index_replay_count(const tq_index* h, uint64_t* count) {
+  return vcb::guarded([&] {
+    require(h && count, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    vcb::DeviceGuard g(h->device);
+    unsigned long long c = 0;
+    vcb::check(cudaMemcpy(&c, h->d_counter.get(), 8, cudaMemcpyDeviceToHost), "D2H");
+    *count = c;
+  });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int tq_index_get_stream(tq_index* h, void** stream) {
+  return vcb::guarded([&] {
+    require(h && stream, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    *stream = static_cast<void*>(h->stream);
+  });
+}
+
+int tq_index_set_profiling(tq_index* h, int enabled) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    h->profiling = enabled != 0;
+  });
+}
+
+int tq_index_read_profile(tq_index* h, tq_profile* out) {
+  return vcb::guarded([&] {
+    require(h && out, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    vcb::DeviceGuard g(h->device);
+    tq_profile p{};
+    double* ms[4] = {&p.prep_ms, &p.scan_ms, &p.merge_ms, &p.encode_ms};
+    for (auto& t : h->timed_launches) {
+      vcb::check(cudaEventSynchronize(t.stop), "cudaEventSynchronize");
+      float e = 0.f;
+      vcb::check(cudaEventElapsedTime(&e, t.start, t.stop), "cudaEventElapsedTime");
+      *ms[t.kind] += e;
+      h->event_pool.push_back(t.start);
+      h->event_pool.push_back(t.stop);
+    }
+    h->timed_launches.clear();
+    p.prep_launches = h->launches[tq_index::kPrep];
+    p.scan_launches = h->launches[tq_index::kScan];
+    p.merge_launches = h->launches[tq_index::kMerge];
+    p.encode_launches = h->launches[tq_index::kEncode];
+    p.scan_stream_bytes = h->scan_stream_bytes;
+    p.scan_queries = h->scan_queries;
+    for (auto& c : h->launches) c = 0;
+    h->scan_stream_bytes = 0;
+    h->scan_queries = 0;
+    *out = p;
+  });
+}
+
+}  // extern "C"
