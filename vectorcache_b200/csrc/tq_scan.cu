@@ -28,6 +28,8 @@ namespace {
 
 constexpr int kScanWarps = 8;
 constexpr int kMergeBuf = 512;  // per-warp sort buffer: 256 new + up to 256 kept
+constexpr int kPrefetch = 4;    // byte groups of codes in flight per thread
+constexpr int kRegTopK = 32;    // k up to this is kept in registers, one entry per lane
 
 struct __align__(16) LutHalf {
   uint32_t w[4];
@@ -56,19 +58,97 @@ __device__ __forceinline__ void warp_sort_best_first(float* s, uint32_t* id, int
   }
 }
 
-template <int Q, int KMAX>
-__global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
+// k-th largest of the 32 lane values (k <= 32), by a shuffle bitonic sort.
+__device__ __forceinline__ float warp_kth_largest(float v, int k, int lane) {
+#pragma unroll
+  for (int size = 2; size <= kWarp; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const float o = __shfl_xor_sync(full_mask(), v, stride);
+      const bool lower = (lane & stride) == 0;
+      const bool desc = (lane & size) == 0;  // final pass: descending everywhere
+      // keep the larger value in the lower lane of a descending block
+      const bool take_max = (lower == desc);
+      v = take_max ? fmaxf(v, o) : fminf(v, o);
+    }
+  }
+  return __shfl_sync(full_mask(), v, k - 1);
+}
+
+// Running top-k of one warp for one query, one entry per lane (k <= 32),
+// sorted best first; empty slots hold (-inf, 0xffffffff).
+struct RegTopK {
+  float s = -INFINITY;
+  uint32_t i = 0xffffffffu;
+  float thr_s = -INFINITY;  // entry k-1
+  uint32_t thr_i = 0xffffffffu;
+
+  __device__ __forceinline__ void insert(float cs, uint32_t ci, int k, int lane) {
+    const unsigned ahead = __ballot_sync(full_mask(), lane < k && better(s, i, cs, ci));
+    const int pos = __popc(ahead);
+    const float up_s = __shfl_up_sync(full_mask(), s, 1);
+    const uint32_t up_i = __shfl_up_sync(full_mask(), i, 1);
+    if (lane > pos) {
+      s = up_s;
+      i = up_i;
+    } else if (lane == pos) {
+      s = cs;
+      i = ci;
+    }
+    thr_s = __shfl_sync(full_mask(), s, k - 1);
+    thr_i = __shfl_sync(full_mask(), i, k - 1);
+  }
+
+  // Offer the 8 scores of every lane (vectors vbase..vbase+7 of that lane).
+  __device__ __forceinline__ void offer(const float (&sc)[8], unsigned valid, uint32_t vbase, int k,
+                                        int lane) {
+    unsigned pass = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if ((valid >> j & 1u) && better(sc[j], vbase + j, thr_s, thr_i)) pass |= 1u << j;
+    }
+    if (!(thr_s > -INFINITY)) {
+      // List not full yet (first block): a lane maximum ranked k-th among the
+      // 32 lane maxima is a lower bound of the k-th best score, so anything
+      // strictly below it cannot enter the final top-k.
+      float mx = -INFINITY;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (pass >> j & 1u) mx = fmaxf(mx, sc[j]);
+      }
+      const float bound = warp_kth_largest(mx, k, lane);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if ((pass >> j & 1u) && sc[j] < bound) pass &= ~(1u << j);
+      }
+    }
+    unsigned any = __ballot_sync(full_mask(), pass != 0);
+    while (any) {
+      const int src = __ffs(any) - 1;
+      const int my_j = __ffs(pass) - 1;
+      float my_s = sc[0];
+#pragma unroll
+      for (int j = 1; j < 8; ++j) {
+        if (j == my_j) my_s = sc[j];
+      }
+      const int j = __shfl_sync(full_mask(), my_j, src);
+      const float cs = __shfl_sync(full_mask(), my_s, src);
+      const uint32_t ci = __shfl_sync(full_mask(), vbase, src) + static_cast<uint32_t>(j);
+      if (lane == src) pass &= pass - 1;
+      any = __ballot_sync(full_mask(), pass != 0);
+      if (better(cs, ci, thr_s, thr_i)) insert(cs, ci, k, lane);
+    }
+  }
+};
+
+template <int Q, int KMAX, int MIN_BLOCKS>
+__global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
+  constexpr bool kReg = KMAX <= kRegTopK;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nbg = a.nbg;
   const int chunk = a.lut_chunk_groups;
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [Q][chunk][2]
-  unsigned char* warp_area = smem + static_cast<size_t>(Q) * chunk * 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const size_t warp_bytes = static_cast<size_t>(Q) * KMAX * 8 + kMergeBuf * 8;
-  float* list_s = reinterpret_cast<float*>(warp_area + warp * warp_bytes);
-  uint32_t* list_i = reinterpret_cast<uint32_t*>(list_s + Q * KMAX);
-  float* buf_s = reinterpret_cast<float*>(list_i + Q * KMAX);
-  uint32_t* buf_i = reinterpret_cast<uint32_t*>(buf_s + kMergeBuf);
 
   const long long q0 = static_cast<long long>(blockIdx.x) * Q;
   const int range = blockIdx.y;
@@ -84,9 +164,24 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
     scale[q] = ok ? a.lut_scale[q0 + q] : 0.f;
     init[q] = ok ? a.fa_init[q0 + q] : 0.f;
   }
+
+  // Top-k state: registers for k <= 32, shared memory lists otherwise.
+  RegTopK top[kReg ? Q : 1];
   float thr_s[Q];
   uint32_t thr_i[Q];
   int cnt[Q];
+  float* list_s = nullptr;
+  uint32_t* list_i = nullptr;
+  float* buf_s = nullptr;
+  uint32_t* buf_i = nullptr;
+  if constexpr (!kReg) {
+    unsigned char* warp_area = smem + static_cast<size_t>(Q) * chunk * 32;
+    const size_t warp_bytes = static_cast<size_t>(Q) * KMAX * 8 + kMergeBuf * 8;
+    list_s = reinterpret_cast<float*>(warp_area + warp * warp_bytes);
+    list_i = reinterpret_cast<uint32_t*>(list_s + Q * KMAX);
+    buf_s = reinterpret_cast<float*>(list_i + Q * KMAX);
+    buf_i = reinterpret_cast<uint32_t*>(buf_s + kMergeBuf);
+  }
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     thr_s[q] = -FLT_MAX;
@@ -113,6 +208,7 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
   }
 
   const int half = warp & 1;
+  constexpr long long kGroupStride = kTileWords / 2;  // uint2 per group row
   for (long long blk = v_begin; blk < v_end; blk += kScanBlockVectors) {
     const long long tile = blk / kTileVectors + (warp >> 1);
     const uint2* wp = reinterpret_cast<const uint2*>(a.codes + tile * nbg * kTileWords + half * 64) + lane;
@@ -137,26 +233,39 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
         __syncthreads();
       }
       const int chunk_base = resident ? 0 : (gb / chunk) * chunk;
-      uint2 nxt = wp[static_cast<long long>(gb) * (kTileWords / 2)];
-      for (int g = gb; g < g_stop; ++g) {
-        const uint2 w = nxt;
-        if (g + 1 < g_stop) nxt = wp[static_cast<long long>(g + 1) * (kTileWords / 2)];
-        const uint32_t x0 = w.x, x1 = w.y;
-        const uint32_t t0 = x0 ^ 0x88888888u, t1 = x1 ^ 0x88888888u;
-        const uint32_t x0h = x0 >> 16, x1h = x1 >> 16, t0h = t0 >> 16, t1h = t1 >> 16;
-        const LutHalf* lg = s_lut + (g - chunk_base) * 2;
+      uint2 ring[kPrefetch];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-          const LutHalf F = lg[q * chunk * 2];      // entries 0..15: high nibble
-          const LutHalf S = lg[q * chunk * 2 + 1];  // entries 16..31: low nibble
-          const uint32_t s0 = prmt(S.w[0], S.w[1], x0) + prmt(S.w[2], S.w[3], t0) +
-                              prmt(F.w[0], F.w[1], x0h) + prmt(F.w[2], F.w[3], t0h);
-          const uint32_t s1 = prmt(S.w[0], S.w[1], x1) + prmt(S.w[2], S.w[3], t1) +
-                              prmt(F.w[0], F.w[1], x1h) + prmt(F.w[2], F.w[3], t1h);
+      for (int u = 0; u < kPrefetch; ++u) {
+        ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
+      }
+      for (int g = gb; g < g_stop; g += kPrefetch) {
+        uint2 cur[kPrefetch];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            acc[q][j] = __dp4a(s0, 1u << (8 * j), acc[q][j]);
-            acc[q][4 + j] = __dp4a(s1, 1u << (8 * j), acc[q][4 + j]);
+        for (int u = 0; u < kPrefetch; ++u) {
+          cur[u] = ring[u];
+          const int gn = g + kPrefetch + u;
+          ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < kPrefetch; ++u) {
+          if (g + u >= g_stop) break;
+          const uint32_t x0 = cur[u].x, x1 = cur[u].y;
+          const uint32_t t0 = x0 ^ 0x88888888u, t1 = x1 ^ 0x88888888u;
+          const uint32_t x0h = x0 >> 16, x1h = x1 >> 16, t0h = t0 >> 16, t1h = t1 >> 16;
+          const LutHalf* lg = s_lut + (g + u - chunk_base) * 2;
+#pragma unroll
+          for (int q = 0; q < Q; ++q) {
+            const LutHalf F = lg[q * chunk * 2];      // entries 0..15: high nibble
+            const LutHalf S = lg[q * chunk * 2 + 1];  // entries 16..31: low nibble
+            const uint32_t s0 = prmt(S.w[0], S.w[1], x0) + prmt(S.w[2], S.w[3], t0) +
+                                prmt(F.w[0], F.w[1], x0h) + prmt(F.w[2], F.w[3], t0h);
+            const uint32_t s1 = prmt(S.w[0], S.w[1], x1) + prmt(S.w[2], S.w[3], t1) +
+                                prmt(F.w[0], F.w[1], x1h) + prmt(F.w[2], F.w[3], t1h);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              acc[q][j] = __dp4a(s0, 1u << (8 * j), acc[q][j]);
+              acc[q][4 + j] = __dp4a(s1, 1u << (8 * j), acc[q][4 + j]);
+            }
           }
         }
       }
@@ -179,63 +288,77 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
       al[0] = a0.x; al[1] = a0.y; al[2] = a0.z; al[3] = a0.w;
       al[4] = a1.x; al[5] = a1.y; al[6] = a1.z; al[7] = a1.w;
     }
+    unsigned valid = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const long long v = vbase + j;
+      if (v < v_end) valid |= 1u << j;
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       if (q0 + q >= a.nq) break;  // warp-uniform
       float sc[8];
-      unsigned pass = 0;
+      unsigned ok_mask = 0;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), 0.f);
-        const long long v = vbase + j;
-        const bool ok = v < v_end && v >= v_begin && sc[j] > -INFINITY &&
-                        (cnt[q] < k ? true : better(sc[j], static_cast<uint32_t>(v), thr_s[q], thr_i[q]));
-        pass |= static_cast<unsigned>(ok) << j;
+        if ((valid >> j & 1u) && sc[j] > -INFINITY) ok_mask |= 1u << j;
       }
-      const int mine = __popc(pass);
-      int incl = mine;
+      if constexpr (kReg) {
+        top[q].offer(sc, ok_mask, static_cast<uint32_t>(vbase), k, lane);
+      } else {
+        unsigned pass = 0;
 #pragma unroll
-      for (int o = 1; o < kWarp; o <<= 1) {
-        const int t = __shfl_up_sync(full_mask(), incl, o);
-        if (lane >= o) incl += t;
-      }
-      const int total = __shfl_sync(full_mask(), incl, kWarp - 1);
-      if (total == 0) continue;
-      int pos = incl - mine;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (pass >> j & 1u) {
-          buf_s[pos] = sc[j];
-          buf_i[pos] = static_cast<uint32_t>(vbase + j);
-          ++pos;
+        for (int j = 0; j < 8; ++j) {
+          const bool ok = (ok_mask >> j & 1u) &&
+                          (cnt[q] < k ? true : better(sc[j], static_cast<uint32_t>(vbase + j), thr_s[q], thr_i[q]));
+          pass |= static_cast<unsigned>(ok) << j;
         }
+        const int mine = __popc(pass);
+        int incl = mine;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+          const int t = __shfl_up_sync(full_mask(), incl, o);
+          if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(full_mask(), incl, kWarp - 1);
+        if (total == 0) continue;
+        int pos = incl - mine;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (pass >> j & 1u) {
+            buf_s[pos] = sc[j];
+            buf_i[pos] = static_cast<uint32_t>(vbase + j);
+            ++pos;
+          }
+        }
+        float* ls = list_s + q * KMAX;
+        uint32_t* li = list_i + q * KMAX;
+        for (int t = lane; t < cnt[q]; t += kWarp) {
+          buf_s[total + t] = ls[t];
+          buf_i[total + t] = li[t];
+        }
+        const int tot = total + cnt[q];
+        int p = 32;
+        while (p < tot) p <<= 1;
+        for (int t = tot + lane; t < p; t += kWarp) {
+          buf_s[t] = -INFINITY;
+          buf_i[t] = 0xffffffffu;
+        }
+        __syncwarp();
+        warp_sort_best_first(buf_s, buf_i, p, lane);
+        const int keep = min(k, tot);
+        for (int t = lane; t < keep; t += kWarp) {
+          ls[t] = buf_s[t];
+          li[t] = buf_i[t];
+        }
+        cnt[q] = keep;
+        if (keep == k) {
+          thr_s[q] = buf_s[k - 1];
+          thr_i[q] = buf_i[k - 1];
+        }
+        __syncwarp();
       }
-      float* ls = list_s + q * KMAX;
-      uint32_t* li = list_i + q * KMAX;
-      for (int t = lane; t < cnt[q]; t += kWarp) {
-        buf_s[total + t] = ls[t];
-        buf_i[total + t] = li[t];
-      }
-      const int tot = total + cnt[q];
-      int p = 32;
-      while (p < tot) p <<= 1;
-      for (int t = tot + lane; t < p; t += kWarp) {
-        buf_s[t] = -INFINITY;
-        buf_i[t] = 0xffffffffu;
-      }
-      __syncwarp();
-      warp_sort_best_first(buf_s, buf_i, p, lane);
-      const int keep = min(k, tot);
-      for (int t = lane; t < keep; t += kWarp) {
-        ls[t] = buf_s[t];
-        li[t] = buf_i[t];
-      }
-      cnt[q] = keep;
-      if (keep == k) {
-        thr_s[q] = buf_s[k - 1];
-        thr_i[q] = buf_i[k - 1];
-      }
-      __syncwarp();
     }
   }
 
@@ -247,10 +370,17 @@ __global__ void __launch_bounds__(kScanWarps * 32) scan_kernel(ScanArgs a) {
     const long long list = ((q0 + q) * a.n_ranges + range) * kScanWarps + warp;
     float* os = a.cand_score + list * k;
     uint32_t* oi = a.cand_id + list * k;
-    for (int t = lane; t < k; t += kWarp) {
-      const bool have = t < cnt[q];
-      os[t] = have ? list_s[q * KMAX + t] : -INFINITY;
-      oi[t] = have ? list_i[q * KMAX + t] : 0xffffffffu;
+    if constexpr (kReg) {
+      if (lane < k) {
+        os[lane] = top[q].s;
+        oi[lane] = top[q].i;
+      }
+    } else {
+      for (int t = lane; t < k; t += kWarp) {
+        const bool have = t < cnt[q];
+        os[t] = have ? list_s[q * KMAX + t] : -INFINITY;
+        oi[t] = have ? list_i[q * KMAX + t] : 0xffffffffu;
+      }
     }
   }
 }
@@ -374,17 +504,18 @@ __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const fl
   if (out_score) out_score[idx] = __fadd_rn(__fmul_rn(fa, alpha[v]), 0.f);
 }
 
-template <int Q, int KMAX>
+template <int Q, int KMAX, int MINB>
 cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(plan.smem_bytes));
   if (e != cudaSuccess) return e;
   dim3 grid(static_cast<unsigned>((a.nq + Q - 1) / Q), static_cast<unsigned>(plan.n_ranges));
-  scan_kernel<Q, KMAX><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
+  scan_kernel<Q, KMAX, MINB><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
   return cudaGetLastError();
 }
 
 size_t scan_warp_bytes(int q, int kmax) {
+  if (kmax <= kRegTopK) return 0;
   return static_cast<size_t>(q) * kmax * 8 + kMergeBuf * 8;
 }
 
@@ -392,28 +523,30 @@ size_t scan_warp_bytes(int q, int kmax) {
 
 bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan) {
   if (k < 1 || k > kMaxK || n <= 0 || nq <= 0) return false;
-  const int kmax = k <= 16 ? 16 : (k <= 64 ? 64 : 256);
-  int q = 4;
-  if (kmax == 256) q = 2;
+  const int kmax = k <= kRegTopK ? kRegTopK : (k <= 64 ? 64 : 256);
+  const bool reg = kmax <= kRegTopK;
+  // Register top-k leaves shared memory to the LUTs: two CTAs per SM.
+  const size_t budget = reg ? 110 * 1024 : 220 * 1024;
+  int q = (kmax == 256) ? 2 : 4;
   while (q > 1 && nq <= q / 2) q >>= 1;
-  const size_t budget = 220 * 1024;
-  size_t warp_total = kScanWarps * scan_warp_bytes(q, kmax);
+  // Prefer fewer queries per CTA over streaming the LUT in chunks.
+  while (q > 1 && static_cast<size_t>(q) * nbg * 32 + kScanWarps * scan_warp_bytes(q, kmax) > budget &&
+         static_cast<size_t>(q / 2) * nbg * 32 + kScanWarps * scan_warp_bytes(q / 2, kmax) <= budget) {
+    q >>= 1;
+  }
+  const size_t warp_total = kScanWarps * scan_warp_bytes(q, kmax);
   int chunk = nbg;
   while (static_cast<size_t>(q) * chunk * 32 + warp_total > budget) {
     if (chunk > kFlushGroups) {
       chunk = ((chunk - 1) / kFlushGroups) * kFlushGroups;
       if (chunk < kFlushGroups) chunk = kFlushGroups;
-    } else if (q > 1) {
-      q >>= 1;
-      warp_total = kScanWarps * scan_warp_bytes(q, kmax);
-      chunk = nbg;
     } else {
       return false;
     }
   }
   const long long blocks = (n + kScanBlockVectors - 1) / kScanBlockVectors;
   const long long qgroups = (nq + q - 1) / q;
-  const long long target = static_cast<long long>(sms) * 4;
+  const long long target = static_cast<long long>(sms) * (reg ? 8 : 4);
   long long ranges = (target + qgroups - 1) / qgroups;
   if (ranges < 1) ranges = 1;
   if (ranges > blocks) ranges = blocks;
@@ -431,11 +564,11 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
 
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
   const int q = plan.q_per_cta, km = plan.kmax;
-#define VCB_SCAN(QQ, KK) \
-  if (q == QQ && km == KK) return launch_scan_t<QQ, KK>(a, plan, stream);
-  VCB_SCAN(1, 16) VCB_SCAN(2, 16) VCB_SCAN(4, 16)
-  VCB_SCAN(1, 64) VCB_SCAN(2, 64) VCB_SCAN(4, 64)
-  VCB_SCAN(1, 256) VCB_SCAN(2, 256)
+#define VCB_SCAN(QQ, KK, MB) \
+  if (q == QQ && km == KK) return launch_scan_t<QQ, KK, MB>(a, plan, stream);
+  VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
+  VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
+  VCB_SCAN(1, 256, 1) VCB_SCAN(2, 256, 1)
 #undef VCB_SCAN
   return cudaErrorInvalidValue;
 }
