@@ -162,21 +162,11 @@ def max_over_ranks(world, value: float) -> float:
 
 def merge_shards(world, scores, ids, k):
     """All-gather every rank's top-k and merge: score desc, equal scores by lower id."""
-    import torch
-    import torch.distributed as dist
-
     if world == 1:
         return scores, ids
-    gs = [torch.empty_like(scores) for _ in range(world)]
-    gi = [torch.empty_like(ids) for _ in range(world)]
-    dist.all_gather(gs, scores)
-    dist.all_gather(gi, ids)
-    s = torch.cat(gs, dim=1)
-    i = torch.cat(gi, dim=1)
-    order = torch.argsort(i, dim=1, stable=True)
-    s, i = torch.gather(s, 1, order), torch.gather(i, 1, order)
-    order = torch.argsort(s, dim=1, descending=True, stable=True)
-    return torch.gather(s, 1, order)[:, :k], torch.gather(i, 1, order)[:, :k]
+    from vectorcache_b200.sharded import allgather_merge
+
+    return allgather_merge(scores, ids, k)
 
 
 def exact_topk(db, q, k):
@@ -347,6 +337,25 @@ def run_ours(args, world, rank, local):
     queries_scanned = args.nq * args.steps * world  # one query against one 1M-vector shard = one unit
     value = queries_scanned / (elapsed_ms / 1e3)
 
+    # Latency of small batches (device-resident queries): p50 / p99 over repeats.
+    latency = {}
+    if world == 1:
+        for bsz, reps in ((1, 50), (16, 30), (256, 15)):
+            times = []
+            sub = q[:bsz]
+            for r in range(reps + 3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                index.search_device(sub, k, d_scores, d_ids, stream=stream)
+                e1.record(stream)
+                e1.synchronize()
+                if r >= 3:
+                    times.append(e0.elapsed_time(e1))
+            latency[f"nq={bsz}"] = {"p50_ms": float(np.percentile(times, 50)),
+                                    "p99_ms": float(np.percentile(times, 99)),
+                                    "qps": bsz / (float(np.median(times)) / 1e3)}
+        index.read_profile()
+
     # End to end through the public host-buffer API: pinned host queries in,
     # host top-k out, copies inside the timed region.
     q_host = q.cpu().pin_memory()
@@ -432,6 +441,7 @@ def run_ours(args, world, rank, local):
                                        "merge": prof["merge_ms"] / args.steps},
                 "nibble_lookups_per_s": lookups * args.steps / (prof["scan_ms"] / 1e3) if prof["scan_ms"] else None,
                 "encode_kernel_ms": prof_build["encode_ms"],
+                "latency_ms": latency,
             },
             "roofline": {"kernel": "scan_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": tr,

@@ -59,6 +59,10 @@ CASES = [
     ("pl", 2048, 300, 5, 4, True),
     ("mix", 8, 100, 4, 4, False),
     ("mix", 96, 64, 3, 3, True),
+    # wider than 2048: the shared-memory row kernels
+    ("mix", 3072, 300, 4, 3, True),
+    ("mix", 4096, 257, 3, 4, False),
+    ("mix", 16384, 70, 2, 2, True),
 ]
 
 

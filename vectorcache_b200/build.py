@@ -19,7 +19,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libvectorcache_b200.so"
-SOURCES = ["tq_host_math.cpp", "tq_encode.cu", "tq_query.cu", "tq_scan.cu", "tq_index.cu"]
+SOURCES = ["tq_host_math.cpp", "tq_encode.cu", "tq_query.cu", "tq_scan.cu", "tq_bigdim.cu", "tq_index.cu"]
 HEADERS = ["tq_host_math.h", "tq_kernels.h", "tq_device.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -330,12 +330,13 @@ size_t encode_smem_bytes(int dim, bool tqplus) {
   return static_cast<size_t>(dim) * 4 * (tqplus ? 4 : 1) + 32 * 4 + static_cast<size_t>(8) * dim * 4;
 }
 
-bool encode_dim_supported(int dim) { return rows_template(dim) > 0; }
+bool encode_dim_supported(int dim) { return dim > 0 && dim <= 16384; }
 
 #define VCB_ROWS_CASES(X) X(1) X(2) X(3) X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64)
 
 cudaError_t launch_encode(const EncodeArgs& a, int sms, cudaStream_t stream) {
   if (a.n == 0) return cudaSuccess;
+  if (a.dim > kRegisterRowMaxDim) return launch_encode_big(a, sms, stream);
   const int r = rows_template(a.dim);
   const size_t smem = encode_smem_bytes(a.dim, a.tqplus);
   const int grid = grid_for_quads(a.n, sms);
@@ -377,6 +378,7 @@ cudaError_t launch_export_flat(const uint32_t* codes, long long n, int nbg, uint
 
 cudaError_t launch_rotate_rows_t(const RotateArgs& a, int sms, cudaStream_t stream) {
   if (a.n == 0) return cudaSuccess;
+  if (a.dim > kRegisterRowMaxDim) return launch_rotate_rows_t_big(a, sms, stream);
   const int r = rows_template(a.dim);
   const size_t smem = static_cast<size_t>(a.dim) * 4 + static_cast<size_t>(8) * a.dim * 4;
   const int grid = grid_for_quads(a.n, sms);

@@ -325,6 +325,7 @@ struct tq_index {
       a.range_vectors = plan.range_vectors;
       a.n_ranges = plan.n_ranges;
       a.lut_chunk_groups = plan.lut_chunk_groups;
+      a.bits = static_cast<int>(bits);
       a.cand_score = d_cand_s.as<float>();
       a.cand_id = d_cand_i.as<uint32_t>();
       launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });

@@ -89,6 +89,7 @@ struct ScanArgs {
   long long range_vectors; // vectors per CTA range (multiple of kScanBlockVectors)
   int n_ranges;
   int lut_chunk_groups;    // groups resident in shared memory at once (multiple of 256 or nbg)
+  int bits = 4;            // 3 selects the lookup that skips nibble values >= 8
   float* cand_score;       // nq x n_ranges x k
   uint32_t* cand_id;
 };
@@ -115,6 +116,13 @@ cudaError_t launch_order_stats(const float* yt, long long n, int dim, long long 
                                long long hi_rank, float* q_lo, float* q_hi, cudaStream_t stream);
 
 cudaError_t launch_query_prep(const QueryPrepArgs& a, int sms, cudaStream_t stream);
+
+// Rows wider than 2048 coordinates: one CTA per row, row in shared memory
+// (tq_bigdim.cu). The launchers above dispatch here by themselves.
+constexpr int kRegisterRowMaxDim = 2048;
+cudaError_t launch_encode_big(const EncodeArgs& a, int sms, cudaStream_t stream);
+cudaError_t launch_query_prep_big(const QueryPrepArgs& a, int sms, cudaStream_t stream);
+cudaError_t launch_rotate_rows_t_big(const RotateArgs& a, int sms, cudaStream_t stream);
 
 // Scan plan: queries per CTA, ranges, chunking. Filled by plan_scan().
 struct ScanPlan {

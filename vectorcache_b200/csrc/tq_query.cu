@@ -213,6 +213,7 @@ int rows_template_q(int dim) {
 
 cudaError_t launch_query_prep(const QueryPrepArgs& a, int sms, cudaStream_t stream) {
   if (a.nq == 0) return cudaSuccess;
+  if (a.dim > kRegisterRowMaxDim) return launch_query_prep_big(a, sms, stream);
   const int r = rows_template_q(a.dim);
   const size_t smem = static_cast<size_t>(a.dim) * 4 * (a.tqplus ? 3 : 1) + 16 * 4 +
                       static_cast<size_t>(kPrepWarps) * (a.dim + 4 * a.nbg) * 4;

@@ -141,7 +141,7 @@ struct RegTopK {
   }
 };
 
-template <int Q, int KMAX, int MIN_BLOCKS>
+template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
   constexpr bool kReg = KMAX <= kRegTopK;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -257,10 +257,17 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           for (int q = 0; q < Q; ++q) {
             const LutHalf F = lg[q * chunk * 2];      // entries 0..15: high nibble
             const LutHalf S = lg[q * chunk * 2 + 1];  // entries 16..31: low nibble
-            const uint32_t s0 = prmt(S.w[0], S.w[1], x0) + prmt(S.w[2], S.w[3], t0) +
-                                prmt(F.w[0], F.w[1], x0h) + prmt(F.w[2], F.w[3], t0h);
-            const uint32_t s1 = prmt(S.w[0], S.w[1], x1) + prmt(S.w[2], S.w[3], t1) +
-                                prmt(F.w[0], F.w[1], x1h) + prmt(F.w[2], F.w[3], t1h);
+            uint32_t s0, s1;
+            if constexpr (NIBBLE8) {
+              // 3-bit codes: every nibble is < 8, entries 8..15 are never used.
+              s0 = prmt(S.w[0], S.w[1], x0) + prmt(F.w[0], F.w[1], x0h);
+              s1 = prmt(S.w[0], S.w[1], x1) + prmt(F.w[0], F.w[1], x1h);
+            } else {
+              s0 = prmt(S.w[0], S.w[1], x0) + prmt(S.w[2], S.w[3], t0) +
+                   prmt(F.w[0], F.w[1], x0h) + prmt(F.w[2], F.w[3], t0h);
+              s1 = prmt(S.w[0], S.w[1], x1) + prmt(S.w[2], S.w[3], t1) +
+                   prmt(F.w[0], F.w[1], x1h) + prmt(F.w[2], F.w[3], t1h);
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               acc[q][j] = __dp4a(s0, 1u << (8 * j), acc[q][j]);
@@ -504,13 +511,13 @@ __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const fl
   if (out_score) out_score[idx] = __fadd_rn(__fmul_rn(fa, alpha[v]), 0.f);
 }
 
-template <int Q, int KMAX, int MINB>
+template <int Q, int KMAX, int MINB, bool N8>
 cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB, N8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(plan.smem_bytes));
   if (e != cudaSuccess) return e;
   dim3 grid(static_cast<unsigned>((a.nq + Q - 1) / Q), static_cast<unsigned>(plan.n_ranges));
-  scan_kernel<Q, KMAX, MINB><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
+  scan_kernel<Q, KMAX, MINB, N8><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -564,8 +571,12 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
 
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
   const int q = plan.q_per_cta, km = plan.kmax;
-#define VCB_SCAN(QQ, KK, MB) \
-  if (q == QQ && km == KK) return launch_scan_t<QQ, KK, MB>(a, plan, stream);
+  const bool n8 = a.bits == 3;  // 3-bit codes never set a nibble's top bit
+#define VCB_SCAN(QQ, KK, MB)                                                             \
+  if (q == QQ && km == KK) {                                                             \
+    return n8 ? launch_scan_t<QQ, KK, MB, true>(a, plan, stream)                         \
+              : launch_scan_t<QQ, KK, MB, false>(a, plan, stream);                       \
+  }
   VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
   VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
   VCB_SCAN(1, 256, 1) VCB_SCAN(2, 256, 1)
