@@ -156,6 +156,34 @@ typedef struct tq_profile {
 int tq_index_set_profiling(tq_index* h, int enabled);
 int tq_index_read_profile(tq_index* h, tq_profile* out);
 
+/* ---- search without device allocation --------------------------------------
+ * No counterpart in the reference.
+ *
+ * Same inputs, outputs and results as tq_index_search_device, but the call
+ * allocates no device memory: its temporary buffers (query LUTs, per-query
+ * constants, candidate lists) live in one fixed 16 MiB array compiled into the
+ * library, which every GPU that loads the library holds until the process
+ * exits. It is meant for callers that may not allocate while serving queries —
+ * for example a server that hands all free HBM to its own pool up front, or a
+ * latency-critical loop that cannot afford cudaMalloc's implicit
+ * synchronization. The index itself must already be prepared.
+ *
+ * Limits: a request must fit in the 16 MiB array — nq * (dim / (8 / bits)) * 32
+ * bytes of LUTs plus 16 bytes per query plus the candidate lists (at least
+ * nq * 8 * k_eff * 8 bytes). Larger requests fail with TQ_ERR_INVALID_ARGUMENT
+ * before any work is queued; split them into smaller batches.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. All calls on one device share the array and each
+ * call overwrites everything it reads from it (nothing has to start at zero),
+ * so calls whose work overlaps on the GPU — on different streams or for
+ * different indexes on the same device — race and must be serialized by the
+ * caller. Returns without synchronizing `stream` (NULL: the index's stream). */
+int tq_index_search_device_noalloc(tq_index* h, const float* d_queries, size_t nq, size_t k,
+                                   float* d_scores, uint64_t* d_ids, size_t* k_eff,
+                                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

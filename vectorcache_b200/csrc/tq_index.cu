@@ -12,6 +12,7 @@
 #include <cstring>
 #include <exception>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -801,3 +802,142 @@ int tq_index_read_profile(tq_index* h, tq_profile* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Search without device allocation (tq_index_search_device_noalloc).
+//
+// Callers that may not allocate device memory while serving (a server that
+// reserved all free HBM for its own pool, a loop that cannot take cudaMalloc's
+// implicit synchronization) get the same search with its temporaries placed in
+// one fixed array compiled into the library. Every GPU that loads the library
+// holds this array until the process exits.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t{16} << 20;  // 16 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current).
+// In host code the symbol's name is only a host-side handle, so the address is
+// looked up once per device and cached.
+unsigned char* noalloc_scratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    vcb::fail(TQ_ERR_UNSUPPORTED, "device ordinal out of range for the no-alloc scratch table");
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[device] == nullptr) {
+    void* p = nullptr;
+    vcb::check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+    g_noalloc_addr[device] = p;
+  }
+  return static_cast<unsigned char*>(g_noalloc_addr[device]);
+}
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+}  // namespace
+
+extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_queries, size_t nq, size_t k,
+                                              float* d_scores, uint64_t* d_ids, size_t* k_eff,
+                                              void* stream) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    require(h->prepared, TQ_ERR_STATE, "search before prepare");
+    require(k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be <= 256");
+    const size_t ke = std::min(k, h->n);
+    if (k_eff) *k_eff = ke;
+    if (nq == 0 || ke == 0) return;
+    require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    check_aligned(d_queries, "queries");
+
+    // Carve the fixed array: LUTs, per-query constants, candidate lists.
+    const size_t lut_bytes = align256(nq * h->nbg * 32);
+    const size_t qf_bytes = align256(nq * 4 * sizeof(float));
+    const size_t per_list = nq * ke * (sizeof(float) + sizeof(uint32_t));
+    if (lut_bytes + qf_bytes + 8 * per_list > kNoAllocScratchBytes) {
+      vcb::fail(TQ_ERR_INVALID_ARGUMENT,
+                "request needs " + std::to_string(lut_bytes + qf_bytes + 8 * per_list) +
+                    " bytes of no-alloc scratch; the fixed array holds " +
+                    std::to_string(kNoAllocScratchBytes) + " bytes (search fewer queries per call)");
+    }
+    vcb::ScanPlan plan;
+    if (!vcb::plan_scan(static_cast<long long>(h->n), static_cast<long long>(nq), static_cast<int>(h->nbg),
+                        static_cast<int>(ke), h->sms, &plan)) {
+      vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
+    }
+    // Fewer vector ranges if their candidate lists would not fit.
+    const size_t max_lists = (kNoAllocScratchBytes - lut_bytes - qf_bytes) / per_list;
+    if (static_cast<size_t>(plan.n_ranges) * 8 > max_lists) {
+      const long long blocks = (static_cast<long long>(h->n) + vcb::kScanBlockVectors - 1) / vcb::kScanBlockVectors;
+      long long ranges = static_cast<long long>(max_lists / 8);
+      const long long per_range = (blocks + ranges - 1) / ranges;
+      ranges = (blocks + per_range - 1) / per_range;
+      plan.n_ranges = static_cast<int>(ranges);
+      plan.range_vectors = per_range * vcb::kScanBlockVectors;
+    }
+    const size_t lists = static_cast<size_t>(plan.n_ranges) * 8;
+
+    vcb::DeviceGuard g(h->device);
+    unsigned char* base = noalloc_scratch(h->device);
+    uint8_t* luts = base;
+    float* qf = reinterpret_cast<float*>(base + lut_bytes);
+    float* cand_s = reinterpret_cast<float*>(base + lut_bytes + qf_bytes);
+    uint32_t* cand_i = reinterpret_cast<uint32_t*>(cand_s + nq * lists * ke);
+    cudaStream_t s = h->pick(stream);
+
+    vcb::QueryPrepArgs p{};
+    p.q = d_queries;
+    p.nq = static_cast<long long>(nq);
+    p.dim = static_cast<int>(h->dim);
+    p.bits = static_cast<int>(h->bits);
+    p.block = static_cast<int>(h->block);
+    p.nbg = static_cast<int>(h->nbg);
+    p.inv_sqrt_block = h->inv_sqrt_block;
+    p.perm_sign = h->d_perm_sign.as<uint32_t>();
+    p.centroids = h->d_cen.as<float>();
+    p.tqplus = h->calibrated;
+    p.shift = h->d_shift.as<float>();
+    p.scale = h->d_scale.as<float>();
+    p.luts = luts;
+    p.lut_scale = qf;
+    p.lut_bias = qf + nq;
+    p.bias_corr = qf + 2 * nq;
+    p.fa_init = qf + 3 * nq;
+    p.q_rot = nullptr;
+    p.replay_count = h->d_counter.as<unsigned long long>();
+    vcb::check(vcb::launch_query_prep(p, h->sms, s), "query prep kernel");
+
+    vcb::ScanArgs a{};
+    a.codes = h->d_codes.as<uint32_t>();
+    a.alpha = h->d_alpha.as<float>();
+    a.luts = luts;
+    a.lut_scale = qf;
+    a.fa_init = qf + 3 * nq;
+    a.n = static_cast<long long>(h->n);
+    a.nbg = static_cast<int>(h->nbg);
+    a.nq = static_cast<long long>(nq);
+    a.k = static_cast<int>(ke);
+    a.q_per_cta = plan.q_per_cta;
+    a.range_vectors = plan.range_vectors;
+    a.n_ranges = plan.n_ranges;
+    a.lut_chunk_groups = plan.lut_chunk_groups;
+    a.cand_score = cand_s;
+    a.cand_id = cand_i;
+    vcb::check(vcb::launch_scan(a, plan, s), "scan kernel");
+
+    vcb::MergeArgs m{};
+    m.cand_score = cand_s;
+    m.cand_id = cand_i;
+    m.nq = static_cast<long long>(nq);
+    m.n_lists = static_cast<int>(lists);
+    m.k = static_cast<int>(ke);
+    m.k_out = static_cast<int>(ke);
+    m.out_score = d_scores;
+    m.out_id = d_ids;
+    vcb::check(vcb::launch_merge(m, s), "merge kernel");
+  });
+}
