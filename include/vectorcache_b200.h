@@ -99,6 +99,45 @@ int tq_index_search_device(tq_index* h, const float* d_queries, size_t nq, size_
 /* Block until the index's queued work is done. */
 int tq_index_synchronize(tq_index* h);
 
+/* ---- persistence and file formats -------------------------------------------
+ * Index files: no counterpart in the reference, which keeps no index on disk.
+ * The file holds dim, bits, the TQ+ shift/scale, codes_flat, alpha and a
+ * checksum; tq_index_load returns a prepared index on `device`. */
+int tq_index_save(tq_index* h, const char* path);
+int tq_index_load(const char* path, int device, tq_index** out);
+
+/* Append the rows of a float32 C-order (rows, dim) .npy file, streamed in
+ * chunks. Replaces NpyReader (include/vectorcache/datasets/npy.hpp:33-61)
+ * feeding add(). */
+int tq_index_add_npy(tq_index* h, const char* path);
+
+/* .npy float32 matrices: NpyReader / write_npy_f32_matrix
+ * (include/vectorcache/datasets/npy.hpp:33-66). */
+int tq_npy_f32_info(const char* path, size_t* rows, size_t* cols);
+int tq_npy_f32_read(const char* path, size_t row0, size_t nrows, float* out);
+int tq_npy_f32_write(const char* path, size_t rows, size_t cols, const float* data);
+
+/* VCEX exact-top-k files (tools/query-bench.cpp:180-340): ground-truth ids
+ * nq x k with the index size, seed and three labels. */
+int tq_vcex_write(const char* path, const uint64_t* ids, size_t nq, size_t k, uint64_t index_n,
+                  uint64_t seed, const char* source_label, const char* split,
+                  const char* query_split);
+int tq_vcex_read_header(const char* path, size_t* nq, size_t* k, uint64_t* index_n,
+                        uint64_t* seed);
+int tq_vcex_read_ids(const char* path, uint64_t* ids);
+
+/* ---- exact float re-rank ---------------------------------------------------
+ * Re-scores each query's k candidates with the exact float inner product
+ * <query, corpus[id]> (the reference's AVX2 summation order) and re-sorts the
+ * row: score descending, equal scores by lower id; ids >= n_corpus score -inf.
+ * scores/ids are nq x k, rewritten in place. Replaces float_rescore_topk
+ * (src/search/float_rescore.cpp:80-164). k <= 4096. */
+int tq_rescore(const float* queries, size_t nq, size_t dim, const float* corpus, size_t n_corpus,
+               size_t k, float* scores, uint64_t* ids, int device);
+/* Device buffers, queued on `stream` (a cudaStream_t; NULL = legacy default). */
+int tq_rescore_device(const float* d_queries, size_t nq, size_t dim, const float* d_corpus,
+                      size_t n_corpus, size_t k, float* d_scores, uint64_t* d_ids, void* stream);
+
 /* ---- introspection (parity exports) --------------------------------------- */
 
 int tq_index_info(const tq_index* h, size_t* dim, size_t* bits, size_t* n, int* prepared,

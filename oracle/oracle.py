@@ -217,3 +217,24 @@ class ReferenceIndex:
 
     def __del__(self):
         self.close()
+
+
+def _float_rescore(lib, fn, queries, corpus, ids, scores_init=None):
+    q = np.ascontiguousarray(queries, np.float32)
+    c = np.ascontiguousarray(corpus, np.float32)
+    ids = np.ascontiguousarray(ids, np.uint64).copy()
+    nq, k = ids.shape
+    s = np.zeros((nq, k), np.float32)
+    rc = getattr(lib, fn)(_p(q), _SZ(nq), _SZ(q.shape[1]), _p(c), _SZ(c.shape[0]), _SZ(k), _p(s), _p(ids))
+    assert rc in (0, None)
+    return s, ids
+
+
+def oracle_float_rescore(orc: "Oracle", queries, corpus, ids):
+    """Exact float re-rank of candidate ids (the C restatement)."""
+    return _float_rescore(orc.lib, "tqo_float_rescore", queries, corpus, ids)
+
+
+def reference_float_rescore(ref: "Reference", queries, corpus, ids):
+    """The reference's own float_rescore_topk on the same candidate ids."""
+    return _float_rescore(ref.lib, "tqref_float_rescore", queries, corpus, ids)

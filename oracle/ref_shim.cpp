@@ -32,6 +32,7 @@
 #include "vectorcache/encode/encode.hpp"
 #include "vectorcache/pack/pack.hpp"
 #include "vectorcache/quantize/codebook.hpp"
+#include "vectorcache/search/float_rescore.hpp"
 #include "vectorcache/search/search.hpp"
 #include "vectorcache/transform/rotation.hpp"
 
@@ -207,6 +208,24 @@ int tqref_prepare_queries(const float* q, std::size_t nq, std::size_t dim, std::
       lut_scale[i] = prep.luts[i].scale;
       lut_bias[i] = prep.luts[i].bias;
     }
+  });
+}
+
+// Exact float re-rank of given top-k ids (float_rescore_topk,
+// src/search/float_rescore.cpp:80-164); scores/ids are nq x k, in place.
+int tqref_float_rescore(const float* q, std::size_t nq, std::size_t dim, const float* corpus,
+                        std::size_t n_corpus, std::size_t k, float* scores, std::uint64_t* ids) {
+  return guarded([&] {
+    vectorcache::SearchResults res;
+    res.nq = nq;
+    res.k = k;
+    res.scores.assign(nq * k, 0.f);
+    res.ids.resize_uninitialized(nq * k);
+    std::memcpy(res.ids.data(), ids, nq * k * sizeof(std::uint64_t));
+    vectorcache::float_rescore_topk(res, std::span<const float>(q, nq * dim),
+                                    std::span<const float>(corpus, n_corpus * dim), dim);
+    std::memcpy(scores, res.scores.data(), nq * k * sizeof(float));
+    std::memcpy(ids, res.ids.data(), nq * k * sizeof(std::uint64_t));
   });
 }
 

@@ -655,3 +655,53 @@ size_t tqo_search_flat(const float* q, size_t nq, size_t dim, size_t bits, const
   free(sc);
   return ke;
 }
+
+/* ----------------------------------------------------------------------------
+ * Exact float re-rank (float_rescore.cpp:23-58 dot product, :80-164 driver).
+ * The dot product: 16 fused multiply-add chains over the first dim - dim % 16
+ * elements (element i feeds chain i % 16), chains 8..15 added lane-wise into
+ * 0..7, an 8-element tail into chains 0..7 when dim % 16 == 8, then
+ * ((c0+c4)+(c1+c5))+((c2+c6)+(c3+c7)).
+ * ------------------------------------------------------------------------- */
+static float dot_avx2_order(const float* a, const float* b, size_t dim) {
+  float c[16] = {0};
+  const size_t main_end = dim - dim % 16;
+  for (size_t i = 0; i < main_end; ++i) c[i % 16] = fmaf(a[i], b[i], c[i % 16]);
+  for (int l = 0; l < 8; ++l) c[l] = c[l] + c[l + 8];
+  if (dim % 16 == 8) {
+    for (int l = 0; l < 8; ++l) c[l] = fmaf(a[main_end + (size_t)l], b[main_end + (size_t)l], c[l]);
+  }
+  const float b0 = c[0] + c[4], b1 = c[1] + c[5], b2 = c[2] + c[6], b3 = c[3] + c[7];
+  return (b0 + b1) + (b2 + b3);
+}
+
+void tqo_float_rescore(const float* queries, size_t nq, size_t dim, const float* corpus,
+                       size_t n_corpus, size_t k, float* scores, uint64_t* ids) {
+#pragma omp parallel
+  {
+    cand_t* row = malloc((k ? k : 1) * sizeof(cand_t));
+#pragma omp for schedule(static)
+    for (long long qq = 0; qq < (long long)nq; ++qq) {
+      const size_t qi = (size_t)qq;
+      for (size_t j = 0; j < k; ++j) {
+        const uint64_t id = ids[qi * k + j];
+        row[j].id = id;
+        row[j].s = (id < n_corpus) ? dot_avx2_order(queries + qi * dim, corpus + id * dim, dim) : -INFINITY;
+      }
+      for (size_t j = 1; j < k; ++j) {  /* insertion sort, best first */
+        cand_t c = row[j];
+        size_t p = j;
+        while (p > 0 && better(&c, &row[p - 1])) {
+          row[p] = row[p - 1];
+          --p;
+        }
+        row[p] = c;
+      }
+      for (size_t j = 0; j < k; ++j) {
+        scores[qi * k + j] = row[j].s;
+        ids[qi * k + j] = row[j].id;
+      }
+    }
+    free(row);
+  }
+}

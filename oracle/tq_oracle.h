@@ -66,6 +66,12 @@ size_t tqo_search_flat(const float* q, size_t nq, size_t dim, size_t bits, const
                        const float* scale, const uint8_t* packed, const float* alpha, size_t n,
                        size_t k, float* out_scores, uint64_t* out_ids);
 
+/* Exact float re-rank in place: scores[q][j] = <q, corpus[ids[q][j]]> in the
+ * reference's AVX2 summation order, rows re-sorted (score desc, id asc);
+ * ids >= n_corpus score -inf. */
+void tqo_float_rescore(const float* queries, size_t nq, size_t dim, const float* corpus,
+                       size_t n_corpus, size_t k, float* scores, uint64_t* ids);
+
 #ifdef __cplusplus
 }
 #endif

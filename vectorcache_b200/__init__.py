@@ -96,6 +96,19 @@ def _declare(lib):
         "tq_index_prepare_queries": (C.c_int, [_P, _P, _SZ, _P, _P, _P, _P, _P]),
         "tq_index_dense_scores": (C.c_int, [_P, _P, _SZ, _P, _P]),
         "tq_index_replay_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+        "tq_index_save": (C.c_int, [_P, C.c_char_p]),
+        "tq_index_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
+        "tq_index_add_npy": (C.c_int, [_P, C.c_char_p]),
+        "tq_npy_f32_info": (C.c_int, [C.c_char_p, C.POINTER(_SZ), C.POINTER(_SZ)]),
+        "tq_npy_f32_read": (C.c_int, [C.c_char_p, _SZ, _SZ, _P]),
+        "tq_npy_f32_write": (C.c_int, [C.c_char_p, _SZ, _SZ, _P]),
+        "tq_vcex_write": (C.c_int, [C.c_char_p, _P, _SZ, _SZ, C.c_uint64, C.c_uint64, C.c_char_p, C.c_char_p,
+                                    C.c_char_p]),
+        "tq_vcex_read_header": (C.c_int, [C.c_char_p, C.POINTER(_SZ), C.POINTER(_SZ), C.POINTER(C.c_uint64),
+                                          C.POINTER(C.c_uint64)]),
+        "tq_vcex_read_ids": (C.c_int, [C.c_char_p, _P]),
+        "tq_rescore": (C.c_int, [_P, _SZ, _SZ, _P, _SZ, _SZ, _P, _P, C.c_int]),
+        "tq_rescore_device": (C.c_int, [_P, _SZ, _SZ, _P, _SZ, _SZ, _P, _P, _P]),
         "tq_index_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
         "tq_index_set_profiling": (C.c_int, [_P, C.c_int]),
         "tq_index_read_profile": (C.c_int, [_P, C.POINTER(Profile)]),
@@ -164,6 +177,22 @@ def rotation_tables(dim: int) -> tuple[np.ndarray, np.ndarray]:
     return s, p
 
 
+def rescore(queries, corpus, results: "SearchResults", device: int = 0) -> "SearchResults":
+    """Exact float inner-product re-rank of a top-k (float_rescore_topk,
+    src/search/float_rescore.cpp:80-164): each candidate is re-scored as
+    <query, corpus[id]> and every row re-sorted (score desc, id asc)."""
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    c = np.ascontiguousarray(corpus, dtype=np.float32)
+    dim = q.shape[1]
+    if c.ndim != 2 or c.shape[1] != dim:
+        raise InvalidArgument(TQ_ERR_INVALID_ARGUMENT, "corpus must be [n, dim] float32")
+    scores = np.ascontiguousarray(results.scores, dtype=np.float32).copy()
+    ids = np.ascontiguousarray(results.ids, dtype=np.uint64).copy()
+    nq, k = ids.shape
+    _check(load_library().tq_rescore(_ptr(q), nq, dim, _ptr(c), c.shape[0], k, _ptr(scores), _ptr(ids), device))
+    return SearchResults(scores, ids)
+
+
 @dataclass
 class SearchResults:
     """Row-major top-k, like vectorcache::SearchResults (search.hpp:77-84)."""
@@ -196,16 +225,35 @@ class TurboQuantIndex:
     search() after prepare(); k_eff = min(k, size).
     """
 
-    def __init__(self, dim: int, bits: int, device: int = 0):
+    def __init__(self, dim: int, bits: int, device: int = 0, _handle=None):
         lib = load_library()
-        h = _P()
-        _check(lib.tq_index_create(dim, bits, 0, device, C.byref(h)))
+        h = _handle
+        if h is None:
+            h = _P()
+            _check(lib.tq_index_create(dim, bits, 0, device, C.byref(h)))
         self._h = h
         self._lib = lib
         self.dim = int(dim)
         self.bits = int(bits)
         self.device = int(device)
         self.n_byte_groups = self.dim // (8 // self.bits)
+
+    @classmethod
+    def load(cls, path, device: int = 0) -> "TurboQuantIndex":
+        """Open an index written by save(); it comes back prepared."""
+        lib = load_library()
+        h = _P()
+        _check(lib.tq_index_load(str(path).encode(), device, C.byref(h)))
+        d, b = _SZ(), _SZ()
+        _check(lib.tq_index_info(h, C.byref(d), C.byref(b), None, None, None))
+        return cls(d.value, b.value, device, _handle=h)
+
+    def save(self, path) -> None:
+        _check(self._lib.tq_index_save(self._h, str(path).encode()))
+
+    def add_npy(self, path) -> None:
+        """Append the rows of a float32 (rows, dim) .npy file."""
+        _check(self._lib.tq_index_add_npy(self._h, str(path).encode()))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -19,46 +19,20 @@
 #include <vector>
 
 #include "../../include/vectorcache_b200.h"
+#include "tq_abi.h"
 #include "tq_host_math.h"
 #include "tq_kernels.h"
 
 namespace vcb {
-namespace {
 
 thread_local std::string g_last_error;
 
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
+namespace {
 
 void check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;
   const int code = (e == cudaErrorMemoryAllocation) ? TQ_ERR_OUT_OF_MEMORY : TQ_ERR_CUDA;
   throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-[[noreturn]] void fail(int code, const std::string& msg) { throw Error(code, msg); }
-
-template <typename F>
-int guarded(F&& f) {
-  try {
-    f();
-    g_last_error.clear();
-    return TQ_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return TQ_ERR_OUT_OF_MEMORY;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return TQ_ERR_INVALID_ARGUMENT;
-  } catch (...) {
-    g_last_error = "unknown error";
-    return TQ_ERR_CUDA;
-  }
 }
 
 // Grow-only device allocation.
@@ -308,7 +282,7 @@ struct tq_index {
                           static_cast<int>(k_eff), sms, &plan)) {
         vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
       }
-      const size_t lists = static_cast<size_t>(plan.n_ranges) * 8;
+      const size_t lists = static_cast<size_t>(plan.n_ranges) * plan.lists_per_range;
       d_cand_s.reserve(m * lists * k_eff * 4);
       d_cand_i.reserve(m * lists * k_eff * 4);
       const float* qf = d_qf.as<float>();
@@ -349,9 +323,7 @@ struct tq_index {
 
 namespace {
 
-void require(bool ok, int code, const char* msg) {
-  if (!ok) vcb::fail(code, msg);
-}
+using vcb::require;
 
 void check_aligned(const void* p, const char* what) {
   if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
@@ -871,15 +843,16 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     }
     // Fewer vector ranges if their candidate lists would not fit.
     const size_t max_lists = (kNoAllocScratchBytes - lut_bytes - qf_bytes) / per_list;
-    if (static_cast<size_t>(plan.n_ranges) * 8 > max_lists) {
+    const size_t per_range = static_cast<size_t>(plan.lists_per_range);
+    if (static_cast<size_t>(plan.n_ranges) * per_range > max_lists) {
       const long long blocks = (static_cast<long long>(h->n) + vcb::kScanBlockVectors - 1) / vcb::kScanBlockVectors;
-      long long ranges = static_cast<long long>(max_lists / 8);
-      const long long per_range = (blocks + ranges - 1) / ranges;
-      ranges = (blocks + per_range - 1) / per_range;
+      long long ranges = static_cast<long long>(max_lists / per_range);
+      const long long blocks_each = (blocks + ranges - 1) / ranges;
+      ranges = (blocks + blocks_each - 1) / blocks_each;
       plan.n_ranges = static_cast<int>(ranges);
-      plan.range_vectors = per_range * vcb::kScanBlockVectors;
+      plan.range_vectors = blocks_each * vcb::kScanBlockVectors;
     }
-    const size_t lists = static_cast<size_t>(plan.n_ranges) * 8;
+    const size_t lists = static_cast<size_t>(plan.n_ranges) * per_range;
 
     vcb::DeviceGuard g(h->device);
     unsigned char* base = noalloc_scratch(h->device);
@@ -939,5 +912,225 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     m.out_score = d_scores;
     m.out_id = d_ids;
     vcb::check(vcb::launch_merge(m, s), "merge kernel");
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Index persistence (the reference has none). File layout, little-endian:
+//   "VCBTQIX1", u32 version = 1, u32 dim, u32 bits, u32 flags (bit 0: TQ+),
+//   u64 n, [f32 shift[dim], f32 scale[dim] when TQ+], u8 codes_flat[n * nbg],
+//   f32 alpha[n], u64 FNV-1a of every byte after the magic.
+namespace {
+
+constexpr char kIndexMagic[8] = {'V', 'C', 'B', 'T', 'Q', 'I', 'X', '1'};
+
+struct Fnv1a {
+  uint64_t h = 1469598103934665603ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  }
+};
+
+}  // namespace
+
+extern "C" int tq_index_save(tq_index* h, const char* path) {
+  return vcb::guarded([&] {
+    require(h && path, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(h->prepared, TQ_ERR_STATE, "save before prepare");
+    std::vector<uint8_t> flat(h->n * h->nbg);
+    std::vector<float> alpha(h->n);
+    if (h->n) {
+      int rc = tq_index_export_codes_flat(h, flat.data());
+      if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+      rc = tq_index_export_alpha(h, alpha.data());
+      if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+    }
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    require(f != nullptr, TQ_ERR_INVALID_ARGUMENT, "cannot create index file");
+    Fnv1a sum;
+    bool ok = std::fwrite(kIndexMagic, 1, 8, f) == 8;
+    auto put = [&](const void* p, size_t n) {
+      if (n == 0 || !ok) return;
+      ok = std::fwrite(p, 1, n, f) == n;
+      sum.add(p, n);
+    };
+    const uint32_t hdr[4] = {1u, static_cast<uint32_t>(h->dim), static_cast<uint32_t>(h->bits),
+                             h->calibrated ? 1u : 0u};
+    const uint64_t n64 = h->n;
+    put(hdr, sizeof(hdr));
+    put(&n64, sizeof(n64));
+    if (h->calibrated) {
+      put(h->shift.data(), h->dim * 4);
+      put(h->scale.data(), h->dim * 4);
+    }
+    put(flat.data(), flat.size());
+    put(alpha.data(), alpha.size() * 4);
+    if (ok) ok = std::fwrite(&sum.h, 1, 8, f) == 8;
+    ok = (std::fclose(f) == 0) && ok;
+    require(ok, TQ_ERR_INVALID_ARGUMENT, "write failed");
+    require(std::rename(tmp.c_str(), path) == 0, TQ_ERR_INVALID_ARGUMENT, "rename failed");
+  });
+}
+
+extern "C" int tq_index_load(const char* path, int device, tq_index** out) {
+  return vcb::guarded([&] {
+    require(path && out, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    require(f != nullptr, TQ_ERR_INVALID_ARGUMENT, "cannot open index file");
+    struct Closer {
+      FILE* f;
+      ~Closer() { std::fclose(f); }
+    } closer{f};
+    Fnv1a sum;
+    auto get = [&](void* p, size_t n) {
+      if (n == 0) return;
+      require(std::fread(p, 1, n, f) == n, TQ_ERR_INVALID_ARGUMENT, "truncated index file");
+      sum.add(p, n);
+    };
+    char magic[8];
+    require(std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kIndexMagic, 8) == 0, TQ_ERR_INVALID_ARGUMENT,
+            "not a vectorcache_b200 index file");
+    uint32_t hdr[4];
+    uint64_t n64 = 0;
+    get(hdr, sizeof(hdr));
+    require(hdr[0] == 1u, TQ_ERR_INVALID_ARGUMENT, "unsupported index file version");
+    get(&n64, sizeof(n64));
+    const size_t dim = hdr[1], bits = hdr[2];
+    require(vcb::dim_supported(dim) && vcb::bits_supported(bits), TQ_ERR_INVALID_ARGUMENT, "corrupt index header");
+    const size_t nbg = vcb::byte_groups(bits, dim);
+    std::vector<float> shift, scale;
+    if (hdr[3] & 1u) {
+      shift.resize(dim);
+      scale.resize(dim);
+      get(shift.data(), dim * 4);
+      get(scale.data(), dim * 4);
+    }
+    std::vector<uint8_t> flat(static_cast<size_t>(n64) * nbg);
+    std::vector<float> alpha(static_cast<size_t>(n64));
+    get(flat.data(), flat.size());
+    get(alpha.data(), alpha.size() * 4);
+    uint64_t stored = 0;
+    require(std::fread(&stored, 1, 8, f) == 8, TQ_ERR_INVALID_ARGUMENT, "truncated index file");
+    require(stored == sum.h, TQ_ERR_INVALID_ARGUMENT, "index file checksum mismatch");
+
+    tq_index* raw = nullptr;
+    int rc = tq_index_create(dim, bits, 0, device, &raw);
+    if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+    std::unique_ptr<tq_index, int (*)(tq_index*)> h(raw, tq_index_destroy);
+    vcb::DeviceGuard g(device);
+    if (!shift.empty()) {
+      h->shift = shift;
+      h->scale = scale;
+      std::vector<float> inv(dim);
+      for (size_t d = 0; d < dim; ++d) inv[d] = 1.f / scale[d];
+      h->d_shift.reserve(dim * 4);
+      h->d_scale.reserve(dim * 4);
+      h->d_inv_scale.reserve(dim * 4);
+      h->upload(h->d_shift.get(), shift.data(), dim * 4);
+      h->upload(h->d_scale.get(), scale.data(), dim * 4);
+      h->upload(h->d_inv_scale.get(), inv.data(), dim * 4);
+      h->calibrated = true;
+    }
+    const size_t n = static_cast<size_t>(n64);
+    if (n > 0) {
+      h->ensure_capacity(n);
+      const size_t stride = h->flat_stride();
+      std::vector<uint8_t> padded(n * stride, 0);
+      for (size_t v = 0; v < n; ++v) std::memcpy(padded.data() + v * stride, flat.data() + v * nbg, nbg);
+      h->d_flat.reserve(padded.size());
+      h->upload(h->d_flat.get(), padded.data(), padded.size());
+      h->upload(h->d_alpha.get(), alpha.data(), n * 4);
+      vcb::RelayoutArgs r{};
+      r.flat = h->d_flat.as<uint8_t>();
+      r.src_first = 0;
+      r.src_n = static_cast<long long>(n);
+      r.flat_stride = static_cast<int>(stride);
+      r.keep_below = 0;
+      r.n_total = static_cast<long long>(n);
+      r.nbg = static_cast<int>(nbg);
+      r.bits = static_cast<int>(bits);
+      r.codes = h->d_codes.as<uint32_t>();
+      vcb::check(vcb::launch_relayout(r, h->stream), "relayout kernel");
+      h->sync();
+      h->d_flat.release();
+      h->n = n;
+    }
+    h->prepared = true;
+    *out = h.release();
+  });
+}
+
+// Append the rows of a float32 .npy matrix (rows, dim), streamed in chunks
+// (the reference's NpyReader::copy_rows_into, src/datasets/npy.cpp).
+extern "C" int tq_npy_f32_info(const char* path, size_t* rows, size_t* cols);
+extern "C" int tq_npy_f32_read(const char* path, size_t row0, size_t nrows, float* out);
+
+extern "C" int tq_index_add_npy(tq_index* h, const char* path) {
+  return vcb::guarded([&] {
+    require(h && path, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    size_t rows = 0, cols = 0;
+    int rc = tq_npy_f32_info(path, &rows, &cols);
+    if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+    require(cols == h->dim, TQ_ERR_INVALID_ARGUMENT, ".npy column count differs from the index dim");
+    const size_t chunk = std::max<size_t>(1, (size_t{256} << 20) / (cols * 4));
+    std::vector<float> buf(std::min(rows, chunk) * cols);
+    for (size_t r0 = 0; r0 < rows; r0 += chunk) {
+      const size_t m = std::min(chunk, rows - r0);
+      rc = tq_npy_f32_read(path, r0, m, buf.data());
+      if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+      rc = tq_index_add(h, buf.data(), m);
+      if (rc != TQ_OK) vcb::fail(rc, vcb::g_last_error);
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Exact float re-rank of a top-k (float_rescore_topk, src/search/float_rescore.cpp:80-164).
+extern "C" int tq_rescore_device(const float* d_queries, size_t nq, size_t dim, const float* d_corpus,
+                                 size_t n_corpus, size_t k, float* d_scores, uint64_t* d_ids, void* stream) {
+  return vcb::guarded([&] {
+    if (nq == 0 || k == 0 || dim == 0) return;
+    require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(n_corpus == 0 || d_corpus != nullptr, TQ_ERR_INVALID_ARGUMENT, "null corpus");
+    require(k <= 4096, TQ_ERR_UNSUPPORTED, "rescore k must be <= 4096");
+    vcb::check(vcb::launch_rescore(d_queries, static_cast<long long>(nq), static_cast<int>(dim), d_corpus,
+                                   static_cast<long long>(n_corpus), static_cast<int>(k), d_scores, d_ids,
+                                   static_cast<cudaStream_t>(stream)),
+               "rescore kernel");
+  });
+}
+
+extern "C" int tq_rescore(const float* queries, size_t nq, size_t dim, const float* corpus, size_t n_corpus,
+                          size_t k, float* scores, uint64_t* ids, int device) {
+  return vcb::guarded([&] {
+    if (nq == 0 || k == 0 || dim == 0) return;
+    require(queries && scores && ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(n_corpus == 0 || corpus != nullptr, TQ_ERR_INVALID_ARGUMENT, "null corpus");
+    require(k <= 4096, TQ_ERR_UNSUPPORTED, "rescore k must be <= 4096");
+    vcb::DeviceGuard g(device);
+    cudaStream_t s = nullptr;
+    vcb::check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    struct StreamGuard {
+      cudaStream_t s;
+      ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{s};
+    vcb::DeviceBuffer dq, dc, ds, di;
+    dq.reserve(nq * dim * 4);
+    dc.reserve(std::max<size_t>(n_corpus, 1) * dim * 4);
+    ds.reserve(nq * k * 4);
+    di.reserve(nq * k * 8);
+    vcb::check(cudaMemcpyAsync(dq.get(), queries, nq * dim * 4, cudaMemcpyHostToDevice, s), "H2D");
+    if (n_corpus) vcb::check(cudaMemcpyAsync(dc.get(), corpus, n_corpus * dim * 4, cudaMemcpyHostToDevice, s), "H2D");
+    vcb::check(cudaMemcpyAsync(di.get(), ids, nq * k * 8, cudaMemcpyHostToDevice, s), "H2D");
+    vcb::check(vcb::launch_rescore(dq.as<float>(), static_cast<long long>(nq), static_cast<int>(dim), dc.as<float>(),
+                                   static_cast<long long>(n_corpus), static_cast<int>(k), ds.as<float>(),
+                                   di.as<uint64_t>(), s),
+               "rescore kernel");
+    vcb::check(cudaMemcpyAsync(scores, ds.get(), nq * k * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    vcb::check(cudaMemcpyAsync(ids, di.get(), nq * k * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   });
 }

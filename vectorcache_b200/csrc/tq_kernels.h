@@ -132,6 +132,7 @@ struct ScanPlan {
   int n_ranges = 1;
   int lut_chunk_groups = 0;
   size_t smem_bytes = 0;
+  int lists_per_range = 1;  // candidate lists each (query, range) publishes
 };
 bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan);
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);
@@ -145,5 +146,9 @@ cudaError_t launch_dense_scores(const uint32_t* codes, const float* alpha, const
                                 cudaStream_t stream);
 
 constexpr int kMaxK = 256;
+
+// Exact float re-rank of nq rows of k (score, id) in place (tq_rescore.cu).
+cudaError_t launch_rescore(const float* queries, long long nq, int dim, const float* corpus, long long n_corpus,
+                           int k, float* scores, uint64_t* ids, cudaStream_t stream);
 
 }  // namespace vcb

@@ -3,6 +3,11 @@
 //
 // Follows the reference's prepare_queries / build_query_lut
 // (src/search/search.cpp:149-219, :762-860) bit for bit.
+//
+// One CTA of 4 warps prepares 4 queries: the rows are staged in shared memory,
+// warp 0 runs the 8 sequential norm chains of all 4 rows, warp w rotates query
+// w in registers, and then all 128 threads build the 4 queries' LUTs together
+// (so a single query still gets the whole CTA for its byte groups).
 #include <cfloat>
 
 #include "tq_kernels.h"
@@ -11,20 +16,59 @@
 namespace vcb {
 namespace {
 
-constexpr int kPrepWarps = 4;
+constexpr int kPrepWarps = 4;  // = queries per CTA
+constexpr int kPrepThreads = kPrepWarps * 32;
 
-template <int R>
-__global__ void __launch_bounds__(kPrepWarps * 32) query_prep_kernel(QueryPrepArgs a) {
+// The 16 entries of one LUT half: entry nv = sum over the cpn codes packed in
+// nibble value nv (first code in the high bits) of q[c] * centroid[code], each
+// step one fused multiply-add from 0 (search.cpp:159-173). Fully unrolled so
+// the entries stay in registers.
+template <int BITS>
+__device__ __forceinline__ void lut_half(const float* __restrict__ qd, const float* __restrict__ cen,
+                                         float (&v)[16]) {
+  if constexpr (BITS == 2) {
+    const float q0 = qd[0], q1 = qd[1];
+#pragma unroll
+    for (int nv = 0; nv < 16; ++nv) {
+      v[nv] = __fmaf_rn(q1, cen[nv & 3], __fmaf_rn(q0, cen[(nv >> 2) & 3], 0.f));
+    }
+  } else {
+    const float q0 = qd[0];
+#pragma unroll
+    for (int nv = 0; nv < 16; ++nv) v[nv] = __fmaf_rn(q0, cen[nv & ((1 << BITS) - 1)], 0.f);
+  }
+}
+
+template <int BITS>
+__device__ __forceinline__ void half_min_max(const float (&v)[16], float* mn, float* mx) {
+  float lo = FLT_MAX, hi = -FLT_MAX;
+#pragma unroll
+  for (int nv = 0; nv < 16; ++nv) {
+    lo = (v[nv] < lo) ? v[nv] : lo;  // std::min / std::max semantics
+    hi = (hi < v[nv]) ? v[nv] : hi;
+  }
+  *mn = lo;
+  *mx = hi;
+}
+
+template <int R, int BITS>
+__global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int dim = a.dim, nbg = a.nbg;
+  constexpr int kCpb = 8 / BITS;      // codes per byte group
+  constexpr int kCpn = kCpb / 2;      // codes per nibble
   uint32_t* s_perm = reinterpret_cast<uint32_t*>(smem);
   float* s_shift = reinterpret_cast<float*>(s_perm + dim);
   float* s_scale = s_shift + (a.tqplus ? dim : 0);
-  float* s_cen = s_scale + (a.tqplus ? dim : 0);
-  float* s_rows = s_cen + 16;
+  float* s_rows = s_scale + (a.tqplus ? dim : 0);   // 4 x dim
+  float* s_gmin = s_rows + kPrepWarps * dim;         // 4 x nbg
+  __shared__ float s_cen[16];
+  __shared__ float s_norm[kPrepWarps];
+  __shared__ float s_bias_corr[kPrepWarps];
+  __shared__ unsigned s_span_bits[kPrepWarps];
+  __shared__ float s_inv[kPrepWarps];
+  __shared__ float s_lut_scale[kPrepWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* qrow = s_rows + static_cast<size_t>(warp) * (dim + 4 * nbg);
-  float* gmin = qrow + dim;  // 4 queries x nbg per-group (min_first + min_second)
 
   for (int i = threadIdx.x; i < dim; i += blockDim.x) {
     s_perm[i] = a.perm_sign[i];
@@ -34,40 +78,48 @@ __global__ void __launch_bounds__(kPrepWarps * 32) query_prep_kernel(QueryPrepAr
     }
   }
   if (threadIdx.x < 16) s_cen[threadIdx.x] = a.centroids[threadIdx.x];
-  __syncthreads();
 
-  const int cpb = 8 / a.bits;
-  const int cpn = cpb / 2;  // codes per nibble
-  const unsigned code_mask = (1u << a.bits) - 1u;
+  for (long long q0 = static_cast<long long>(blockIdx.x) * kPrepWarps; q0 < a.nq;
+       q0 += static_cast<long long>(gridDim.x) * kPrepWarps) {
+    const int nloc = static_cast<int>(min(static_cast<long long>(kPrepWarps), a.nq - q0));
+    __syncthreads();
+    // Stage the rows (coalesced 16-byte loads).
+    const int vec_per_row = dim / 4;
+    for (int t = threadIdx.x; t < nloc * vec_per_row; t += blockDim.x) {
+      const int r = t / vec_per_row, c = t % vec_per_row;
+      reinterpret_cast<float4*>(s_rows + r * dim)[c] =
+          __ldg(reinterpret_cast<const float4*>(a.q + (q0 + r) * static_cast<long long>(dim)) + c);
+    }
+    if (threadIdx.x < kPrepWarps) s_span_bits[threadIdx.x] = 0u;
+    __syncthreads();
 
-  const long long warps_total = static_cast<long long>(gridDim.x) * kPrepWarps;
-  for (long long quad = static_cast<long long>(blockIdx.x) * kPrepWarps + warp; quad * 4 < a.nq;
-       quad += warps_total) {
-    const long long q_lane = quad * 4 + (lane >> 3);
-    const bool lane_valid = q_lane < a.nq;
-    const float nrm_lane =
-        warp_norm4(a.q + (lane_valid ? q_lane : 0) * static_cast<long long>(dim), dim, lane_valid, lane);
-    float my_bias_corr = 0.f;   // lane j (< 4) keeps query j's values for the final step
-    float my_span = 0.f;
-
-    for (int j = 0; j < 4; ++j) {
-      const long long qi = quad * 4 + j;
-      const float nrm = __shfl_sync(full_mask(), nrm_lane, 8 * j);
-      if (qi >= a.nq) break;
-      const float* src = a.q + qi * static_cast<long long>(dim);
-      __syncwarp();
-      for (int i = lane * 4; i < dim; i += kWarp * 4) {
-        *reinterpret_cast<float4*>(qrow + i) = __ldg(reinterpret_cast<const float4*>(src + i));
+    // Norms: lane 8v + c of warp 0 runs chain c of row v (encode.cpp:16-26).
+    if (warp == 0) {
+      const int v = lane >> 3, c = lane & 7;
+      float s = 0.f;
+      if (v < nloc) {
+        const float* row = s_rows + v * dim;
+        for (int j = c; j < dim; j += 8) s = __fmaf_rn(row[j], row[j], s);
       }
-      __syncwarp();
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 1));
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 2));
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 4));
+      if (c == 0 && v < nloc) s_norm[v] = __fsqrt_rn(s);
+    }
+    __syncthreads();
+
+    // Rotation (and TQ+) of query `warp`, written back over its staged row.
+    if (warp < nloc) {
+      const long long qi = q0 + warp;
+      float* row = s_rows + warp * dim;
+      const float nrm = s_norm[warp];
       const float inv = (nrm > kMinInputNorm) ? __fdiv_rn(1.f, nrm) : 0.f;
       float y[R];
-      warp_rotate<R>(qrow, s_perm, dim, a.block, inv, a.inv_sqrt_block, y, lane);
-
+      warp_rotate<R>(row, s_perm, dim, a.block, inv, a.inv_sqrt_block, y, lane);
       float bias_corr = 0.f;
       if (a.tqplus) {
-        // bias_corr = -sum_d y_d * shift_d, accumulated sequentially in double by
-        // the reference (search.cpp:792-799); the products are exact in double.
+        // bias_corr = -sum_d y_d * shift_d, sequential in double in the
+        // reference (search.cpp:792-799); the products are exact in double.
         double est = 0.0, mag = 0.0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -86,14 +138,14 @@ __global__ void __launch_bounds__(kPrepWarps * 32) query_prep_kernel(QueryPrepAr
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int i = lane + kWarp * r;
-            if (i < dim) qrow[i] = y[r];
+            if (i < dim) row[i] = y[r];
           }
           __syncwarp();
           double bc = 0.0;
           if (lane == 0) {
 #pragma unroll 1
             for (int i = 0; i < dim; ++i) {
-              bc = __dsub_rn(bc, __dmul_rn(static_cast<double>(qrow[i]), static_cast<double>(s_shift[i])));
+              bc = __dsub_rn(bc, __dmul_rn(static_cast<double>(row[i]), static_cast<double>(s_shift[i])));
             }
           }
           bias_corr = __double2float_rn(__shfl_sync(full_mask(), bc, 0));
@@ -110,93 +162,95 @@ __global__ void __launch_bounds__(kPrepWarps * 32) query_prep_kernel(QueryPrepAr
       for (int r = 0; r < R; ++r) {
         const int i = lane + kWarp * r;
         if (i < dim) {
-          qrow[i] = y[r];
+          row[i] = y[r];
           if (a.q_rot) a.q_rot[qi * dim + i] = y[r];
         }
       }
-      __syncwarp();
+      if (lane == 0) s_bias_corr[warp] = bias_corr;
+    }
+    __syncthreads();
 
-      // Pass 1: per-group minima and the largest span (search.cpp:163-199).
-      float span = 0.f;
-      for (int g = lane; g < nbg; g += kWarp) {
-        const float* qd = qrow + g * cpb;
-        float mins[2];
-        for (int h = 0; h < 2; ++h) {
-          float mn = FLT_MAX, mx = -FLT_MAX;
-          for (unsigned nv = 0; nv < 16; ++nv) {
-            float s = 0.f;
-            for (int c = 0; c < cpn; ++c) {
-              const unsigned code = (nv >> ((cpn - 1 - c) * a.bits)) & code_mask;
-              s = __fmaf_rn(qd[h * cpn + c], s_cen[code], s);
-            }
-            mn = (s < mn) ? s : mn;  // std::min / std::max semantics
-            mx = (mx < s) ? s : mx;
-          }
-          mins[h] = mn;
-          const float d = __fsub_rn(mx, mn);
-          span = (span < d) ? d : span;
-        }
-        gmin[j * nbg + g] = __fadd_rn(mins[0], mins[1]);
+    // LUT pass 1: per-group minima and per-query largest span (search.cpp:163-199).
+    float span[kPrepWarps] = {0.f, 0.f, 0.f, 0.f};
+    for (int t = threadIdx.x; t < nloc * nbg; t += blockDim.x) {
+      const int r = t / nbg, g = t % nbg;
+      const float* qd = s_rows + r * dim + g * kCpb;
+      float v[16], mn0, mx0, mn1, mx1;
+      lut_half<BITS>(qd, s_cen, v);
+      half_min_max<BITS>(v, &mn0, &mx0);
+      lut_half<BITS>(qd + kCpn, s_cen, v);
+      half_min_max<BITS>(v, &mn1, &mx1);
+      const float d0 = __fsub_rn(mx0, mn0), d1 = __fsub_rn(mx1, mn1);
+      float sp = (0.f < d0) ? d0 : 0.f;
+      sp = (sp < d1) ? d1 : sp;
+#pragma unroll
+      for (int rr = 0; rr < kPrepWarps; ++rr) {
+        if (rr == r) span[rr] = (span[rr] < sp) ? sp : span[rr];
       }
-      span = warp_max_f(span);
-      float lut_scale = (span > 0.f) ? __fdiv_rn(span, 127.f) : 1.f;
-      float lut_inv = 1.f;
-      if (lut_scale >= FLT_MIN) {
-        lut_inv = __fdiv_rn(1.f, lut_scale);
+      s_gmin[r * nbg + g] = __fadd_rn(mn0, mn1);
+    }
+#pragma unroll
+    for (int rr = 0; rr < kPrepWarps; ++rr) {
+      const float m = warp_max_f(span[rr]);
+      // Spans are >= 0, so their IEEE bit patterns order like the values.
+      if (lane == 0 && rr < nloc) atomicMax(&s_span_bits[rr], __float_as_uint(m));
+    }
+    __syncthreads();
+    if (threadIdx.x < nloc) {
+      const float sp = __uint_as_float(s_span_bits[threadIdx.x]);
+      float scale = (sp > 0.f) ? __fdiv_rn(sp, 127.f) : 1.f;
+      float inv = 1.f;
+      if (scale >= FLT_MIN) {
+        inv = __fdiv_rn(1.f, scale);
       } else {
-        lut_scale = 1.f;
+        scale = 1.f;
       }
+      s_lut_scale[threadIdx.x] = scale;
+      s_inv[threadIdx.x] = inv;
+    }
+    __syncthreads();
 
-      // Pass 2: quantized LUT bytes, 32 per group: first half indexed by the
-      // high nibble, second half by the low nibble.
-      uint8_t* out = a.luts + qi * static_cast<long long>(nbg) * 32;
-      for (int g = lane; g < nbg; g += kWarp) {
-        const float* qd = qrow + g * cpb;
-        uint32_t words[8];
-        for (int h = 0; h < 2; ++h) {
-          float vals[16];
-          float mn = FLT_MAX;
-          for (unsigned nv = 0; nv < 16; ++nv) {
-            float s = 0.f;
-            for (int c = 0; c < cpn; ++c) {
-              const unsigned code = (nv >> ((cpn - 1 - c) * a.bits)) & code_mask;
-              s = __fmaf_rn(qd[h * cpn + c], s_cen[code], s);
-            }
-            vals[nv] = s;
-            mn = (s < mn) ? s : mn;
+    // LUT pass 2: quantized bytes, 32 per group (first half indexed by the
+    // high nibble, second half by the low nibble).
+    for (int t = threadIdx.x; t < nloc * nbg; t += blockDim.x) {
+      const int r = t / nbg, g = t % nbg;
+      const float* qd = s_rows + r * dim + g * kCpb;
+      const float inv = s_inv[r];
+      uint32_t words[8];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float v[16], mn, mx;
+        lut_half<BITS>(qd + h * kCpn, s_cen, v);
+        half_min_max<BITS>(v, &mn, &mx);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            float x = roundf(__fmul_rn(__fsub_rn(v[4 * w + b], mn), inv));
+            x = (x < 0.f) ? 0.f : ((127.f < x) ? 127.f : x);  // std::clamp
+            word |= static_cast<uint32_t>(x) << (8 * b);
           }
-          for (int w = 0; w < 4; ++w) {
-            uint32_t word = 0;
-            for (int b = 0; b < 4; ++b) {
-              float r = roundf(__fmul_rn(__fsub_rn(vals[4 * w + b], mn), lut_inv));
-              r = (r < 0.f) ? 0.f : ((127.f < r) ? 127.f : r);  // std::clamp
-              word |= static_cast<uint32_t>(r) << (8 * b);
-            }
-            words[4 * h + w] = word;
-          }
+          words[4 * h + w] = word;
         }
-        uint4* dst = reinterpret_cast<uint4*>(out + static_cast<long long>(g) * 32);
-        dst[0] = make_uint4(words[0], words[1], words[2], words[3]);
-        dst[1] = make_uint4(words[4], words[5], words[6], words[7]);
       }
-      if (lane == j) {
-        my_bias_corr = bias_corr;
-        my_span = lut_scale;
-      }
+      uint4* dst = reinterpret_cast<uint4*>(a.luts + ((q0 + r) * nbg + g) * 32LL);
+      dst[0] = make_uint4(words[0], words[1], words[2], words[3]);
+      dst[1] = make_uint4(words[4], words[5], words[6], words[7]);
     }
-    __syncwarp();
-    // The LUT bias is a sequential f32 sum over groups (search.cpp:196); lane j
-    // replays it for query j of this quad.
-    const long long qi = quad * 4 + lane;
-    if (lane < 4 && qi < a.nq) {
+    __syncthreads();
+
+    // The LUT bias is a sequential f32 sum over groups (search.cpp:196).
+    if (threadIdx.x < nloc) {
+      const int r = threadIdx.x;
       float bias = 0.f;
-      for (int g = 0; g < nbg; ++g) bias = __fadd_rn(bias, gmin[lane * nbg + g]);
-      a.lut_scale[qi] = my_span;
+      for (int g = 0; g < nbg; ++g) bias = __fadd_rn(bias, s_gmin[r * nbg + g]);
+      const long long qi = q0 + r;
+      a.lut_scale[qi] = s_lut_scale[r];
       a.lut_bias[qi] = bias;
-      a.bias_corr[qi] = my_bias_corr;
-      a.fa_init[qi] = __fadd_rn(bias, my_bias_corr);
+      a.bias_corr[qi] = s_bias_corr[r];
+      a.fa_init[qi] = __fadd_rn(bias, s_bias_corr[r]);
     }
-    __syncwarp();
   }
 }
 
@@ -209,27 +263,44 @@ int rows_template_q(int dim) {
   return -1;
 }
 
+template <int R, int BITS>
+cudaError_t launch_prep_t(const QueryPrepArgs& a, size_t smem, unsigned grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(query_prep_kernel<R, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  query_prep_kernel<R, BITS><<<grid, kPrepThreads, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int R>
+cudaError_t launch_prep_bits(const QueryPrepArgs& a, size_t smem, unsigned grid, cudaStream_t stream) {
+  switch (a.bits) {
+    case 2:
+      return launch_prep_t<R, 2>(a, smem, grid, stream);
+    case 3:
+      return launch_prep_t<R, 3>(a, smem, grid, stream);
+    case 4:
+      return launch_prep_t<R, 4>(a, smem, grid, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_query_prep(const QueryPrepArgs& a, int sms, cudaStream_t stream) {
   if (a.nq == 0) return cudaSuccess;
   if (a.dim > kRegisterRowMaxDim) return launch_query_prep_big(a, sms, stream);
   const int r = rows_template_q(a.dim);
-  const size_t smem = static_cast<size_t>(a.dim) * 4 * (a.tqplus ? 3 : 1) + 16 * 4 +
-                      static_cast<size_t>(kPrepWarps) * (a.dim + 4 * a.nbg) * 4;
-  const long long quads = (a.nq + 3) / 4;
-  long long grid = (quads + kPrepWarps - 1) / kPrepWarps;
+  const size_t smem = static_cast<size_t>(a.dim) * 4 * (a.tqplus ? 3 : 1) +
+                      static_cast<size_t>(kPrepWarps) * (a.dim + a.nbg) * 4;
+  long long grid = (a.nq + kPrepWarps - 1) / kPrepWarps;
   if (grid > static_cast<long long>(sms) * 16) grid = static_cast<long long>(sms) * 16;
+  const unsigned g = static_cast<unsigned>(grid);
   switch (r) {
-#define VCB_CASE(RR)                                                                          \
-  case RR: {                                                                                  \
-    cudaError_t e = cudaFuncSetAttribute(query_prep_kernel<RR>,                               \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,         \
-                                         static_cast<int>(smem));                             \
-    if (e != cudaSuccess) return e;                                                           \
-    query_prep_kernel<RR><<<static_cast<unsigned>(grid), kPrepWarps * 32, smem, stream>>>(a); \
-    return cudaGetLastError();                                                                \
-  }
+#define VCB_CASE(RR) \
+  case RR:           \
+    return launch_prep_bits<RR>(a, smem, g, stream);
     VCB_CASE(1) VCB_CASE(2) VCB_CASE(3) VCB_CASE(4) VCB_CASE(6) VCB_CASE(8) VCB_CASE(12)
     VCB_CASE(16) VCB_CASE(24) VCB_CASE(32) VCB_CASE(48) VCB_CASE(64)
 #undef VCB_CASE

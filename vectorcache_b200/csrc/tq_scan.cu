@@ -246,33 +246,61 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           const int gn = g + kPrefetch + u;
           ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
         }
+        // Byte groups in pairs (nbg and every 256-group batch are even): the
+        // second-half lookups of both groups add into one byte per vector
+        // (<= 2 * 127), the first-half lookups into another; one prmt
+        // interleaves the two bytes of each vector so a single dp4a adds both.
 #pragma unroll
-        for (int u = 0; u < kPrefetch; ++u) {
+        for (int u = 0; u < kPrefetch; u += 2) {
           if (g + u >= g_stop) break;
-          const uint32_t x0 = cur[u].x, x1 = cur[u].y;
-          const uint32_t t0 = x0 ^ 0x88888888u, t1 = x1 ^ 0x88888888u;
-          const uint32_t x0h = x0 >> 16, x1h = x1 >> 16, t0h = t0 >> 16, t1h = t1 >> 16;
+          const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
+          const uint32_t a0h = a0 >> 16, a1h = a1 >> 16, b0h = b0 >> 16, b1h = b1 >> 16;
+          uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
+          if constexpr (!NIBBLE8) {
+            ta0 = a0 ^ 0x88888888u;
+            ta1 = a1 ^ 0x88888888u;
+            tb0 = b0 ^ 0x88888888u;
+            tb1 = b1 ^ 0x88888888u;
+            ta0h = ta0 >> 16;
+            ta1h = ta1 >> 16;
+            tb0h = tb0 >> 16;
+            tb1h = tb1 >> 16;
+          }
           const LutHalf* lg = s_lut + (g + u - chunk_base) * 2;
 #pragma unroll
           for (int q = 0; q < Q; ++q) {
-            const LutHalf F = lg[q * chunk * 2];      // entries 0..15: high nibble
-            const LutHalf S = lg[q * chunk * 2 + 1];  // entries 16..31: low nibble
-            uint32_t s0, s1;
+            const LutHalf Fa = lg[q * chunk * 2];      // group g+u: entries 0..15 (high nibble)
+            const LutHalf Sa = lg[q * chunk * 2 + 1];  //            entries 16..31 (low nibble)
+            const LutHalf Fb = lg[q * chunk * 2 + 2];  // group g+u+1
+            const LutHalf Sb = lg[q * chunk * 2 + 3];
+            uint32_t lo0, hi0, lo1, hi1;
             if constexpr (NIBBLE8) {
               // 3-bit codes: every nibble is < 8, entries 8..15 are never used.
-              s0 = prmt(S.w[0], S.w[1], x0) + prmt(F.w[0], F.w[1], x0h);
-              s1 = prmt(S.w[0], S.w[1], x1) + prmt(F.w[0], F.w[1], x1h);
+              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sb.w[0], Sb.w[1], b0);
+              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fb.w[0], Fb.w[1], b0h);
+              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sb.w[0], Sb.w[1], b1);
+              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fb.w[0], Fb.w[1], b1h);
             } else {
-              s0 = prmt(S.w[0], S.w[1], x0) + prmt(S.w[2], S.w[3], t0) +
-                   prmt(F.w[0], F.w[1], x0h) + prmt(F.w[2], F.w[3], t0h);
-              s1 = prmt(S.w[0], S.w[1], x1) + prmt(S.w[2], S.w[3], t1) +
-                   prmt(F.w[0], F.w[1], x1h) + prmt(F.w[2], F.w[3], t1h);
+              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sa.w[2], Sa.w[3], ta0) +
+                    prmt(Sb.w[0], Sb.w[1], b0) + prmt(Sb.w[2], Sb.w[3], tb0);
+              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fa.w[2], Fa.w[3], ta0h) +
+                    prmt(Fb.w[0], Fb.w[1], b0h) + prmt(Fb.w[2], Fb.w[3], tb0h);
+              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sa.w[2], Sa.w[3], ta1) +
+                    prmt(Sb.w[0], Sb.w[1], b1) + prmt(Sb.w[2], Sb.w[3], tb1);
+              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fa.w[2], Fa.w[3], ta1h) +
+                    prmt(Fb.w[0], Fb.w[1], b1h) + prmt(Fb.w[2], Fb.w[3], tb1h);
             }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              acc[q][j] = __dp4a(s0, 1u << (8 * j), acc[q][j]);
-              acc[q][4 + j] = __dp4a(s1, 1u << (8 * j), acc[q][4 + j]);
-            }
+            // [lo.b0, hi.b0, lo.b1, hi.b1] and [lo.b2, hi.b2, lo.b3, hi.b3]
+            const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
+            const uint32_t m10 = prmt(lo1, hi1, 0x5140u), m11 = prmt(lo1, hi1, 0x7362u);
+            acc[q][0] = __dp4a(m00, 0x00000101u, acc[q][0]);
+            acc[q][1] = __dp4a(m00, 0x01010000u, acc[q][1]);
+            acc[q][2] = __dp4a(m01, 0x00000101u, acc[q][2]);
+            acc[q][3] = __dp4a(m01, 0x01010000u, acc[q][3]);
+            acc[q][4] = __dp4a(m10, 0x00000101u, acc[q][4]);
+            acc[q][5] = __dp4a(m10, 0x01010000u, acc[q][5]);
+            acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
+            acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
           }
         }
       }
@@ -369,20 +397,39 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
     }
   }
 
-  // Each warp publishes its sorted list per query; the merge kernel combines
-  // the n_ranges * 8 lists of a query.
+  if constexpr (kReg) {
+    // The CTA merges its 8 warp lists of each query in shared memory (the LUT
+    // area is free now) and publishes one list per (query, range).
+    __syncthreads();
+    float* m_s = reinterpret_cast<float*>(smem);  // [Q][8 warps x 32]
+    uint32_t* m_i = reinterpret_cast<uint32_t*>(m_s + Q * kScanWarps * kWarp);
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    if (q0 + q >= a.nq) break;
-    const long long list = ((q0 + q) * a.n_ranges + range) * kScanWarps + warp;
-    float* os = a.cand_score + list * k;
-    uint32_t* oi = a.cand_id + list * k;
-    if constexpr (kReg) {
+    for (int q = 0; q < Q; ++q) {
+      const int slot = (q * kScanWarps + warp) * kWarp + lane;
+      m_s[slot] = lane < k ? top[q].s : -INFINITY;
+      m_i[slot] = lane < k ? top[q].i : 0xffffffffu;
+    }
+    __syncthreads();
+    for (int q = warp; q < Q; q += kScanWarps) {
+      if (q0 + q >= a.nq) break;
+      float* qs = m_s + q * kScanWarps * kWarp;
+      uint32_t* qi = m_i + q * kScanWarps * kWarp;
+      warp_sort_best_first(qs, qi, kScanWarps * kWarp, lane);
+      const long long list = (q0 + q) * a.n_ranges + range;
       if (lane < k) {
-        os[lane] = top[q].s;
-        oi[lane] = top[q].i;
+        a.cand_score[list * k + lane] = qs[lane];
+        a.cand_id[list * k + lane] = qi[lane];
       }
-    } else {
+    }
+  } else {
+    // Shared-memory lists (k > 32): each warp publishes its own sorted list;
+    // the merge kernel combines the n_ranges * 8 lists of a query.
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if (q0 + q >= a.nq) break;
+      const long long list = ((q0 + q) * a.n_ranges + range) * kScanWarps + warp;
+      float* os = a.cand_score + list * k;
+      uint32_t* oi = a.cand_id + list * k;
       for (int t = lane; t < k; t += kWarp) {
         const bool have = t < cnt[q];
         os[t] = have ? list_s[q * KMAX + t] : -INFINITY;
@@ -566,6 +613,11 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
   plan->n_ranges = static_cast<int>(ranges);
   plan->lut_chunk_groups = chunk;
   plan->smem_bytes = static_cast<size_t>(q) * chunk * 32 + warp_total;
+  if (reg) {
+    // the end-of-range merge of the 8 warp lists reuses the LUT area
+    plan->smem_bytes = std::max(plan->smem_bytes, static_cast<size_t>(q) * kScanWarps * kWarp * 8);
+  }
+  plan->lists_per_range = reg ? 1 : kScanWarps;
   return true;
 }
 
