@@ -600,10 +600,26 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
   }
   const long long blocks = (n + kScanBlockVectors - 1) / kScanBlockVectors;
   const long long qgroups = (nq + q - 1) / q;
+  const long long resident = static_cast<long long>(sms) * (reg ? 2 : 1);  // CTAs per wave
   const long long target = static_cast<long long>(sms) * (reg ? 8 : 4);
-  long long ranges = (target + qgroups - 1) / qgroups;
-  if (ranges < 1) ranges = 1;
-  if (ranges > blocks) ranges = blocks;
+  long long base = (target + qgroups - 1) / qgroups;
+  if (base < 1) base = 1;
+  // Among up to 4x the minimum range count, take the one whose last wave of
+  // CTAs is fullest (fewer idle SMs at the tail); ties keep fewer ranges.
+  long long ranges = base, best_waste = -1;
+  for (long long r = base; r <= base * 4; ++r) {
+    long long rr = r > blocks ? blocks : r;
+    const long long per = (blocks + rr - 1) / rr;
+    rr = (blocks + per - 1) / per;
+    const long long ctas = qgroups * rr;
+    const long long waste = ((ctas + resident - 1) / resident) * resident - ctas;
+    // compare waste relative to the work: waste / ctas, as a cross-multiplied ratio
+    if (best_waste < 0 || waste * ranges < best_waste * rr) {
+      best_waste = waste;
+      ranges = rr;
+    }
+    if (rr == blocks) break;
+  }
   if (ranges > 65535) ranges = 65535;
   const long long blocks_per_range = (blocks + ranges - 1) / ranges;
   ranges = (blocks + blocks_per_range - 1) / blocks_per_range;
