@@ -161,8 +161,48 @@ class Oracle(_Common):
         return s[: nq * ke].reshape(nq, ke), i[: nq * ke].reshape(nq, ke)
 
 
+    def ivf_search(self, prep, codes_flat, alpha, ids, bucket_start, bucket_size, probes, n_probe, offsets, k):
+        """IVF residual search over bucket-ordered slots (score_prepared_into
+        composed over each query's probed buckets)."""
+        codes_flat = np.ascontiguousarray(codes_flat, np.uint8)
+        nq = prep["luts"].shape[0]
+        nbg = codes_flat.shape[1]
+        probes = np.ascontiguousarray(probes, np.uint32)
+        max_probe = probes.shape[1]
+        s = np.zeros((nq, k), np.float32)
+        i = np.zeros((nq, k), np.uint64)
+        self.lib.tqo_ivf_search(
+            _p(prep["luts"]), _p(prep["lut_scale"]), _p(prep["lut_bias"]), _p(prep["bias_corr"]), _SZ(nq),
+            _SZ(nbg), _p(codes_flat), _p(np.ascontiguousarray(alpha, np.float32)),
+            _p(np.ascontiguousarray(ids, np.uint64)), _p(np.ascontiguousarray(bucket_start, np.uint64)),
+            _p(np.ascontiguousarray(bucket_size, np.uint64)), _p(probes),
+            _p(np.ascontiguousarray(n_probe, np.uint32)), _SZ(max_probe),
+            _p(np.ascontiguousarray(offsets, np.float32)), _SZ(k), _p(s), _p(i))
+        return s, i
+
+
 class Reference(_Common):
     prefix = "tqref_"
+
+    def ivf_search(self, q, bits, residuals, ids, bucket_start, bucket_size, probes, n_probe, offsets, k,
+                   shift=None, scale=None):
+        """The reference's own score_prepared_into over the same buckets: its
+        encode + repack per bucket, LUTs from prepare_queries, one call per
+        (query, probed bucket) in probe order, heaps sorted at the end."""
+        q = np.ascontiguousarray(q, np.float32)
+        nq, dim = q.shape
+        probes = np.ascontiguousarray(probes, np.uint32)
+        s = np.zeros((nq, k), np.float32)
+        i = np.zeros((nq, k), np.uint64)
+        rc = self.lib.tqref_ivf_search(
+            _p(q), _SZ(nq), _SZ(dim), _SZ(bits), _p(shift), _p(scale),
+            _p(np.ascontiguousarray(residuals, np.float32)), _p(np.ascontiguousarray(ids, np.uint64)),
+            _p(np.ascontiguousarray(bucket_start, np.uint64)), _p(np.ascontiguousarray(bucket_size, np.uint64)),
+            _SZ(len(bucket_size)), _p(probes), _p(np.ascontiguousarray(n_probe, np.uint32)), _SZ(probes.shape[1]),
+            _p(np.ascontiguousarray(offsets, np.float32)), _SZ(k), _p(s), _p(i))
+        if rc != 0:
+            raise RuntimeError(self.lib.tqref_last_error().decode())
+        return s, i
 
     def __init__(self, path: Path = REF_SO):
         super().__init__(path)

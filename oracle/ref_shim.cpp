@@ -20,10 +20,12 @@
 //   repack                     src/pack/pack.cpp:366
 //   prepare_queries            src/search/search.cpp:762
 //   score_prepared/search_flat src/search/search.cpp:1072, :1293
+//   score_prepared_into        src/search/search.cpp:1156 (IVF residual scoring)
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <limits>
 #include <memory>
 #include <span>
 #include <string>
@@ -302,6 +304,86 @@ int tqref_index_search(void* hv, const float* q, std::size_t nq, std::size_t k, 
       std::memcpy(scores, res.scores.data(), nq * res.k * sizeof(float));
       std::memcpy(ids, res.ids.data(), nq * res.k * sizeof(std::uint64_t));
     }
+  });
+}
+
+// ---- IVF residual scoring (bucketed index parity) --------------------------
+//
+// The reference's building block for its IVF index: score_prepared_into
+// (src/search/search.cpp:1156-1264) scores one bucket's codes into existing
+// per-query top-k heaps, remapping local ids through the bucket's id map and
+// adding a per-query score offset <q_hat, encode_c> after alpha * LUT score.
+// This driver encodes every bucket's residual rows with the reference's own
+// encode + repack, builds the query LUTs once (prepare_queries), then visits
+// each query's probed buckets in the given order, one score_prepared_into call
+// per (query, bucket), and sorts the heaps (heaps_to_search_results).
+// residuals: n_slots x dim rows, bucket b at rows [start[b], start[b]+size[b]);
+// ids: the original id of every slot; probes/offsets: nq x max_probe, the
+// first n_probe[q] entries valid.
+int tqref_ivf_search(const float* q, std::size_t nq, std::size_t dim, std::size_t bits,
+                     const float* shift, const float* scale, const float* residuals,
+                     const std::uint64_t* ids, const std::uint64_t* bucket_start,
+                     const std::uint64_t* bucket_size, std::size_t n_buckets,
+                     const std::uint32_t* probes, const std::uint32_t* n_probe,
+                     std::size_t max_probe, const float* offsets, std::size_t k,
+                     float* out_scores, std::uint64_t* out_ids) {
+  return guarded([&] {
+    pin_backend(0);
+    vectorcache::Rotation r(dim);
+    auto cb = vectorcache::codebook(bits, dim);
+    vectorcache::Calibration calib;
+    std::span<const float> sh, sc;
+    if (shift) {
+      calib.shift.assign(shift, shift + dim);
+      calib.scale_tq.assign(scale, scale + dim);
+      sh = calib.shift;
+      sc = calib.scale_tq;
+    }
+    struct Bucket {
+      std::vector<std::uint8_t> blocked;
+      std::size_t n_blocks = 0;
+      std::vector<float> alpha;
+      std::vector<std::uint64_t> ids;
+    };
+    std::vector<Bucket> buckets(n_buckets);
+    std::vector<float> scratch;
+    for (std::size_t b = 0; b < n_buckets; ++b) {
+      const std::size_t n = bucket_size[b];
+      if (n == 0) continue;
+      std::vector<std::uint8_t> packed;
+      vectorcache::encode(std::span<const float>(residuals + bucket_start[b] * dim, n * dim), n, dim,
+                          r, cb.first, cb.second, bits, shift ? &calib : nullptr, scratch, packed,
+                          buckets[b].alpha);
+      auto [blocked, nbl] = vectorcache::repack(packed, n, bits, dim);
+      buckets[b].blocked = std::move(blocked);
+      buckets[b].n_blocks = nbl;
+      buckets[b].ids.assign(ids + bucket_start[b], ids + bucket_start[b] + n);
+    }
+    auto prep = vectorcache::prepare_queries(std::span<const float>(q, nq * dim), nq, dim, r,
+                                             cb.second, bits, sh, sc);
+    if (prep.backend != vectorcache::SearchBackendKind::Avx2) {
+      throw std::runtime_error("reference backend is not avx2_perm0");
+    }
+    std::vector<float> heap_s(nq * k), heap_min(nq, -std::numeric_limits<float>::infinity());
+    std::vector<std::uint64_t> heap_i(nq * k);
+    std::vector<std::size_t> heap_sz(nq, 0), heap_mi(nq, 0);
+    std::vector<float> offs(nq, 0.f);
+    for (std::size_t qi = 0; qi < nq; ++qi) {
+      const std::size_t one[1] = {qi};
+      for (std::size_t j = 0; j < n_probe[qi]; ++j) {
+        const Bucket& bk = buckets[probes[qi * max_probe + j]];
+        if (bk.alpha.empty()) continue;
+        offs[qi] = offsets[qi * max_probe + j];
+        vectorcache::score_prepared_into(prep, k, bk.blocked, bk.n_blocks, bk.alpha, bk.ids,
+                                         std::span<const std::size_t>(one, 1), heap_s.data(),
+                                         heap_i.data(), heap_sz.data(), heap_min.data(),
+                                         heap_mi.data(), offs.data());
+      }
+    }
+    vectorcache::SearchResults res;
+    vectorcache::heaps_to_search_results(res, nq, k, heap_s.data(), heap_i.data(), heap_sz.data());
+    std::memcpy(out_scores, res.scores.data(), nq * k * sizeof(float));
+    std::memcpy(out_ids, res.ids.data(), nq * k * sizeof(std::uint64_t));
   });
 }
 

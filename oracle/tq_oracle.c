@@ -705,3 +705,79 @@ void tqo_float_rescore(const float* queries, size_t nq, size_t dim, const float*
     free(row);
   }
 }
+
+/* ----------------------------------------------------------------------------
+ * IVF residual search over bucket-ordered slots: the composition of
+ * score_prepared_into (search.cpp:1156-1264) the bucketed index performs.
+ * Each query visits its probed buckets in probe order; every vector's score is
+ * (fa * alpha) + offset with two roundings (search_avx2.cpp:150-161, :217-219:
+ * the multiply and the offset add are separate instructions), and enters the
+ * query's top-k collector under the reference heap rule (topk_heap.hpp:101-157):
+ * admitted only when strictly above the current minimum, replacing the worst
+ * entry (lowest score, ties: larger id). The kept entries are finally sorted
+ * score descending, equal scores by lower id (heaps_to_search_results,
+ * search.cpp:1266-1290); rows with fewer than k entries are padded with
+ * (0, 0).
+ * ------------------------------------------------------------------------- */
+void tqo_ivf_search(const uint8_t* luts, const float* lut_scale, const float* lut_bias,
+                    const float* bias_corr, size_t nq, size_t nbg, const uint8_t* codes_flat,
+                    const float* alpha, const uint64_t* ids, const uint64_t* bucket_start,
+                    const uint64_t* bucket_size, const uint32_t* probes,
+                    const uint32_t* n_probe, size_t max_probe, const float* offsets, size_t k,
+                    float* out_scores, uint64_t* out_ids) {
+#pragma omp parallel
+  {
+    cand_t* heap = malloc((k ? k : 1) * sizeof(cand_t));
+#pragma omp for schedule(dynamic)
+    for (long long qi = 0; qi < (long long)nq; ++qi) {
+      const uint8_t* lut = luts + (size_t)qi * nbg * 32;
+      size_t sz = 0, mi = 0;
+      float hmin = -INFINITY;
+      for (size_t j = 0; j < n_probe[qi]; ++j) {
+        const uint32_t b = probes[(size_t)qi * max_probe + j];
+        const float off = offsets[(size_t)qi * max_probe + j];
+        for (uint64_t t = 0; t < bucket_size[b]; ++t) {
+          const size_t slot = (size_t)(bucket_start[b] + t);
+          const uint8_t* c = codes_flat + slot * nbg;
+          float fa = lut_bias[qi] + (bias_corr ? bias_corr[qi] : 0.f);
+          for (size_t g0 = 0; g0 < nbg; g0 += 256) {
+            const size_t g1 = (g0 + 256 < nbg) ? g0 + 256 : nbg;
+            uint32_t acc = 0;
+            for (size_t g = g0; g < g1; ++g) acc += lut[g * 32 + (c[g] >> 4)] + lut[g * 32 + 16 + (c[g] & 15)];
+            fa = fmaf(lut_scale[qi], (float)acc, fa);
+          }
+          const float prod = fa * alpha[slot];
+          const cand_t cd = {prod + off, ids[slot]};
+          if (!(cd.s > hmin)) continue;
+          if (sz < k) {
+            heap[sz++] = cd;
+            if (sz < k) continue;
+          } else {
+            heap[mi] = cd;
+          }
+          /* rescan for the worst entry */
+          mi = 0;
+          for (size_t h = 1; h < k; ++h) {
+            if (better(&heap[mi], &heap[h])) mi = h;
+          }
+          hmin = heap[mi].s;
+        }
+      }
+      /* insertion sort, best first */
+      for (size_t a = 1; a < sz; ++a) {
+        cand_t x = heap[a];
+        size_t pos = a;
+        while (pos > 0 && better(&x, &heap[pos - 1])) {
+          heap[pos] = heap[pos - 1];
+          --pos;
+        }
+        heap[pos] = x;
+      }
+      for (size_t j = 0; j < k; ++j) {
+        out_scores[(size_t)qi * k + j] = j < sz ? heap[j].s : 0.f;
+        out_ids[(size_t)qi * k + j] = j < sz ? heap[j].id : 0;
+      }
+    }
+    free(heap);
+  }
+}

@@ -72,6 +72,15 @@ size_t tqo_search_flat(const float* q, size_t nq, size_t dim, size_t bits, const
 void tqo_float_rescore(const float* queries, size_t nq, size_t dim, const float* corpus,
                        size_t n_corpus, size_t k, float* scores, uint64_t* ids);
 
+/* IVF residual search over bucket-ordered slots (score_prepared_into,
+ * search.cpp:1156-1264, composed per query over its probed buckets). */
+void tqo_ivf_search(const uint8_t* luts, const float* lut_scale, const float* lut_bias,
+                    const float* bias_corr, size_t nq, size_t nbg, const uint8_t* codes_flat,
+                    const float* alpha, const uint64_t* ids, const uint64_t* bucket_start,
+                    const uint64_t* bucket_size, const uint32_t* probes,
+                    const uint32_t* n_probe, size_t max_probe, const float* offsets, size_t k,
+                    float* out_scores, uint64_t* out_ids);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,318 @@
+// The flat TurboQuant index object shared by the C ABI translation units:
+// tq_index.cu (flat index entry points) and tq_bucketed.cu, which uses one
+// flat index as its encoder and query-LUT engine over bucket-ordered slots.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/vectorcache_b200.h"
+#include "tq_abi.h"
+#include "tq_host_math.h"
+#include "tq_kernels.h"
+
+namespace vcb {
+
+inline void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  const int code = (e == cudaErrorMemoryAllocation) ? TQ_ERR_OUT_OF_MEMORY : TQ_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Grow-only device allocation.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+
+  void* reserve(size_t bytes) {
+    if (bytes <= bytes_ && ptr_) return ptr_;
+    release();
+    if (bytes == 0) bytes = 16;
+    check(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    bytes_ = bytes;
+    return ptr_;
+  }
+  void release() {
+    if (ptr_) cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+  }
+  void swap(DeviceBuffer& o) noexcept {
+    std::swap(ptr_, o.ptr_);
+    std::swap(bytes_, o.bytes_);
+  }
+  void* get() const { return ptr_; }
+  size_t bytes() const { return bytes_; }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr_);
+  }
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    check(cudaGetDevice(&prev_), "cudaGetDevice");
+    if (prev_ != device) check(cudaSetDevice(device), "cudaSetDevice");
+    restore_ = prev_ != device;
+  }
+  ~DeviceGuard() {
+    if (restore_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0;
+  bool restore_ = false;
+};
+
+inline size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+}  // namespace vcb
+
+struct tq_index;
+
+namespace vcb {
+// TQ+ fit (encode.cpp:242-286, 327-335) from n device rows; defined in tq_index.cu.
+void calibrate_index(tq_index* h, const float* d_sample, size_t n, cudaStream_t s);
+}  // namespace vcb
+
+struct tq_index {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  size_t dim = 0, bits = 0, nbg = 0, block = 0;
+  float inv_sqrt_block = 0.f;
+  vcb::Codebook cb;
+  bool calibrated = false;
+  std::vector<float> shift, scale;
+  bool prepared = false;
+  size_t n = 0;          // encoded vectors
+  size_t staged_n = 0;   // rows waiting for prepare()
+  size_t cap = 0;        // layout capacity in vectors (multiple of kScanBlockVectors)
+
+  vcb::DeviceBuffer d_perm_sign, d_bnd, d_cen, d_shift, d_scale, d_inv_scale;
+  vcb::DeviceBuffer d_codes, d_alpha, d_staged, d_flat, d_counter;
+  // search scratch
+  vcb::DeviceBuffer d_queries, d_luts, d_qf, d_cand_s, d_cand_i, d_out_s, d_out_i, d_qrot;
+
+  // Optional per-launch timing (tq_index_set_profiling).
+  enum Kind { kPrep = 0, kScan = 1, kMerge = 2, kEncode = 3 };
+  struct Timed {
+    int kind;
+    cudaEvent_t start, stop;
+  };
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<Timed> timed_launches;
+  uint64_t launches[4] = {0, 0, 0, 0};
+  uint64_t scan_stream_bytes = 0, scan_queries = 0;
+
+  ~tq_index() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+    for (auto& t : timed_launches) {
+      cudaEventDestroy(t.start);
+      cudaEventDestroy(t.stop);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
+  }
+
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    vcb::check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+  }
+
+  // Runs one kernel launch, bracketed by events when profiling is on.
+  template <typename F>
+  void launch(int kind, cudaStream_t s, const char* what, F&& fn) {
+    ++launches[kind];
+    if (!profiling) {
+      vcb::check(fn(), what);
+      return;
+    }
+    Timed t{kind, take_event(), take_event()};
+    vcb::check(cudaEventRecord(t.start, s), "cudaEventRecord");
+    vcb::check(fn(), what);
+    vcb::check(cudaEventRecord(t.stop, s), "cudaEventRecord");
+    timed_launches.push_back(t);
+  }
+
+  void sync() { vcb::check(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+
+  cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
+
+  size_t flat_stride() const { return vcb::round_up(nbg, 32); }
+
+  void upload(void* dst, const void* src, size_t bytes) {
+    vcb::check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "cudaMemcpyAsync H2D");
+  }
+
+  // Grow the scan layout and alpha buffers to hold `want` vectors.
+  void ensure_capacity(size_t want) {
+    if (want <= cap) return;
+    size_t new_cap = std::max(want, cap + cap / 2);
+    new_cap = vcb::round_up(new_cap, vcb::kScanBlockVectors);
+    const size_t code_bytes = (new_cap / vcb::kTileVectors) * nbg * vcb::kTileWords * 4;
+    vcb::DeviceBuffer codes, alpha;
+    codes.reserve(code_bytes);
+    alpha.reserve(new_cap * 4);
+    vcb::check(cudaMemsetAsync(codes.get(), 0, code_bytes, stream), "cudaMemsetAsync");
+    vcb::check(cudaMemsetAsync(alpha.get(), 0, new_cap * 4, stream), "cudaMemsetAsync");
+    if (cap > 0) {
+      // Tiles are self-contained, so the old layout is a prefix of the new one.
+      const size_t old_code_bytes = (cap / vcb::kTileVectors) * nbg * vcb::kTileWords * 4;
+      vcb::check(cudaMemcpyAsync(codes.get(), d_codes.get(), old_code_bytes, cudaMemcpyDeviceToDevice, stream),
+                 "cudaMemcpyAsync D2D");
+      vcb::check(cudaMemcpyAsync(alpha.get(), d_alpha.get(), cap * 4, cudaMemcpyDeviceToDevice, stream),
+                 "cudaMemcpyAsync D2D");
+    }
+    sync();
+    codes.swap(d_codes);
+    alpha.swap(d_alpha);
+    cap = new_cap;
+  }
+
+  // Encode `count` rows at device pointer x and append them after the current n.
+  void encode_append(const float* x, size_t count, cudaStream_t s) {
+    if (count == 0) return;
+    ensure_capacity(n + count);
+    const size_t stride = flat_stride();
+    const size_t chunk = std::max<size_t>(1, std::min<size_t>(count, (size_t{512} << 20) / stride));
+    d_flat.reserve(chunk * stride);
+    for (size_t done = 0; done < count; done += chunk) {
+      const size_t m = std::min(chunk, count - done);
+      vcb::EncodeArgs a{};
+      a.x = x + done * dim;
+      a.n = static_cast<long long>(m);
+      a.dim = static_cast<int>(dim);
+      a.bits = static_cast<int>(bits);
+      a.block = static_cast<int>(block);
+      a.inv_sqrt_block = inv_sqrt_block;
+      a.perm_sign = d_perm_sign.as<uint32_t>();
+      a.boundaries = d_bnd.as<float>();
+      a.centroids = d_cen.as<float>();
+      a.tqplus = calibrated;
+      a.shift = d_shift.as<float>();
+      a.scale = d_scale.as<float>();
+      a.inv_scale = d_inv_scale.as<float>();
+      a.out_flat = d_flat.as<uint8_t>();
+      a.flat_stride = static_cast<int>(stride);
+      a.out_alpha = d_alpha.as<float>() + n + done;
+      a.replay_count = d_counter.as<unsigned long long>();
+      launch(kEncode, s, "encode kernel", [&] { return vcb::launch_encode(a, sms, s); });
+      vcb::RelayoutArgs r{};
+      r.flat = d_flat.as<uint8_t>();
+      r.src_first = static_cast<long long>(n + done);
+      r.src_n = static_cast<long long>(m);
+      r.flat_stride = static_cast<int>(stride);
+      r.keep_below = static_cast<long long>(n + done);
+      r.n_total = static_cast<long long>(n + done + m);
+      r.nbg = static_cast<int>(nbg);
+      r.bits = static_cast<int>(bits);
+      r.codes = d_codes.as<uint32_t>();
+      launch(kEncode, s, "relayout kernel", [&] { return vcb::launch_relayout(r, s); });
+    }
+    n += count;
+  }
+
+  // LUTs and per-query constants for nq device rows.
+  void prep_queries(const float* d_q, size_t nq, cudaStream_t s, float* q_rot_out) {
+    d_luts.reserve(nq * nbg * 32);
+    d_qf.reserve(nq * 4 * sizeof(float));
+    float* qf = d_qf.as<float>();
+    vcb::QueryPrepArgs a{};
+    a.q = d_q;
+    a.nq = static_cast<long long>(nq);
+    a.dim = static_cast<int>(dim);
+    a.bits = static_cast<int>(bits);
+    a.block = static_cast<int>(block);
+    a.nbg = static_cast<int>(nbg);
+    a.inv_sqrt_block = inv_sqrt_block;
+    a.perm_sign = d_perm_sign.as<uint32_t>();
+    a.centroids = d_cen.as<float>();
+    a.tqplus = calibrated;
+    a.shift = d_shift.as<float>();
+    a.scale = d_scale.as<float>();
+    a.luts = d_luts.as<uint8_t>();
+    a.lut_scale = qf;
+    a.lut_bias = qf + nq;
+    a.bias_corr = qf + 2 * nq;
+    a.fa_init = qf + 3 * nq;
+    a.q_rot = q_rot_out;
+    a.replay_count = d_counter.as<unsigned long long>();
+    launch(kPrep, s, "query prep kernel", [&] { return vcb::launch_query_prep(a, sms, s); });
+  }
+
+  // Full device search of nq rows at d_q into d_scores/d_ids (stride k_eff).
+  void search_device(const float* d_q, size_t nq, size_t k, float* d_scores, uint64_t* d_ids,
+                     size_t k_eff, cudaStream_t s) {
+    if (nq == 0 || k_eff == 0) return;
+    // Bound the scratch per pass: LUTs + candidate lists.
+    const size_t max_pass = 1 << 16;
+    for (size_t q0 = 0; q0 < nq; q0 += max_pass) {
+      const size_t m = std::min(max_pass, nq - q0);
+      prep_queries(d_q + q0 * dim, m, s, nullptr);
+      vcb::ScanPlan plan;
+      if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
+                          static_cast<int>(k_eff), sms, &plan)) {
+        vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
+      }
+      const size_t lists = static_cast<size_t>(plan.n_ranges) * plan.lists_per_range;
+      d_cand_s.reserve(m * lists * k_eff * 4);
+      d_cand_i.reserve(m * lists * k_eff * 4);
+      const float* qf = d_qf.as<float>();
+      vcb::ScanArgs a{};
+      a.codes = d_codes.as<uint32_t>();
+      a.alpha = d_alpha.as<float>();
+      a.luts = d_luts.as<uint8_t>();
+      a.lut_scale = qf;
+      a.fa_init = qf + 3 * m;
+      a.n = static_cast<long long>(n);
+      a.nbg = static_cast<int>(nbg);
+      a.nq = static_cast<long long>(m);
+      a.k = static_cast<int>(k_eff);
+      a.q_per_cta = plan.q_per_cta;
+      a.range_vectors = plan.range_vectors;
+      a.n_ranges = plan.n_ranges;
+      a.lut_chunk_groups = plan.lut_chunk_groups;
+      a.bits = static_cast<int>(bits);
+      a.cand_score = d_cand_s.as<float>();
+      a.cand_id = d_cand_i.as<uint32_t>();
+      launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
+      scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
+      scan_queries += m;
+      vcb::MergeArgs mg{};
+      mg.cand_score = a.cand_score;
+      mg.cand_id = a.cand_id;
+      mg.nq = static_cast<long long>(m);
+      mg.n_lists = static_cast<int>(lists);
+      mg.k = static_cast<int>(k_eff);
+      mg.k_out = static_cast<int>(k_eff);
+      mg.out_score = d_scores + q0 * k_eff;
+      mg.out_id = d_ids + q0 * k_eff;
+      launch(kMerge, s, "merge kernel", [&] { return vcb::launch_merge(mg, s); });
+    }
+    (void)k;
+  }
+};
+
