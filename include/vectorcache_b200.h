@@ -195,6 +195,85 @@ typedef struct tq_profile {
 int tq_index_set_profiling(tq_index* h, int enabled);
 int tq_index_read_profile(tq_index* h, tq_profile* out);
 
+/* ---- bucketed (IVF) index ---------------------------------------------------
+ * BucketedTurboQuantIndex / BucketParams of the reference's README
+ * (README.md:56, :91-98, :113-120); the reference ships no implementation of
+ * them, only the per-bucket scoring they compose, score_prepared_into
+ * (src/search/search.cpp:1156-1264), which the search reproduces bit for bit:
+ * score = (fa * alpha) + <q_hat, encode_c> over each probed bucket's residual
+ * codes x_hat - encode_c, top-k in (score desc, id asc) order.
+ *
+ * Rows and queries are L2-normalized (cosine); dim need not be a multiple of 8
+ * (rows are zero-padded to the next multiple of 8 internally, dim <= 2048).
+ * The partition: ceil(expected_n / energy_soft) seeds, kmeans_iters rounds of
+ * spherical k-means, then 2-means fission of every bucket above
+ * max_bucket_size; it is deterministic for a given seed. */
+typedef struct tq_bucket_params {
+  uint32_t n_probe;         /* buckets scanned per query by default (64), <= 256 */
+  uint32_t max_bucket_size; /* hard cap; larger buckets are split (800), <= 8192 */
+  uint32_t energy_soft;     /* target mean bucket size of the initial partition (400) */
+  uint32_t kmeans_iters;    /* spherical k-means rounds of the initial partition (4) */
+  uint64_t expected_n;      /* corpus size the partition is sized for; 0 = rows at prepare() */
+  uint64_t seed;            /* seed of the initial centroid choice */
+} tq_bucket_params;
+
+typedef struct tq_bucketed tq_bucketed;
+
+/* Default parameters (the values in parentheses above). */
+void tq_bucket_params_init(tq_bucket_params* p);
+
+/* params may be NULL (defaults). */
+int tq_bucketed_create(size_t dim, size_t bits, const tq_bucket_params* params, int device,
+                       tq_bucketed** out);
+int tq_bucketed_destroy(tq_bucketed* h);
+/* Optional TQ+ calibration sample (host rows); fitted at prepare() on the
+ * residuals of these rows against their nearest bucket. */
+int tq_bucketed_calibrate(tq_bucketed* h, const float* sample, size_t n);
+int tq_bucketed_add(tq_bucketed* h, const float* vectors, size_t n);
+int tq_bucketed_add_device(tq_bucketed* h, const float* d_vectors, size_t n, void* stream);
+/* Builds the partition and encodes the residuals. Rows added after prepare()
+ * are assigned to their nearest routing centroid by the next prepare(), which
+ * also splits buckets that grew past max_bucket_size; encode centroids of
+ * buckets that were not split stay frozen. */
+int tq_bucketed_prepare(tq_bucketed* h);
+/* Top-k over the n_probe best-routed buckets (n_probe = 0: the index's
+ * default). n_probe_per_query (optional, nq entries, each <= n_probe) scans
+ * fewer buckets for some queries — the learned probe predictor's output. */
+int tq_bucketed_search(tq_bucketed* h, const float* queries, size_t nq, size_t k, size_t n_probe,
+                       const uint32_t* n_probe_per_query, float* scores, uint64_t* ids,
+                       size_t* k_eff);
+int tq_bucketed_search_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t k,
+                              size_t n_probe, const uint32_t* d_n_probe, float* d_scores,
+                              uint64_t* d_ids, size_t* k_eff, void* stream);
+/* Routing only: the top p (<= 256) buckets per query and their scores
+ * <q_hat, routing centroid>, best first (device buffers nq x p). */
+int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t p,
+                             float* d_top_scores, uint32_t* d_top_ids, void* stream);
+
+/* Introspection for parity checks. */
+int tq_bucketed_info(const tq_bucketed* h, size_t* dim, size_t* dim_padded, size_t* bits, size_t* n,
+                     size_t* n_buckets, size_t* n_slots, int* prepared);
+/* Search that also returns the probes (nq x n_probe bucket ids, routing
+ * order), the offsets <q_hat, encode_c> of those probes and q_hat
+ * (nq x dim_padded). */
+int tq_bucketed_search_trace(tq_bucketed* h, const float* queries, size_t nq, size_t k,
+                             size_t n_probe, const uint32_t* n_probe_per_query, float* scores,
+                             uint64_t* ids, size_t* k_eff, uint32_t* probes, float* offsets,
+                             float* q_hat);
+/* q_hat (nq x dim_padded) and all routing scores (nq x n_buckets). */
+int tq_bucketed_route(tq_bucketed* h, const float* queries, size_t nq, float* q_hat, float* scores);
+/* slot_start: n_buckets + 1; bucket_size: n_buckets; slot_ids: n_slots
+ * (0xffffffff in padding slots); labels: n (bucket of every row). */
+int tq_bucketed_export_layout(tq_bucketed* h, uint64_t* slot_start, uint32_t* bucket_size,
+                              uint32_t* slot_ids, uint32_t* labels);
+/* routing and encode centroids, n_buckets x dim_padded each. */
+int tq_bucketed_export_centroids(tq_bucketed* h, float* route, float* enc);
+/* the normalized, padded rows (n x dim_padded). */
+int tq_bucketed_export_rows(tq_bucketed* h, float* x_hat);
+/* The flat index over the residual slots (owned by h): its codes_flat,
+ * alpha, calibration and query LUT exports describe the bucketed layout. */
+int tq_bucketed_engine(tq_bucketed* h, tq_index** engine);
+
 /* ---- search without device allocation --------------------------------------
  * No counterpart in the reference.
  *

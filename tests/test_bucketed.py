@@ -1,0 +1,192 @@
+"""Bucketed (IVF) index on the GPU through the C ABI.
+
+* the partition is well formed and deterministic (every row in exactly one
+  bucket, no bucket above max_bucket_size, slot layout aligned, encode
+  centroids = member means, routing centroids = their normalized means);
+* routing scores and probe offsets are fp32 dot products checked against fp64
+  to 1e-5;
+* the residual codes equal the oracle's encoding of x_hat - encode_c;
+* search results equal the C oracle's restatement of the reference's
+  score_prepared_into composition (tests/test_ivf_oracle.py pins that oracle to
+  the reference) on the same probes and offsets: ids and scores bit for bit;
+* recall against exact brute force grows with n_probe.
+"""
+import numpy as np
+import pytest
+
+import vectorcache_b200 as vcb
+from vectorcache_b200.synthetic import vmf_mixture
+
+TOL = 1e-5  # fp32 routing / offset dot products against fp64
+
+
+def bits_equal(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_params_are_validated_before_any_device_work():
+    with pytest.raises(vcb.InvalidArgument):
+        vcb.BucketedTurboQuantIndex(100, 4, vcb.BucketParams(n_probe=0))
+    with pytest.raises(vcb.InvalidArgument):
+        vcb.BucketedTurboQuantIndex(100, 4, vcb.BucketParams(max_bucket_size=1))
+
+
+def _data(n, nq, dim, seed):
+    db = vmf_mixture(n, dim, seed=seed, clusters=60)
+    q = vmf_mixture(nq, dim, seed=seed + 1, clusters=60)
+    return db, q
+
+
+def _build(db, bits, params, calib=None):
+    idx = vcb.BucketedTurboQuantIndex(db.shape[1], bits, params)
+    if calib is not None:
+        idx.calibrate(calib)
+    idx.add(db)
+    idx.prepare()
+    return idx
+
+
+@pytest.fixture(scope="module")
+def small():
+    db, q = _data(12000, 24, 100, seed=11)
+    params = vcb.BucketParams(n_probe=8, max_bucket_size=300, energy_soft=150, kmeans_iters=3, seed=7)
+    return db, q, params
+
+
+@pytest.mark.gpu
+def test_partition_invariants_and_determinism(small):
+    db, q, params = small
+    idx = _build(db, 4, params)
+    inf = idx.info()
+    assert inf["dim_padded"] == 104 and inf["size"] == db.shape[0]
+    lay = idx.layout()
+    nb = inf["n_buckets"]
+    sizes = lay["bucket_size"].astype(np.int64)
+    assert sizes.sum() == db.shape[0] and sizes.min() >= 1 and sizes.max() <= params.max_bucket_size
+    starts = lay["slot_start"].astype(np.int64)
+    assert np.all(starts % 256 == 0) and starts[-1] == inf["n_slots"]
+    assert np.all(np.diff(starts) == (sizes + 255) // 256 * 256)
+    labels = lay["labels"]
+    seen = np.zeros(db.shape[0], np.int64)
+    x_hat = idx.rows()
+    route, enc = idx.centroids()
+    for b in range(nb):
+        ids = lay["slot_ids"][starts[b]:starts[b] + sizes[b]]
+        assert np.all(np.diff(ids.astype(np.int64)) > 0)  # members sorted by id
+        assert np.all(labels[ids] == b)
+        assert np.all(lay["slot_ids"][starts[b] + sizes[b]:starts[b + 1]] == 0xFFFFFFFF)
+        seen[ids] += 1
+        mean = x_hat[ids].astype(np.float64).mean(axis=0)
+        assert np.max(np.abs(enc[b] - mean)) < 1e-6
+        assert np.max(np.abs(route[b] - mean / np.linalg.norm(mean))) < 1e-6
+    assert np.all(seen == 1)
+    # x_hat: unit rows padded with zeros
+    assert np.allclose(np.linalg.norm(x_hat, axis=1), 1.0, atol=1e-6)
+    assert np.all(x_hat[:, 100:] == 0)
+    again = _build(db, 4, params)
+    lay2 = again.layout()
+    assert all(np.array_equal(lay[key], lay2[key]) for key in lay)
+    assert all(bits_equal(a, b) for a, b in zip(idx.centroids(), again.centroids()))
+    idx.close()
+    again.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bits,k,tq", [(4, 10, False), (4, 64, True), (2, 10, True), (3, 1, False)])
+def test_search_matches_oracle(oracle, small, bits, k, tq):
+    db, q, params = small
+    idx = _build(db, bits, params, calib=db[:2000] if tq else None)
+    eng = idx.engine()
+    shift = scale = None
+    if tq:
+        shift, scale = eng.calibration()
+    lay = idx.layout()
+    route, enc = idx.centroids()
+    x_hat = idx.rows()
+    starts = lay["slot_start"].astype(np.int64)
+    sizes = lay["bucket_size"].astype(np.int64)
+    # residual codes: the oracle's encoding of x_hat - encode_c in slot order
+    ns = idx.info()["n_slots"]
+    resid = np.zeros((ns, 104), np.float32)
+    for b in range(len(sizes)):
+        ids = lay["slot_ids"][starts[b]:starts[b] + sizes[b]]
+        resid[starts[b]:starts[b] + sizes[b]] = x_hat[ids] - enc[b]
+    packed, alpha = oracle.encode(resid, bits, shift, scale)
+    flat = oracle.codes_flat(packed, bits, 104)
+    got_flat = eng.codes_flat()[:ns]
+    got_alpha = eng.alpha()[:ns]
+    valid = lay["slot_ids"] != 0xFFFFFFFF
+    assert bits_equal(got_flat[valid], flat[valid])
+    assert bits_equal(got_alpha[valid], alpha[valid])
+
+    tr = idx.search_trace(q, k)
+    qh = tr["q_hat"]
+    # routing scores against fp64, and the probes are the best-routed buckets
+    _, rs = idx.route(q)
+    r64 = qh.astype(np.float64) @ route.astype(np.float64).T
+    assert np.max(np.abs(rs - r64)) < TOL
+    for r in range(q.shape[0]):
+        order = sorted(range(rs.shape[1]), key=lambda b: (-rs[r, b], b))[: tr["probes"].shape[1]]
+        assert np.array_equal(tr["probes"][r], order)
+    off64 = np.einsum("qd,qpd->qp", qh.astype(np.float64), enc[tr["probes"]].astype(np.float64))
+    assert np.max(np.abs(tr["offsets"] - off64)) < TOL
+
+    prep = oracle.prepare_queries(qh, bits, shift, scale)
+    n_probe = np.full(q.shape[0], tr["probes"].shape[1], np.uint32)
+    ws, wi = oracle.ivf_search(prep, got_flat, got_alpha, lay["slot_ids"].astype(np.uint64), starts, sizes,
+                               tr["probes"], n_probe, tr["offsets"], k)
+    assert np.array_equal(tr["ids"], wi[:, : tr["ids"].shape[1]])
+    assert bits_equal(tr["scores"], ws[:, : tr["scores"].shape[1]])
+    idx.close()
+
+
+@pytest.mark.gpu
+def test_per_query_probe_counts(small):
+    db, q, params = small
+    idx = _build(db, 4, params)
+    counts = (np.arange(q.shape[0]) % 8 + 1).astype(np.uint32)
+    mixed = idx.search(q, 10, n_probe=8, n_probe_per_query=counts)
+    for c in np.unique(counts):
+        rows = np.nonzero(counts == c)[0]
+        alone = idx.search(q[rows], 10, n_probe=int(c))
+        assert np.array_equal(mixed.ids[rows], alone.ids)
+        assert bits_equal(mixed.scores[rows], alone.scores)
+    idx.close()
+
+
+@pytest.mark.gpu
+def test_recall_grows_with_n_probe(small):
+    db, q, params = small
+    idx = _build(db, 4, params)
+    x = db / np.linalg.norm(db, axis=1, keepdims=True)
+    qn = q / np.linalg.norm(q, axis=1, keepdims=True)
+    exact = np.argsort(-(qn.astype(np.float64) @ x.astype(np.float64).T), axis=1, kind="stable")[:, :10]
+    nb = idx.info()["n_buckets"]
+    recalls = []
+    for npb in (1, 4, 16, min(nb, 256)):
+        res = idx.search(q, 10, n_probe=npb)
+        hits = sum(len(set(res.ids[r].tolist()) & set(exact[r].tolist())) for r in range(q.shape[0]))
+        recalls.append(hits / (10 * q.shape[0]))
+    assert all(b >= a - 0.02 for a, b in zip(recalls, recalls[1:]))
+    assert recalls[-1] >= 0.85
+    idx.close()
+
+
+@pytest.mark.gpu
+def test_add_after_prepare_keeps_invariants(small):
+    db, q, params = small
+    idx = _build(db[:8000], 4, params)
+    _, enc0 = idx.centroids()
+    idx.add(db[8000:])
+    idx.prepare()
+    lay = idx.layout()
+    sizes = lay["bucket_size"].astype(np.int64)
+    assert sizes.sum() == db.shape[0] and sizes.max() <= params.max_bucket_size
+    _, enc1 = idx.centroids()
+    # buckets that were not split keep their encode centroid (frozen at birth)
+    kept = sum(any(bits_equal(e, f) for f in enc1) for e in enc0)
+    assert kept >= len(enc0) // 2
+    res = idx.search(q, 10)
+    assert res.ids.shape == (q.shape[0], 10)
+    idx.close()

@@ -396,3 +396,8 @@ def _dev(t, n: int | None = None):
     ptr = t.data_ptr()
     rows = t.shape[0] if n is None else n
     return ptr, int(rows)
+
+
+from .bucketed import BucketedTurboQuantIndex, BucketParams  # noqa: E402
+
+__all__ += ["BucketedTurboQuantIndex", "BucketParams"]

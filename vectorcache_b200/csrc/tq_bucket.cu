@@ -1,0 +1,1202 @@
+// Bucketed (IVF) index kernels on sm_100a: build (spherical k-means, 2-means
+// fission, residual slot layout) and search (routing, probe pairs, bucket
+// scan). Interfaces and layout in tq_bucket.h.
+//
+// The bucket scan applies the reference's IVF residual scoring
+// (score_prepared_into, search.cpp:1156-1264; search_avx2.cpp:150-161):
+// FastScan integer LUT sums flushed into f32 every 256 byte groups, then
+// score = (fa * alpha) + <q_hat, encode_c>, two separately rounded operations,
+// and top-k in (score desc, id asc) order over the original ids.
+#include <cfloat>
+#include <climits>
+
+#include "tq_bucket.h"
+#include "tq_device.cuh"
+#include "tq_kernels.h"
+
+namespace vcb {
+namespace {
+
+constexpr int kTile = 128;  // rows of A per GEMM CTA
+constexpr int kTileB = 64;  // rows of B per GEMM CTA step
+constexpr int kKc = 16;     // coordinates per shared-memory stage
+
+// ---------------------------------------------------------------------------
+// Row normalization
+// ---------------------------------------------------------------------------
+__global__ void normalize_rows_kernel(const float* __restrict__ x, long long n, int dim_in, int dim,
+                                      float* __restrict__ out) {
+  const long long row = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float* xr = x + row * dim_in;
+  float s = 0.f;
+  for (int i = lane; i < dim_in; i += kWarp) s = __fmaf_rn(xr[i], xr[i], s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, o));
+  const float nrm = __fsqrt_rn(s);
+  const float inv = nrm > 1e-30f ? __frcp_rn(nrm) : 0.f;
+  float* orow = out + row * dim;
+  for (int i = lane; i < dim; i += kWarp) orow[i] = i < dim_in ? __fmul_rn(xr[i], inv) : 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// fp32 A . B^T tiles: 256 threads, 128 x 64 outputs per step, 8 x 4 per thread,
+// coordinates staged through shared memory 16 at a time.
+// ---------------------------------------------------------------------------
+struct GemmTile {
+  float a[kKc][kTile + 4];
+  float b[kKc][kTileB + 4];
+};
+
+__device__ __forceinline__ void stage_a(GemmTile& t, const float* __restrict__ A, long long m, int dim,
+                                        long long r0, int k0) {
+  for (int e = threadIdx.x; e < kTile * kKc; e += blockDim.x) {
+    const int r = e / kKc, c = e % kKc;
+    const long long row = r0 + r;
+    const int col = k0 + c;
+    t.a[c][r] = (row < m && col < dim) ? A[row * dim + col] : 0.f;
+  }
+}
+
+__device__ __forceinline__ void stage_b(GemmTile& t, const float* __restrict__ B, long long nb, int dim,
+                                        long long c0, int k0) {
+  for (int e = threadIdx.x; e < kTileB * kKc; e += blockDim.x) {
+    const int r = e / kKc, c = e % kKc;
+    const long long row = c0 + r;
+    const int col = k0 + c;
+    t.b[c][r] = (row < nb && col < dim) ? B[row * dim + col] : 0.f;
+  }
+}
+
+// acc[i][j] = sum over coordinates of A[r0 + ty*8 + i] * B[c0 + tx*4 + j].
+__device__ __forceinline__ void tile_product(GemmTile& t, const float* __restrict__ A, long long m,
+                                             const float* __restrict__ B, long long nb, int dim, long long r0,
+                                             long long c0, float (&acc)[8][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < dim; k0 += kKc) {
+    __syncthreads();
+    stage_a(t, A, m, dim, r0, k0);
+    stage_b(t, B, nb, dim, c0, k0);
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kKc; ++c) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&t.a[c][ty * 8]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&t.a[c][ty * 8 + 4]);
+      const float4 bv = *reinterpret_cast<const float4*>(&t.b[c][tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bw[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = __fmaf_rn(av[i], bw[j], acc[i][j]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) gemm_nt_kernel(const float* __restrict__ A, long long m,
+                                                      const float* __restrict__ B, long long nb, int dim,
+                                                      float* __restrict__ C, long long ldc) {
+  __shared__ __align__(16) GemmTile t;
+  const long long r0 = static_cast<long long>(blockIdx.y) * kTile;
+  const long long c0 = static_cast<long long>(blockIdx.x) * kTileB;
+  float acc[8][4];
+  tile_product(t, A, m, B, nb, dim, r0, c0, acc);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long long row = r0 + ty * 8 + i;
+    if (row >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const long long col = c0 + tx * 4 + j;
+      if (col < nb) C[row * ldc + col] = acc[i][j];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) assign_kernel(const float* __restrict__ A, long long m,
+                                                     const float* __restrict__ B, long long nb, int dim,
+                                                     uint32_t* __restrict__ label, float* __restrict__ best) {
+  __shared__ __align__(16) GemmTile t;
+  const long long r0 = static_cast<long long>(blockIdx.x) * kTile;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float bs[8];
+  uint32_t bc[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    bs[i] = -INFINITY;
+    bc[i] = 0xffffffffu;
+  }
+  for (long long c0 = 0; c0 < nb; c0 += kTileB) {
+    float acc[8][4];
+    tile_product(t, A, m, B, nb, dim, r0, c0, acc);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long col = c0 + tx * 4 + j;
+        if (col < nb && better(acc[i][j], static_cast<uint32_t>(col), bs[i], bc[i])) {
+          bs[i] = acc[i][j];
+          bc[i] = static_cast<uint32_t>(col);
+        }
+      }
+  }
+  // The 16 threads of a row group are one half of a warp.
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      const float os = __shfl_xor_sync(full_mask(), bs[i], o);
+      const uint32_t oc = __shfl_xor_sync(full_mask(), bc[i], o);
+      if (better(os, oc, bs[i], bc[i])) {
+        bs[i] = os;
+        bc[i] = oc;
+      }
+    }
+    const long long row = r0 + ty * 8 + i;
+    if (tx == 0 && row < m) {
+      label[row] = bc[i];
+      if (best) best[row] = bs[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Top-p per row (score desc, column asc): candidates stream through a buffer
+// that is sorted together with the best p kept so far.
+// ---------------------------------------------------------------------------
+constexpr int kSelThreads = 256;
+constexpr int kSelChunk = 1024;
+constexpr int kSelCap = 2048;  // >= kSelChunk + 256, power of two
+
+__device__ void cta_sort(float* s, uint32_t* id, int p) {
+  for (int size = 2; size <= p; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < (p >> 1); t += blockDim.x) {
+        const int i = (t / stride) * 2 * stride + (t % stride);
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const float si = s[i], sj = s[j];
+        const uint32_t ii = id[i], ij = id[j];
+        if (better(sj, ij, si, ii) == up) {
+          s[i] = sj;
+          s[j] = si;
+          id[i] = ij;
+          id[j] = ii;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSelThreads) select_top_kernel(const float* __restrict__ S, long long ld,
+                                                                 int ncols, int p, float* __restrict__ out_s,
+                                                                 uint32_t* __restrict__ out_i) {
+  __shared__ float buf_s[kSelCap];
+  __shared__ uint32_t buf_i[kSelCap];
+  __shared__ float keep_s[256];
+  __shared__ uint32_t keep_i[256];
+  __shared__ int n_new;
+  const long long row = blockIdx.x;
+  const float* sr = S + row * ld;
+  int nkeep = 0;
+  float thr_s = -FLT_MAX;
+  uint32_t thr_i = 0xffffffffu;
+  for (int base = 0; base < ncols; base += kSelChunk) {
+    if (threadIdx.x == 0) n_new = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < kSelChunk; t += blockDim.x) {
+      const int c = base + t;
+      if (c < ncols) {
+        const float v = sr[c];
+        if (v > -INFINITY && (nkeep < p || better(v, static_cast<uint32_t>(c), thr_s, thr_i))) {
+          const int pos = atomicAdd(&n_new, 1);
+          buf_s[pos] = v;
+          buf_i[pos] = static_cast<uint32_t>(c);
+        }
+      }
+    }
+    __syncthreads();
+    const int fresh = n_new;
+    __syncthreads();
+    if (fresh == 0) continue;
+    for (int t = threadIdx.x; t < nkeep; t += blockDim.x) {
+      buf_s[fresh + t] = keep_s[t];
+      buf_i[fresh + t] = keep_i[t];
+    }
+    const int tot = fresh + nkeep;
+    int q = 2;
+    while (q < tot) q <<= 1;
+    for (int t = tot + threadIdx.x; t < q; t += blockDim.x) {
+      buf_s[t] = -INFINITY;
+      buf_i[t] = 0xffffffffu;
+    }
+    __syncthreads();
+    cta_sort(buf_s, buf_i, q);
+    nkeep = min(p, tot);
+    for (int t = threadIdx.x; t < nkeep; t += blockDim.x) {
+      keep_s[t] = buf_s[t];
+      keep_i[t] = buf_i[t];
+    }
+    if (nkeep == p) {
+      thr_s = buf_s[p - 1];
+      thr_i = buf_i[p - 1];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < p; t += blockDim.x) {
+    const bool have = t < nkeep;
+    out_s[row * p + t] = have ? keep_s[t] : -INFINITY;
+    out_i[row * p + t] = have ? keep_i[t] : 0xffffffffu;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Counting sort by label and prefix sums
+// ---------------------------------------------------------------------------
+__global__ void label_hist_kernel(const uint32_t* __restrict__ label, long long n, uint32_t* __restrict__ counts) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&counts[label[i]], 1u);
+}
+
+// Exclusive prefix sums of counts (and of ceil(counts / div) when div > 0) in
+// one CTA; out[nb] = total.
+__global__ void __launch_bounds__(1024) prefix_kernel(const uint32_t* __restrict__ counts, int nb,
+                                                      unsigned long long* __restrict__ out, int div,
+                                                      unsigned long long* __restrict__ out_div,
+                                                      unsigned long long* __restrict__ total_div) {
+  __shared__ unsigned long long part[1024];
+  __shared__ unsigned long long part_d[1024];
+  __shared__ unsigned long long carry, carry_d;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    carry_d = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + threadIdx.x;
+    const unsigned long long c = i < nb ? counts[i] : 0ull;
+    const unsigned long long cd = (i < nb && div > 0) ? (c + div - 1) / div : 0ull;
+    part[threadIdx.x] = c;
+    part_d[threadIdx.x] = cd;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      const unsigned long long v = threadIdx.x >= o ? part[threadIdx.x - o] : 0ull;
+      const unsigned long long vd = threadIdx.x >= o ? part_d[threadIdx.x - o] : 0ull;
+      __syncthreads();
+      part[threadIdx.x] += v;
+      part_d[threadIdx.x] += vd;
+      __syncthreads();
+    }
+    if (i < nb) {
+      out[i] = carry + part[threadIdx.x] - c;
+      if (div > 0) out_div[i] = carry_d + part_d[threadIdx.x] - cd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 1023) {
+      carry += part[1023];
+      carry_d += part_d[1023];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[nb] = carry;
+    if (div > 0) {
+      out_div[nb] = carry_d;
+      if (total_div) *total_div = carry_d;
+    }
+  }
+}
+
+__global__ void label_scatter_kernel(const uint32_t* __restrict__ label, long long n,
+                                     const unsigned long long* __restrict__ starts, uint32_t* __restrict__ fill,
+                                     uint32_t* __restrict__ members) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t b = label[i];
+  const unsigned long long pos = starts[b] + atomicAdd(&fill[b], 1u);
+  members[pos] = static_cast<uint32_t>(i);
+}
+
+__global__ void __launch_bounds__(512) sort_groups_kernel(const unsigned long long* __restrict__ starts,
+                                                          uint32_t* __restrict__ members) {
+  extern __shared__ uint32_t sm[];
+  const int b = blockIdx.x;
+  const unsigned long long s0 = starts[b], s1 = starts[b + 1];
+  const int n = static_cast<int>(s1 - s0);
+  if (n < 2) return;
+  int p = 2;
+  while (p < n) p <<= 1;
+  for (int t = threadIdx.x; t < p; t += blockDim.x) sm[t] = t < n ? members[s0 + t] : 0xffffffffu;
+  __syncthreads();
+  for (int size = 2; size <= p; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < (p >> 1); t += blockDim.x) {
+        const int i = (t / stride) * 2 * stride + (t % stride);
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const uint32_t a = sm[i], c = sm[j];
+        if ((c < a) == up) {
+          sm[i] = c;
+          sm[j] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) members[s0 + t] = sm[t];
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic centroids
+// ---------------------------------------------------------------------------
+constexpr int kCentSplit = 8;
+constexpr int kCentThreads = 256;
+constexpr int kCentMaxDim = 4096;
+
+__device__ __forceinline__ long long to_fixed(float v) {
+  return __double2ll_rn(static_cast<double>(v) * kFixedScale);
+}
+
+__global__ void __launch_bounds__(kCentThreads) centroid_sum_kernel(const float* __restrict__ X, int dim,
+                                                                    const unsigned long long* __restrict__ starts,
+                                                                    const uint32_t* __restrict__ members,
+                                                                    long long* __restrict__ acc) {
+  const int b = blockIdx.x, part = blockIdx.y;
+  const unsigned long long s0 = starts[b], s1 = starts[b + 1];
+  const unsigned long long n = s1 - s0;
+  if (n == 0) return;
+  const unsigned long long per = (n + kCentSplit - 1) / kCentSplit;
+  const unsigned long long m0 = s0 + part * per;
+  const unsigned long long m1 = min(s1, m0 + per);
+  if (m0 >= m1) return;
+  constexpr int kR = kCentMaxDim / kCentThreads;
+  long long sum[kR];
+#pragma unroll
+  for (int r = 0; r < kR; ++r) sum[r] = 0;
+  for (unsigned long long m = m0; m < m1; ++m) {
+    const float* row = X + static_cast<long long>(members[m]) * dim;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const int d = threadIdx.x + r * kCentThreads;
+      if (d < dim) sum[r] += to_fixed(row[d]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const int d = threadIdx.x + r * kCentThreads;
+    if (d < dim) {
+      atomicAdd(reinterpret_cast<unsigned long long*>(acc + static_cast<long long>(b) * dim + d),
+                static_cast<unsigned long long>(sum[r]));
+    }
+  }
+}
+
+// One warp per group: enc = fixed-point sum / (count * 2^32); route = enc / ||enc||.
+__global__ void centroid_finish_kernel(const long long* __restrict__ acc, int dim, int nb,
+                                       const unsigned long long* __restrict__ starts, float* __restrict__ enc,
+                                       float* __restrict__ route) {
+  const int b = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int lane = threadIdx.x & 31;
+  if (b >= nb) return;
+  const unsigned long long n = starts[b + 1] - starts[b];
+  if (n == 0) return;
+  const double inv = 1.0 / (static_cast<double>(n) * kFixedScale);
+  double ss = 0.0;
+  for (int d = lane; d < dim; d += kWarp) {
+    const float v = static_cast<float>(static_cast<double>(acc[static_cast<long long>(b) * dim + d]) * inv);
+    enc[static_cast<long long>(b) * dim + d] = v;
+    ss += static_cast<double>(v) * v;
+  }
+  ss = warp_sum_d(ss);
+  const double rn = ss > 0.0 ? 1.0 / sqrt(ss) : 0.0;
+  for (int d = lane; d < dim; d += kWarp) {
+    route[static_cast<long long>(b) * dim + d] =
+        static_cast<float>(static_cast<double>(enc[static_cast<long long>(b) * dim + d]) * rn);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2-means fission
+// ---------------------------------------------------------------------------
+constexpr int kSplitThreads = 256;
+
+__device__ __forceinline__ float warp_dot(const float* __restrict__ a, const float* __restrict__ b, int dim,
+                                          int lane) {
+  float s = 0.f;
+  for (int d = lane; d < dim; d += kWarp) s = __fmaf_rn(a[d], b[d], s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, o));
+  return s;
+}
+
+// Lowest (value, id) over the CTA; every thread gets the winner's id.
+__device__ uint32_t cta_argmin(float v, uint32_t id, float* red_v, uint32_t* red_i) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(full_mask(), v, o);
+    const uint32_t oi = __shfl_xor_sync(full_mask(), id, o);
+    if (ov < v || (ov == v && oi < id)) {
+      v = ov;
+      id = oi;
+    }
+  }
+  __syncthreads();
+  if (lane == 0) {
+    red_v[warp] = v;
+    red_i[warp] = id;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kSplitThreads / kWarp; ++w) {
+      if (red_v[w] < red_v[0] || (red_v[w] == red_v[0] && red_i[w] < red_i[0])) {
+        red_v[0] = red_v[w];
+        red_i[0] = red_i[w];
+      }
+    }
+  }
+  __syncthreads();
+  return red_i[0];
+}
+
+__global__ void __launch_bounds__(kSplitThreads) split_kernel(const float* __restrict__ X, int dim,
+                                                              const unsigned long long* __restrict__ starts,
+                                                              const uint32_t* __restrict__ members,
+                                                              const uint32_t* __restrict__ groups,
+                                                              const uint32_t* __restrict__ new_label,
+                                                              const float* __restrict__ route,
+                                                              uint32_t* __restrict__ label, int force_bits) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* cA = reinterpret_cast<float*>(smem);             // dim
+  float* cB = cA + dim;                                   // dim
+  unsigned long long* sum0 = reinterpret_cast<unsigned long long*>(cB + dim);  // dim
+  unsigned long long* sum1 = sum0 + dim;                  // dim
+  __shared__ float red_v[kSplitThreads / kWarp];
+  __shared__ uint32_t red_i[kSplitThreads / kWarp];
+  __shared__ unsigned int n_side[2];
+  __shared__ unsigned int id_or, id_and;
+  const int g = groups[blockIdx.x];
+  const uint32_t lab1 = new_label[blockIdx.x];
+  const unsigned long long s0 = starts[g], s1 = starts[g + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kSplitThreads / kWarp;
+  const float* c = route + static_cast<long long>(g) * dim;
+
+  // Seed A: the member least aligned with the routing centroid.
+  float bv = INFINITY;
+  uint32_t bi = 0xffffffffu;
+  for (unsigned long long m = s0 + warp; m < s1; m += kWarps) {
+    const uint32_t id = members[m];
+    const float d = warp_dot(X + static_cast<long long>(id) * dim, c, dim, lane);
+    if (d < bv || (d == bv && id < bi)) {
+      bv = d;
+      bi = id;
+    }
+  }
+  const uint32_t seed_a = cta_argmin(bv, bi, red_v, red_i);
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) cA[d] = X[static_cast<long long>(seed_a) * dim + d];
+  __syncthreads();
+  // Seed B: the member least aligned with seed A.
+  bv = INFINITY;
+  bi = 0xffffffffu;
+  for (unsigned long long m = s0 + warp; m < s1; m += kWarps) {
+    const uint32_t id = members[m];
+    const float d = warp_dot(X + static_cast<long long>(id) * dim, cA, dim, lane);
+    if (d < bv || (d == bv && id < bi)) {
+      bv = d;
+      bi = id;
+    }
+  }
+  const uint32_t seed_b = cta_argmin(bv, bi, red_v, red_i);
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) cB[d] = X[static_cast<long long>(seed_b) * dim + d];
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) {
+    sum0[d] = 0ull;
+    sum1[d] = 0ull;
+  }
+  if (threadIdx.x < 2) n_side[threadIdx.x] = 0u;
+  __syncthreads();
+  // Members to the closer seed; fixed-point sums of the two sides.
+  for (unsigned long long m = s0 + warp; m < s1; m += kWarps) {
+    const uint32_t id = members[m];
+    const float* row = X + static_cast<long long>(id) * dim;
+    const float da = warp_dot(row, cA, dim, lane), db = warp_dot(row, cB, dim, lane);
+    unsigned long long* sum = (db > da) ? sum1 : sum0;
+    for (int d = lane; d < dim; d += kWarp) atomicAdd(&sum[d], static_cast<unsigned long long>(to_fixed(row[d])));
+  }
+  __syncthreads();
+  // The two means (sums; their scale does not matter for the cosine comparison).
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) {
+    const float a = static_cast<float>(static_cast<double>(static_cast<long long>(sum0[d])) / kFixedScale);
+    const float b = static_cast<float>(static_cast<double>(static_cast<long long>(sum1[d])) / kFixedScale);
+    cA[d] = a;
+    cB[d] = b;
+  }
+  __syncthreads();
+  // Members to the closer mean (cosine): compare <x, a>/|a| with <x, b>/|b|.
+  __shared__ float norm_ab[2];
+  if (warp == 0) {
+    const float na = warp_dot(cA, cA, dim, lane), nb = warp_dot(cB, cB, dim, lane);
+    if (lane == 0) {
+      norm_ab[0] = __fsqrt_rn(na);
+      norm_ab[1] = __fsqrt_rn(nb);
+    }
+  }
+  if (threadIdx.x == 0) {
+    id_or = 0u;
+    id_and = 0xffffffffu;
+  }
+  __syncthreads();
+  const float na = norm_ab[0], nb = norm_ab[1];
+  for (unsigned long long m = s0 + warp; m < s1; m += kWarps) {
+    const uint32_t id = members[m];
+    const float* row = X + static_cast<long long>(id) * dim;
+    const float da = warp_dot(row, cA, dim, lane), db = warp_dot(row, cB, dim, lane);
+    // db / nb > da / na, cross-multiplied (norms are >= 0)
+    const bool side = __fmul_rn(db, na) > __fmul_rn(da, nb);
+    if (lane == 0) {
+      atomicAdd(&n_side[side ? 1 : 0], 1u);
+      atomicOr(&id_or, id);
+      atomicAnd(&id_and, id);
+    }
+  }
+  __syncthreads();
+  const bool degenerate = force_bits || n_side[0] == 0u || n_side[1] == 0u;
+  // Degenerate split (e.g. identical rows): divide by the lowest id bit that
+  // differs among the members (ids are distinct, so one does).
+  const unsigned diff = id_or ^ id_and;
+  const int bit = diff ? __ffs(static_cast<int>(diff)) - 1 : 0;
+  for (unsigned long long m = s0 + warp; m < s1; m += kWarps) {
+    const uint32_t id = members[m];
+    bool side;
+    if (degenerate) {
+      side = (id >> bit) & 1u;
+    } else {
+      const float* row = X + static_cast<long long>(id) * dim;
+      const float da = warp_dot(row, cA, dim, lane), db = warp_dot(row, cB, dim, lane);
+      side = __fmul_rn(db, na) > __fmul_rn(da, nb);
+    }
+    if (lane == 0 && side) label[id] = lab1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual slot layout
+// ---------------------------------------------------------------------------
+__global__ void build_residuals_kernel(const float* __restrict__ X, int dim,
+                                       const unsigned long long* __restrict__ starts,
+                                       const uint32_t* __restrict__ members,
+                                       const unsigned long long* __restrict__ slot_start,
+                                       const float* __restrict__ enc, float* __restrict__ R,
+                                       uint32_t* __restrict__ slot_ids) {
+  const int b = blockIdx.x;
+  const unsigned long long s0 = starts[b], n = starts[b + 1] - s0;
+  const unsigned long long t0 = slot_start[b], t1 = slot_start[b + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x / kWarp;
+  const float* c = enc + static_cast<long long>(b) * dim;
+  for (unsigned long long t = t0 + warp; t < t1; t += warps) {
+    const unsigned long long r = t - t0;
+    float* out = R + static_cast<long long>(t) * dim;
+    if (r < n) {
+      const uint32_t id = members[s0 + r];
+      const float* row = X + static_cast<long long>(id) * dim;
+      for (int d = lane; d < dim; d += kWarp) out[d] = __fsub_rn(row[d], c[d]);
+      if (lane == 0) slot_ids[t] = id;
+    } else {
+      for (int d = lane; d < dim; d += kWarp) out[d] = 0.f;
+      if (lane == 0) slot_ids[t] = 0xffffffffu;
+    }
+  }
+}
+
+__global__ void residual_rows_kernel(const float* __restrict__ X, long long n, int dim,
+                                     const uint32_t* __restrict__ label, const float* __restrict__ enc,
+                                     float* __restrict__ R) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n * dim) return;
+  const long long row = i / dim;
+  const int d = static_cast<int>(i % dim);
+  R[i] = __fsub_rn(X[i], enc[static_cast<long long>(label[row]) * dim + d]);
+}
+
+// ---------------------------------------------------------------------------
+// Probe pairs and work items
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int probes_of(const PairArgs& a, long long q) {
+  const int np = a.n_probe ? static_cast<int>(a.n_probe[q]) : a.fixed_probe;
+  return np < a.max_probe ? np : a.max_probe;
+}
+
+__global__ void pair_count_kernel(PairArgs a) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= a.nq * a.max_probe) return;
+  const long long q = t / a.max_probe;
+  const int j = static_cast<int>(t % a.max_probe);
+  const int np = probes_of(a, q);
+  if (j == 0) a.list_count[q] = 2u * static_cast<uint32_t>(np);
+  if (j >= np) return;
+  const uint32_t b = a.probes[t];
+  if (b < static_cast<uint32_t>(a.nb)) atomicAdd(&a.counts[b], 1u);
+}
+
+__global__ void pair_scatter_kernel(PairArgs a) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= a.nq * a.max_probe) return;
+  const long long q = t / a.max_probe;
+  const int j = static_cast<int>(t % a.max_probe);
+  if (j >= probes_of(a, q)) return;
+  const uint32_t b = a.probes[t];
+  if (b >= static_cast<uint32_t>(a.nb)) return;
+  const unsigned long long pos = a.pair_start[b] + atomicAdd(&a.fill[b], 1u);
+  a.pairs[pos] = static_cast<uint32_t>(t);
+}
+
+// One warp per (query, probe): offset <q_hat, enc[b]>.
+__global__ void pair_offset_kernel(PairArgs a) {
+  const long long t = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
+  const int lane = threadIdx.x & 31;
+  if (t >= a.nq * a.max_probe) return;
+  const long long q = t / a.max_probe;
+  const int j = static_cast<int>(t % a.max_probe);
+  if (j >= probes_of(a, q)) return;
+  const uint32_t b = a.probes[t];
+  if (b >= static_cast<uint32_t>(a.nb)) return;
+  const float d = warp_dot(a.q_hat + q * a.dim, a.enc + static_cast<long long>(b) * a.dim, a.dim, lane);
+  if (lane == 0) a.offsets[t] = d;
+}
+
+__global__ void item_build_kernel(PairArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nb) return;
+  const unsigned long long c = a.pair_start[b + 1] - a.pair_start[b];
+  const unsigned long long i0 = a.item_start[b];
+  for (unsigned long long t = 0; t * kItemQueries < c; ++t) {
+    const unsigned long long first = a.pair_start[b] + t * kItemQueries;
+    const unsigned long long cnt = min(static_cast<unsigned long long>(kItemQueries), c - t * kItemQueries);
+    a.items[i0 + t] = make_uint4(static_cast<unsigned>(b), static_cast<unsigned>(first),
+                                 static_cast<unsigned>(cnt), 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bucket scan
+// ---------------------------------------------------------------------------
+constexpr int kBsWarps = 4;
+constexpr int kBsPrefetch = 4;
+constexpr int kBsBuf = 512;  // per-warp sort buffer: up to 256 new + 256 kept
+
+// j-th largest (1-based, j <= 8) of the lane's valid scores, -inf if fewer.
+__device__ __forceinline__ float lane_jth_largest(const float (&sc)[8], unsigned ok, int j) {
+  float v[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) v[t] = (ok >> t & 1u) ? sc[t] : -INFINITY;
+  // partial selection: j passes of max extraction
+  float out = -INFINITY;
+  for (int r = 0; r < j; ++r) {
+    int bi = 0;
+    float bv = v[0];
+#pragma unroll
+    for (int t = 1; t < 8; ++t) {
+      if (v[t] > bv) {
+        bv = v[t];
+        bi = t;
+      }
+    }
+    out = bv;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      if (t == bi) v[t] = -INFINITY;
+    }
+  }
+  return out;
+}
+
+template <bool NIBBLE8>
+__global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_q[kItemQueries];
+  __shared__ uint32_t s_pair[kItemQueries];
+  __shared__ float s_scale[kItemQueries], s_init[kItemQueries], s_off[kItemQueries];
+  if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
+  const uint4 it = a.items[blockIdx.x];
+  const int b = static_cast<int>(it.x);
+  const int pc = static_cast<int>(it.z);
+  const int nbg = a.nbg, k = a.k;
+  const int chunk = nbg < kFlushGroups ? nbg : kFlushGroups;
+  const bool resident = chunk >= nbg;
+  if (threadIdx.x < kItemQueries) {
+    const int t = threadIdx.x;
+    if (t < pc) {
+      const uint32_t pr = a.pairs[it.y + t];
+      const int q = static_cast<int>(pr / static_cast<uint32_t>(a.max_probe));
+      s_q[t] = q;
+      s_pair[t] = pr;
+      s_scale[t] = a.lut_scale[q];
+      s_init[t] = a.fa_init[q];
+      s_off[t] = a.offsets[pr];
+    } else {
+      s_q[t] = -1;
+      s_pair[t] = 0u;
+      s_scale[t] = 0.f;
+      s_init[t] = 0.f;
+      s_off[t] = 0.f;
+    }
+  }
+  __syncthreads();
+
+  LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [kItemQueries][chunk][2]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kmax = a.k <= 32 ? 32 : (a.k <= 64 ? 64 : 256);
+  // Per-warp top-k lists and sort buffer after the LUT area.
+  unsigned char* warp_area = smem + static_cast<size_t>(kItemQueries) * chunk * 32 +
+                             warp * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
+  float* list_s = reinterpret_cast<float*>(warp_area);
+  uint32_t* list_i = reinterpret_cast<uint32_t*>(list_s + 4 * kmax);
+  float* buf_s = reinterpret_cast<float*>(list_i + 4 * kmax);
+  uint32_t* buf_i = reinterpret_cast<uint32_t*>(buf_s + kBsBuf);
+
+  auto load_lut_chunk = [&](int g_first, int g_count) {
+    const int halves = g_count * 2;
+    for (int t = threadIdx.x; t < kItemQueries * halves; t += blockDim.x) {
+      const int q = t / halves, r = t % halves;
+      LutHalf h = {{0u, 0u, 0u, 0u}};
+      if (s_q[q] >= 0) {
+        h = *reinterpret_cast<const LutHalf*>(a.luts + (static_cast<long long>(s_q[q]) * nbg + g_first) * 32LL +
+                                              r * 16LL);
+      }
+      s_lut[q * chunk * 2 + r] = h;
+    }
+  };
+  if (resident) {
+    load_lut_chunk(0, nbg);
+    __syncthreads();
+  }
+
+  const int quad = warp & 1, tset = warp >> 1;
+  const bool quad_ok = quad * 4 < pc;
+  const unsigned long long slot0 = a.slot_start[b];
+  const int size = static_cast<int>(a.bucket_size[b]);
+  const int n_sub = (size + kBucketSlotAlign - 1) / kBucketSlotAlign;
+  float scale[4], init[4], off[4], thr_s[4];
+  uint32_t thr_i[4];
+  int cnt[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    scale[q] = s_scale[quad * 4 + q];
+    init[q] = s_init[quad * 4 + q];
+    off[q] = s_off[quad * 4 + q];
+    thr_s[q] = -FLT_MAX;
+    thr_i[q] = 0xffffffffu;
+    cnt[q] = 0;
+  }
+  const int j_rank = (k + 31) / 32;           // per-lane rank used by the prefilter
+  const int k_rank = (k + j_rank - 1) / j_rank;  // rank among the 32 lane values
+  constexpr long long kGroupStride = kTileWords / 2;  // uint2 per group row
+
+  const int rounds = (n_sub + 1) / 2;
+  for (int r = 0; r < rounds; ++r) {
+    const int st = tset + 2 * r;
+    const bool active = quad_ok && st < n_sub;
+    const long long sub = static_cast<long long>(slot0 / kBucketSlotAlign) + st;
+    const long long tile = sub >> 1;
+    const int half = static_cast<int>(sub & 1);
+    const uint2* wp = reinterpret_cast<const uint2*>(a.codes + tile * nbg * kTileWords + half * 64) + lane;
+    const long long vbase = sub * kBucketSlotAlign + 8 * lane;
+    float fa[4][8];
+    uint32_t acc[4][8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        fa[q][j] = init[q];
+        acc[q][j] = 0u;
+      }
+    for (int gb = 0; gb < nbg; gb += kFlushGroups) {
+      const int g_stop = min(gb + kFlushGroups, nbg);
+      if (!resident) {
+        __syncthreads();
+        load_lut_chunk(gb, g_stop - gb);
+        __syncthreads();
+      }
+      if (!active) continue;
+      const int chunk_base = resident ? 0 : gb;
+      uint2 ring[kBsPrefetch];
+#pragma unroll
+      for (int u = 0; u < kBsPrefetch; ++u) {
+        ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
+      }
+      for (int g = gb; g < g_stop; g += kBsPrefetch) {
+        uint2 cur[kBsPrefetch];
+#pragma unroll
+        for (int u = 0; u < kBsPrefetch; ++u) {
+          cur[u] = ring[u];
+          const int gn = g + kBsPrefetch + u;
+          ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+        }
+        // Groups in pairs (nbg and the 256-group batches are even).
+#pragma unroll
+        for (int u = 0; u < kBsPrefetch; u += 2) {
+          if (g + u >= g_stop) break;
+          const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
+          const uint32_t a0h = a0 >> 16, a1h = a1 >> 16, b0h = b0 >> 16, b1h = b1 >> 16;
+          uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
+          if constexpr (!NIBBLE8) {
+            ta0 = a0 ^ 0x88888888u;
+            ta1 = a1 ^ 0x88888888u;
+            tb0 = b0 ^ 0x88888888u;
+            tb1 = b1 ^ 0x88888888u;
+            ta0h = ta0 >> 16;
+            ta1h = ta1 >> 16;
+            tb0h = tb0 >> 16;
+            tb1h = tb1 >> 16;
+          }
+          const LutHalf* lg = s_lut + (quad * 4) * chunk * 2 + (g + u - chunk_base) * 2;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const LutHalf Fa = lg[q * chunk * 2];
+            const LutHalf Sa = lg[q * chunk * 2 + 1];
+            const LutHalf Fb = lg[q * chunk * 2 + 2];
+            const LutHalf Sb = lg[q * chunk * 2 + 3];
+            uint32_t lo0, hi0, lo1, hi1;
+            if constexpr (NIBBLE8) {
+              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sb.w[0], Sb.w[1], b0);
+              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fb.w[0], Fb.w[1], b0h);
+              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sb.w[0], Sb.w[1], b1);
+              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fb.w[0], Fb.w[1], b1h);
+            } else {
+              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sa.w[2], Sa.w[3], ta0) + prmt(Sb.w[0], Sb.w[1], b0) +
+                    prmt(Sb.w[2], Sb.w[3], tb0);
+              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fa.w[2], Fa.w[3], ta0h) + prmt(Fb.w[0], Fb.w[1], b0h) +
+                    prmt(Fb.w[2], Fb.w[3], tb0h);
+              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sa.w[2], Sa.w[3], ta1) + prmt(Sb.w[0], Sb.w[1], b1) +
+                    prmt(Sb.w[2], Sb.w[3], tb1);
+              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fa.w[2], Fa.w[3], ta1h) + prmt(Fb.w[0], Fb.w[1], b1h) +
+                    prmt(Fb.w[2], Fb.w[3], tb1h);
+            }
+            const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
+            const uint32_t m10 = prmt(lo1, hi1, 0x5140u), m11 = prmt(lo1, hi1, 0x7362u);
+            acc[q][0] = __dp4a(m00, 0x00000101u, acc[q][0]);
+            acc[q][1] = __dp4a(m00, 0x01010000u, acc[q][1]);
+            acc[q][2] = __dp4a(m01, 0x00000101u, acc[q][2]);
+            acc[q][3] = __dp4a(m01, 0x01010000u, acc[q][3]);
+            acc[q][4] = __dp4a(m10, 0x00000101u, acc[q][4]);
+            acc[q][5] = __dp4a(m10, 0x01010000u, acc[q][5]);
+            acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
+            acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
+          }
+        }
+      }
+      // f32 flush of this batch (search_avx2.cpp:24-48).
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          fa[q][j] = __fmaf_rn(scale[q], __uint2float_rn(acc[q][j]), fa[q][j]);
+          acc[q][j] = 0u;
+        }
+    }
+    if (!active) continue;  // warp-uniform; no CTA barrier follows in this round
+
+    float al[8];
+    uint32_t ids[8];
+    {
+      const float4 x0 = *reinterpret_cast<const float4*>(a.alpha + vbase);
+      const float4 x1 = *reinterpret_cast<const float4*>(a.alpha + vbase + 4);
+      al[0] = x0.x; al[1] = x0.y; al[2] = x0.z; al[3] = x0.w;
+      al[4] = x1.x; al[5] = x1.y; al[6] = x1.z; al[7] = x1.w;
+      const uint4 i0 = *reinterpret_cast<const uint4*>(a.slot_ids + vbase);
+      const uint4 i1 = *reinterpret_cast<const uint4*>(a.slot_ids + vbase + 4);
+      ids[0] = i0.x; ids[1] = i0.y; ids[2] = i0.z; ids[3] = i0.w;
+      ids[4] = i1.x; ids[5] = i1.y; ids[6] = i1.z; ids[7] = i1.w;
+    }
+    unsigned valid = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (vbase + j - static_cast<long long>(slot0) < size) valid |= 1u << j;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (quad * 4 + q >= pc) break;  // warp-uniform
+      float sc[8];
+      unsigned ok = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), off[q]);
+        if ((valid >> j & 1u) && sc[j] > -INFINITY) ok |= 1u << j;
+      }
+      unsigned pass = 0;
+      if (cnt[q] == k) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if ((ok >> j & 1u) && better(sc[j], ids[j], thr_s[q], thr_i[q])) pass |= 1u << j;
+        }
+      } else {
+        // At least k_rank lanes hold j_rank scores >= bound, i.e. >= k scores of
+        // this block are >= bound, so a score below it cannot be in the top-k.
+        const float mine = lane_jth_largest(sc, ok, j_rank);
+        const float bound = warp_kth_largest(mine, k_rank, lane);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if ((ok >> j & 1u) && !(sc[j] < bound)) pass |= 1u << j;
+        }
+      }
+      const int n_mine = __popc(pass);
+      int incl = n_mine;
+#pragma unroll
+      for (int o = 1; o < kWarp; o <<= 1) {
+        const int t = __shfl_up_sync(full_mask(), incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = __shfl_sync(full_mask(), incl, kWarp - 1);
+      if (total == 0) continue;
+      int pos = incl - n_mine;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (pass >> j & 1u) {
+          buf_s[pos] = sc[j];
+          buf_i[pos] = ids[j];
+          ++pos;
+        }
+      }
+      float* ls = list_s + q * kmax;
+      uint32_t* li = list_i + q * kmax;
+      for (int t = lane; t < cnt[q]; t += kWarp) {
+        buf_s[total + t] = ls[t];
+        buf_i[total + t] = li[t];
+      }
+      const int tot = total + cnt[q];
+      int p = 32;
+      while (p < tot) p <<= 1;
+      for (int t = tot + lane; t < p; t += kWarp) {
+        buf_s[t] = -INFINITY;
+        buf_i[t] = 0xffffffffu;
+      }
+      __syncwarp();
+      warp_sort_best_first(buf_s, buf_i, p, lane);
+      const int keep = min(k, tot);
+      for (int t = lane; t < keep; t += kWarp) {
+        ls[t] = buf_s[t];
+        li[t] = buf_i[t];
+      }
+      cnt[q] = keep;
+      if (keep == k) {
+        thr_s[q] = buf_s[k - 1];
+        thr_i[q] = buf_i[k - 1];
+      }
+      __syncwarp();
+    }
+  }
+  // Publish: list (pair * 2 + tile set) of every valid query of this warp.
+  if (!quad_ok) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    if (quad * 4 + q >= pc) break;
+    const long long list = static_cast<long long>(s_pair[quad * 4 + q]) * 2 + tset;
+    float* os = a.cand_score + list * k;
+    uint32_t* oi = a.cand_id + list * k;
+    for (int t = lane; t < k; t += kWarp) {
+      const bool have = t < cnt[q];
+      os[t] = have ? list_s[q * kmax + t] : -INFINITY;
+      oi[t] = have ? list_i[q * kmax + t] : 0xffffffffu;
+    }
+  }
+}
+
+__global__ void relabel_kernel(uint32_t* __restrict__ label, long long n, const uint32_t* __restrict__ remap) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) label[i] = remap[label[i]];
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ src, const uint32_t* __restrict__ rows, long long n,
+                                   int dim, float* __restrict__ dst) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n * dim) return;
+  const long long r = i / dim;
+  dst[i] = src[static_cast<long long>(rows[r]) * dim + (i % dim)];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+cudaError_t launch_normalize_rows(const float* x, long long n, int dim_in, int dim, float* out,
+                                  cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const long long threads = n * kWarp;
+  normalize_rows_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, stream>>>(x, n, dim_in, dim, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_nt(const float* A, long long m, const float* B, long long nb, int dim, float* C,
+                           long long ldc, cudaStream_t stream) {
+  if (m == 0 || nb == 0) return cudaSuccess;
+  dim3 grid(static_cast<unsigned>((nb + kTileB - 1) / kTileB), static_cast<unsigned>((m + kTile - 1) / kTile));
+  if (grid.y > 65535) return cudaErrorInvalidValue;
+  gemm_nt_kernel<<<grid, 256, 0, stream>>>(A, m, B, nb, dim, C, ldc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assign(const float* A, long long m, const float* B, long long nb, int dim, uint32_t* label,
+                          float* best, cudaStream_t stream) {
+  if (m == 0) return cudaSuccess;
+  assign_kernel<<<static_cast<unsigned>((m + kTile - 1) / kTile), 256, 0, stream>>>(A, m, B, nb, dim, label, best);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_select_top(const float* S, long long rows, long long ld, int ncols, int p, float* out_s,
+                              uint32_t* out_i, cudaStream_t stream) {
+  if (rows == 0) return cudaSuccess;
+  if (p < 1 || p > 256) return cudaErrorInvalidValue;
+  select_top_kernel<<<static_cast<unsigned>(rows), kSelThreads, 0, stream>>>(S, ld, ncols, p, out_s, out_i);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_group_by_label(const uint32_t* label, long long n, int nb, uint32_t* counts,
+                                  unsigned long long* starts, uint32_t* fill, uint32_t* members,
+                                  cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(counts, 0, static_cast<size_t>(nb) * 4, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(fill, 0, static_cast<size_t>(nb) * 4, stream);
+  if (e != cudaSuccess) return e;
+  if (n > 0) {
+    label_hist_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(label, n, counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  prefix_kernel<<<1, 1024, 0, stream>>>(counts, nb, starts, 0, nullptr, nullptr);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (n > 0) {
+    label_scatter_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(label, n, starts, fill,
+                                                                                      members);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort_groups(const unsigned long long* starts, int nb, int max_group, uint32_t* members,
+                               cudaStream_t stream) {
+  if (nb == 0) return cudaSuccess;
+  if (max_group > 8192) return cudaErrorInvalidValue;
+  int p = 2;
+  while (p < max_group) p <<= 1;
+  const size_t smem = static_cast<size_t>(p) * 4;
+  cudaError_t e = cudaFuncSetAttribute(sort_groups_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  sort_groups_kernel<<<nb, 512, smem, stream>>>(starts, members);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_centroids(const float* X, int dim, const unsigned long long* starts, const uint32_t* members,
+                             int nb, long long* acc, float* enc, float* route, cudaStream_t stream) {
+  if (nb == 0) return cudaSuccess;
+  if (dim > kCentMaxDim) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(acc, 0, static_cast<size_t>(nb) * dim * 8, stream);
+  if (e != cudaSuccess) return e;
+  centroid_sum_kernel<<<dim3(nb, kCentSplit), kCentThreads, 0, stream>>>(X, dim, starts, members, acc);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const long long threads = static_cast<long long>(nb) * kWarp;
+  centroid_finish_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, stream>>>(acc, dim, nb, starts,
+                                                                                            enc, route);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split(const float* X, int dim, const unsigned long long* starts, const uint32_t* members,
+                         const uint32_t* groups, const uint32_t* new_label, int n_groups, const float* route,
+                         uint32_t* label, bool force_bits, cudaStream_t stream) {
+  if (n_groups == 0) return cudaSuccess;
+  const size_t smem = static_cast<size_t>(dim) * (4 + 4 + 8 + 8);
+  cudaError_t e = cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  split_kernel<<<n_groups, kSplitThreads, smem, stream>>>(X, dim, starts, members, groups, new_label, route, label,
+                                                          force_bits ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_build_residuals(const float* X, int dim, const unsigned long long* starts,
+                                   const uint32_t* members, int nb, const unsigned long long* slot_start,
+                                   const float* enc, long long n_slots, float* R, uint32_t* slot_ids,
+                                   cudaStream_t stream) {
+  (void)n_slots;
+  if (nb == 0) return cudaSuccess;
+  build_residuals_kernel<<<nb, 256, 0, stream>>>(X, dim, starts, members, slot_start, enc, R, slot_ids);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_rows(const float* X, long long n, int dim, const uint32_t* label, const float* enc,
+                                 float* R, cudaStream_t stream) {
+  const long long total = n * dim;
+  if (total == 0) return cudaSuccess;
+  residual_rows_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(X, n, dim, label, enc, R);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_relabel(uint32_t* label, long long n, const uint32_t* remap, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  relabel_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(label, n, remap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const float* src, const uint32_t* rows, long long n_rows, int dim, float* dst,
+                               cudaStream_t stream) {
+  const long long total = n_rows * dim;
+  if (total == 0) return cudaSuccess;
+  gather_rows_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(src, rows, n_rows, dim, dst);
+  return cudaGetLastError();
+}
+
+long long max_items(long long nq, int max_probe, int nb) {
+  return (nq * max_probe + kItemQueries - 1) / kItemQueries + nb;
+}
+
+cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(a.counts, 0, static_cast<size_t>(a.nb) * 4, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(a.fill, 0, static_cast<size_t>(a.nb) * 4, stream);
+  if (e != cudaSuccess) return e;
+  const long long total = a.nq * a.max_probe;
+  if (total > 0) {
+    pair_count_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  prefix_kernel<<<1, 1024, 0, stream>>>(a.counts, a.nb, a.pair_start, kItemQueries, a.item_start, a.n_items);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (total > 0) {
+    pair_scatter_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    pair_offset_kernel<<<static_cast<unsigned>((total * kWarp + 255) / 256), 256, 0, stream>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  item_build_kernel<<<static_cast<unsigned>((a.nb + 255) / 256), 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream) {
+  if (grid <= 0) return cudaSuccess;
+  if (a.k < 1 || a.k > kMaxK) return cudaErrorInvalidValue;
+  const int chunk = a.nbg < kFlushGroups ? a.nbg : kFlushGroups;
+  const int kmax = a.k <= 32 ? 32 : (a.k <= 64 ? 64 : 256);
+  const size_t smem = static_cast<size_t>(kItemQueries) * chunk * 32 +
+                      static_cast<size_t>(kBsWarps) * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
+  cudaError_t e;
+  if (a.bits == 3) {
+    e = cudaFuncSetAttribute(bucket_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    bucket_scan_kernel<true><<<static_cast<unsigned>(grid), kBsWarps * 32, smem, stream>>>(a);
+  } else {
+    e = cudaFuncSetAttribute(bucket_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    bucket_scan_kernel<false><<<static_cast<unsigned>(grid), kBsWarps * 32, smem, stream>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace vcb

@@ -1,0 +1,138 @@
+// Launch interfaces of the bucketed (IVF) index kernels (tq_bucket.cu).
+//
+// Build: spherical k-means (fp32 routing contraction + argmax), deterministic
+// fixed-point centroid sums, 2-means fission of oversized buckets, and the
+// bucket-ordered slot layout of residual rows. Search: query routing scores,
+// top-n_probe selection, (query, bucket) pairs grouped by bucket into work
+// items, and the bucket scan: FastScan over each probed bucket's residual codes
+// with the per-(query, bucket) offset <q_hat, encode_c> (score_prepared_into,
+// search.cpp:1156-1264).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vcb {
+
+// A bucket starts at a multiple of this many slots: one scan warp covers 256
+// vectors (32 lanes x 8), i.e. one half of a 512-vector scan-layout tile.
+constexpr int kBucketSlotAlign = 256;
+// Queries per bucket-scan work item (two groups of four, one per warp pair).
+constexpr int kItemQueries = 8;
+// Fixed-point scale of the deterministic centroid sums (|x| <= 1 per coordinate).
+constexpr double kFixedScale = 4294967296.0;  // 2^32
+
+// Rows scaled to unit L2 norm and zero-padded from dim_in to dim columns (dim >=
+// dim_in). Rows with norm below 1e-30 become zero rows.
+cudaError_t launch_normalize_rows(const float* x, long long n, int dim_in, int dim, float* out,
+                                  cudaStream_t stream);
+
+// C (m x nb, row stride ldc) = A (m x dim) . B (nb x dim)^T in fp32 with fused
+// multiply-add accumulation over the coordinates in order.
+cudaError_t launch_gemm_nt(const float* A, long long m, const float* B, long long nb, int dim, float* C,
+                           long long ldc, cudaStream_t stream);
+
+// Per row of A: the column of the largest A.B^T entry (ties: lower column) and
+// its value. Same arithmetic as launch_gemm_nt.
+cudaError_t launch_assign(const float* A, long long m, const float* B, long long nb, int dim,
+                          uint32_t* label, float* best, cudaStream_t stream);
+
+// Per row of S (row stride ld, ncols valid columns): the top p entries, score
+// descending, equal scores by lower column; p <= 256. Rows with fewer than p
+// columns are padded with (-inf, 0xffffffff).
+cudaError_t launch_select_top(const float* S, long long rows, long long ld, int ncols, int p, float* out_s,
+                              uint32_t* out_i, cudaStream_t stream);
+
+// Counting sort of labels: counts[nb] (zeroed inside), starts[nb + 1]
+// (exclusive prefix; starts[nb] = total), members[n] (row ids grouped by label,
+// in no particular order inside a group). fill[nb] is scratch.
+cudaError_t launch_group_by_label(const uint32_t* label, long long n, int nb, uint32_t* counts,
+                                  unsigned long long* starts, uint32_t* fill, uint32_t* members,
+                                  cudaStream_t stream);
+
+// Sorts every group's members ascending (groups of at most `max_group` rows,
+// max_group <= 8192).
+cudaError_t launch_sort_groups(const unsigned long long* starts, int nb, int max_group, uint32_t* members,
+                               cudaStream_t stream);
+
+// Deterministic centroids: sums in 2^32 fixed point (exact, order-free) of the
+// member rows of X; enc[b] = mean (fp32), route[b] = mean / ||mean||. Empty
+// groups keep their previous centroids. acc is nb * dim int64 scratch.
+cudaError_t launch_centroids(const float* X, int dim, const unsigned long long* starts, const uint32_t* members,
+                             int nb, long long* acc, float* enc, float* route, cudaStream_t stream);
+
+// One 2-means split of each listed group: seeds are the member least aligned
+// with the group's routing centroid and the member least aligned with that
+// seed; members go to the closer seed, the two means are formed, and members go
+// to the closer mean. Members on the second side get label new_label[t]. A
+// split that leaves one side empty, or any split when force_bits is set,
+// divides the members by the lowest id bit that differs among them (an
+// arbitrary but balanced-in-expectation halving that always makes progress).
+cudaError_t launch_split(const float* X, int dim, const unsigned long long* starts, const uint32_t* members,
+                         const uint32_t* groups, const uint32_t* new_label, int n_groups, const float* route,
+                         uint32_t* label, bool force_bits, cudaStream_t stream);
+
+// Slot layout: residual rows R[slot] = X[id] - enc[b] for the members of every
+// bucket at slot_start[b] + rank (members sorted), zero rows in the padding;
+// slot_ids[slot] = id or 0xffffffff.
+cudaError_t launch_build_residuals(const float* X, int dim, const unsigned long long* starts,
+                                   const uint32_t* members, int nb, const unsigned long long* slot_start,
+                                   const float* enc, long long n_slots, float* R, uint32_t* slot_ids,
+                                   cudaStream_t stream);
+
+// Residuals of arbitrary rows against the encode centroid of their label.
+cudaError_t launch_residual_rows(const float* X, long long n, int dim, const uint32_t* label, const float* enc,
+                                 float* R, cudaStream_t stream);
+
+// label[i] = remap[label[i]] for n labels.
+cudaError_t launch_relabel(uint32_t* label, long long n, const uint32_t* remap, cudaStream_t stream);
+// dst[r] = src[rows[r]] for n_rows rows of dim floats.
+cudaError_t launch_gather_rows(const float* src, const uint32_t* rows, long long n_rows, int dim, float* dst,
+                               cudaStream_t stream);
+
+struct PairArgs {
+  const uint32_t* probes;    // nq x max_probe bucket ids (routing order)
+  const uint32_t* n_probe;   // per query, or nullptr: every query probes `fixed_probe`
+  int fixed_probe;
+  int max_probe;
+  long long nq;
+  int nb;
+  const float* q_hat;        // nq x dim
+  const float* enc;          // nb x dim encode centroids
+  int dim;
+  // outputs / scratch (device)
+  uint32_t* counts;          // nb
+  unsigned long long* pair_start;  // nb + 1
+  unsigned long long* item_start;  // nb + 1
+  uint32_t* fill;            // nb
+  uint32_t* pairs;           // nq * max_probe: q * max_probe + j, grouped by bucket
+  float* offsets;            // nq * max_probe: <q_hat, enc[probe]>
+  uint4* items;              // (bucket, first pair, pair count, 0)
+  unsigned long long* n_items;
+  uint32_t* list_count;      // nq: 2 * n_probe (candidate lists per query)
+};
+// Groups the (query, probe) pairs by bucket and builds the scan work items.
+cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);
+long long max_items(long long nq, int max_probe, int nb);
+
+struct BucketScanArgs {
+  const uint32_t* codes;     // scan layout over slots
+  const float* alpha;        // per slot
+  const uint32_t* slot_ids;  // per slot: original id
+  const unsigned long long* slot_start;  // per bucket (multiple of kBucketSlotAlign)
+  const uint32_t* bucket_size;
+  const uint8_t* luts;       // nq x nbg x 32
+  const float* lut_scale;
+  const float* fa_init;
+  const uint32_t* pairs;
+  const float* offsets;
+  const uint4* items;
+  const unsigned long long* n_items;
+  int nbg, bits, k, max_probe;
+  float* cand_score;         // (nq * max_probe * 2) lists of k
+  uint32_t* cand_id;
+};
+cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
+
+}  // namespace vcb

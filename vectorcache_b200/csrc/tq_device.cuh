@@ -160,4 +160,50 @@ __device__ __forceinline__ bool better(float sa, uint32_t ia, float sb, uint32_t
   return (sa > sb) || (sa == sb && ia < ib);
 }
 
+
+// 16 bytes of a query LUT (one nibble's 16 entries of one byte group).
+struct __align__(16) LutHalf {
+  uint32_t w[4];
+};
+
+// Warp-cooperative bitonic sort of p (a power of two) entries in
+// shared memory, best first under `better`.
+__device__ __forceinline__ void warp_sort_best_first(float* s, uint32_t* id, int p, int lane) {
+  for (int size = 2; size <= p; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = lane; t < (p >> 1); t += kWarp) {
+        const int i = (t / stride) * 2 * stride + (t % stride);
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const float si = s[i], sj = s[j];
+        const uint32_t ii = id[i], ij = id[j];
+        if (better(sj, ij, si, ii) == up) {
+          s[i] = sj;
+          s[j] = si;
+          id[i] = ij;
+          id[j] = ii;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// k-th largest of the 32 lane values (k <= 32), by a shuffle bitonic sort.
+__device__ __forceinline__ float warp_kth_largest(float v, int k, int lane) {
+#pragma unroll
+  for (int size = 2; size <= kWarp; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const float o = __shfl_xor_sync(full_mask(), v, stride);
+      const bool lower = (lane & stride) == 0;
+      const bool desc = (lane & size) == 0;  // final pass: descending everywhere
+      // keep the larger value in the lower lane of a descending block
+      const bool take_max = (lower == desc);
+      v = take_max ? fmaxf(v, o) : fminf(v, o);
+    }
+  }
+  return __shfl_sync(full_mask(), v, k - 1);
+}
+
 }  // namespace vcb

@@ -103,6 +103,9 @@ struct MergeArgs {
   int k_out;     // k_eff = min(k, n)
   float* out_score;     // nq x k_out
   uint64_t* out_id;
+  // Optional: lists actually filled per query (the first list_count[q] of its
+  // n_lists); nullptr means all n_lists.
+  const uint32_t* list_count = nullptr;
 };
 
 size_t encode_smem_bytes(int dim, bool tqplus);

@@ -31,50 +31,6 @@ constexpr int kMergeBuf = 512;  // per-warp sort buffer: 256 new + up to 256 kep
 constexpr int kPrefetch = 4;    // byte groups of codes in flight per thread
 constexpr int kRegTopK = 32;    // k up to this is kept in registers, one entry per lane
 
-struct __align__(16) LutHalf {
-  uint32_t w[4];
-};
-
-// Warp-cooperative bitonic sort of p (power of two, <= kMergeBuf) entries in
-// shared memory, best first under `better`.
-__device__ __forceinline__ void warp_sort_best_first(float* s, uint32_t* id, int p, int lane) {
-  for (int size = 2; size <= p; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = lane; t < (p >> 1); t += kWarp) {
-        const int i = (t / stride) * 2 * stride + (t % stride);
-        const int j = i + stride;
-        const bool up = (i & size) == 0;
-        const float si = s[i], sj = s[j];
-        const uint32_t ii = id[i], ij = id[j];
-        if (better(sj, ij, si, ii) == up) {
-          s[i] = sj;
-          s[j] = si;
-          id[i] = ij;
-          id[j] = ii;
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
-// k-th largest of the 32 lane values (k <= 32), by a shuffle bitonic sort.
-__device__ __forceinline__ float warp_kth_largest(float v, int k, int lane) {
-#pragma unroll
-  for (int size = 2; size <= kWarp; size <<= 1) {
-#pragma unroll
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      const float o = __shfl_xor_sync(full_mask(), v, stride);
-      const bool lower = (lane & stride) == 0;
-      const bool desc = (lane & size) == 0;  // final pass: descending everywhere
-      // keep the larger value in the lower lane of a descending block
-      const bool take_max = (lower == desc);
-      v = take_max ? fmaxf(v, o) : fminf(v, o);
-    }
-  }
-  return __shfl_sync(full_mask(), v, k - 1);
-}
-
 // Running top-k of one warp for one query, one entry per lane (k <= 32),
 // sorted best first; empty slots hold (-inf, 0xffffffff).
 struct RegTopK {
@@ -473,9 +429,11 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   __shared__ uint32_t best_i[kMaxK];
   __shared__ int n_new;
   const long long qi = blockIdx.x;
-  const long long total = static_cast<long long>(a.n_lists) * a.k;
-  const float* cs = a.cand_score + qi * total;
-  const uint32_t* ci = a.cand_id + qi * total;
+  const long long stride = static_cast<long long>(a.n_lists) * a.k;
+  const long long total = (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
+                                        : static_cast<long long>(a.n_lists)) * a.k;
+  const float* cs = a.cand_score + qi * stride;
+  const uint32_t* ci = a.cand_id + qi * stride;
   const int kout = a.k_out;
   int nbest = 0;
   float thr_s = -FLT_MAX;
