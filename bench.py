@@ -53,6 +53,13 @@ def parse():
     p.add_argument("--recall-queries", type=int, default=1000)
     p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["flat", "bucketed"], default="flat",
+                   help="flat: the 1M x 1536 flat search (default); bucketed: the 1.2M x 100 bucketed index, "
+                        "learned n_probe against fixed n_probe = 64")
+    p.add_argument("--bucketed-n", type=int, default=1_200_000)
+    p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
+    p.add_argument("--rerank", type=int, default=100, help="bucketed: candidates re-ranked exactly (0 = off)")
+    p.add_argument("--epochs", type=int, default=30)
     return p.parse_args()
 
 
@@ -457,8 +464,163 @@ def run_ours(args, world, rank, local):
     index.close()
 
 
+BUCKETED_METRIC = "QPS at Recall@10 >= 0.95 (bucketed 1.2Mx100 4-bit cosine, learned n_probe vs fixed n_probe)"
+PROBE_CLASSES = (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048)
+FIXED_PROBES = (64, 128, 256, 384, 512, 768, 1024, 1536, 2048)
+RECALL_TARGET = 0.95
+
+
+def run_bucketed(args, world, rank, local):
+    """The bucketed index workload: a von Mises-Fisher mixture (2000 clusters,
+    kappa log-uniform in [20, 200], Zipf(1.1) sizes), dim 100, 4-bit, cosine;
+    max_bucket_size 800, energy_soft 400, expected_n = corpus size. One step =
+    one search of 10,000 queries (k = 10). The plain path scans the fixed
+    n_probe = 64 best-routed buckets; the learned path routes, runs the probe
+    MLP (trained here on the GPU on labels the plain index generates against
+    exact top-10 for 50,000 training queries) and scans each query's predicted
+    number of buckets. Both re-rank their top `--rerank` candidates exactly."""
+    import torch
+
+    import vectorcache_b200 as vcb
+    from vectorcache_b200.probe import ProbeMLP, probe_labels, recall_rows
+    from vectorcache_b200.synthetic import vmf_mixture
+
+    if world > 1:
+        raise SystemExit("--workload bucketed runs on one GPU")
+    device = torch.device("cuda", local)
+    dim, n, nq, k = 100, args.bucketed_n, args.nq, 10
+    t0 = time.perf_counter()
+    db = vmf_mixture(n, dim, seed=31)
+    test_q = vmf_mixture(nq, dim, seed=32)
+    train_q = vmf_mixture(args.bucketed_train, dim, seed=33)
+    gen_s = time.perf_counter() - t0
+    params = vcb.BucketParams(n_probe=64, max_bucket_size=800, energy_soft=400, expected_n=n, rerank_k=args.rerank)
+    idx = vcb.BucketedTurboQuantIndex(dim, 4, params, device=local)
+    idx.add(db)
+    t0 = time.perf_counter()
+    idx.prepare()
+    build_s = time.perf_counter() - t0
+    info = idx.info()
+
+    # exact top-10 (fp32 brute force on the normalized rows, no TF32)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    x = torch.from_numpy(db).to(device)
+    x = x / torch.linalg.vector_norm(x, dim=1, keepdim=True)
+
+    def exact(q):
+        out = []
+        for s in range(0, q.shape[0], 4096):
+            qq = torch.from_numpy(q[s:s + 4096]).to(device)
+            qq = qq / torch.linalg.vector_norm(qq, dim=1, keepdim=True)
+            out.append(torch.topk(qq @ x.T, k, dim=1).indices.cpu().numpy())
+        return np.concatenate(out)
+
+    ex_test, ex_train = exact(test_q), exact(train_q)
+    del x
+    torch.cuda.empty_cache()
+
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    d_q = torch.from_numpy(test_q).to(device)
+    d_s = torch.empty((nq, k), dtype=torch.float32, device=device)
+    d_i = torch.empty((nq, k), dtype=torch.int64, device=device)
+
+    def timed(step_fn):
+        for _ in range(args.warmup):
+            step_fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    # The plain path at fixed n_probe: QPS and Recall@10 per n_probe; the
+    # operating point is the smallest n_probe reaching the recall target.
+    sweep = {}
+    for p in FIXED_PROBES:
+        ms = timed(lambda p=p: idx.search_device(d_q, k, d_s, d_i, n_probe=p, stream=stream))
+        sweep[p] = {"n_probe": p, "ms_per_step": ms, "qps": nq / (ms / 1e3),
+                    "recall_at_10": float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())}
+    reach = [p for p in FIXED_PROBES if sweep[p]["recall_at_10"] >= RECALL_TARGET]
+    p_op = reach[0] if reach else FIXED_PROBES[-1]
+    fixed = sweep[p_op]
+    recall_fixed = fixed["recall_at_10"]
+    fixed_ms = fixed["ms_per_step"]
+    classes = tuple(c for c in PROBE_CLASSES if c <= p_op)
+
+    # labels from the plain index (reference n_probe = the operating point) and GPU training
+    t0 = time.perf_counter()
+    labels, rec = probe_labels(lambda q, p: idx.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
+    label_s = time.perf_counter() - t0
+    mlp = ProbeMLP(classes=classes, hidden=128, layers=2, seed=17, device=local)
+    d_train = torch.from_numpy(train_q).to(device)
+    tr_s = torch.empty((train_q.shape[0], 256), dtype=torch.float32, device=device)
+    tr_i = torch.empty((train_q.shape[0], 256), dtype=torch.int32, device=device)
+    idx.route_device(d_train, 256, tr_s, tr_i, stream=stream)
+    torch.cuda.synchronize()
+    raw = mlp.features(tr_s.cpu().numpy())
+    mlp.set_normalization(raw.mean(axis=0), raw.std(axis=0) + 1e-6)
+    d_lab = torch.from_numpy(labels.astype(np.int32)).to(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(5)
+    t0 = time.perf_counter()
+    losses = []
+    for epoch in range(args.epochs):
+        perm = torch.randperm(train_q.shape[0], device=device, generator=gen)
+        for s in range(0, train_q.shape[0], 512):
+            sel = perm[s:s + 512]
+            losses.append(mlp.train_step_device(tr_s[sel].contiguous(), d_lab[sel].contiguous(), sel.numel(), 256,
+                                                2e-3))
+    train_s = time.perf_counter() - t0
+
+    te_s = torch.empty((nq, 256), dtype=torch.float32, device=device)
+    te_i = torch.empty((nq, 256), dtype=torch.int32, device=device)
+    npq = torch.empty(nq, dtype=torch.int32, device=device)
+    best = None
+    learned_sweep = []
+    for cov in (0.5, 0.7, 0.8, 0.9, 0.95, 0.98):
+        def learned_step(cov=cov):
+            idx.route_device(d_q, 256, te_s, te_i, stream=stream)
+            mlp.predict_device(te_s, nq, 256, npq, coverage=cov, min_confidence=0.0, fallback=p_op, stream=stream)
+            idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, d_n_probe=npq, stream=stream)
+
+        ms = timed(learned_step)
+        r = float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())
+        mean_probe = float(npq.float().mean().item())
+        cand = {"coverage": cov, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
+                "mean_n_probe": mean_probe}
+        learned_sweep.append(cand)
+        if r >= min(RECALL_TARGET, recall_fixed) and (best is None or cand["qps"] > best["qps"]):
+            best = cand
+    qps_fixed = nq / (fixed_ms / 1e3)
+    line = {
+        "metric": BUCKETED_METRIC, "value": best["qps"] if best else None, "unit": "queries/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"bucketed TurboQuant {n}x{dim} 4-bit cosine vMF mixture, k={k}, {nq} queries per "
+                               f"step, rerank {args.rerank}",
+                   "n_buckets": info["n_buckets"], "n_slots": info["n_slots"], "build_s": build_s, "gen_s": gen_s,
+                   "label_s": label_s, "train_s": train_s, "train_queries": train_q.shape[0],
+                   "label_histogram": np.bincount(labels, minlength=len(classes)).tolist(),
+                   "classes": list(classes), "final_loss": float(np.mean(losses[-50:])),
+                   "recall_target": RECALL_TARGET},
+        "fixed": fixed, "learned": best, "speedup_vs_fixed": (best["qps"] / qps_fixed) if best else None,
+        "fixed_sweep": list(sweep.values()), "learned_sweep": learned_sweep,
+    }
+    print(json.dumps(line), flush=True)
+    mlp.close()
+    idx.close()
+
+
 def main():
     args = parse()
+    if args.workload == "bucketed":
+        world, rank, local = dist_setup(args)
+        run_bucketed(args, world, rank, local)
+        return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

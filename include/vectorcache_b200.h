@@ -209,10 +209,15 @@ int tq_index_read_profile(tq_index* h, tq_profile* out);
  * spherical k-means, then 2-means fission of every bucket above
  * max_bucket_size; it is deterministic for a given seed. */
 typedef struct tq_bucket_params {
-  uint32_t n_probe;         /* buckets scanned per query by default (64), <= 256 */
+  uint32_t n_probe;         /* buckets scanned per query by default (64), <= 2048 */
   uint32_t max_bucket_size; /* hard cap; larger buckets are split (800), <= 8192 */
   uint32_t energy_soft;     /* target mean bucket size of the initial partition (400) */
   uint32_t kmeans_iters;    /* spherical k-means rounds of the initial partition (4) */
+  uint32_t rerank_k;        /* 0: off (default). > k: the scan keeps rerank_k candidates,
+                               re-scored with the exact float <q_hat, x_hat> (the
+                               reference's float_rescore_topk order,
+                               src/search/float_rescore.cpp:80-164); top k returned */
+  uint32_t reserved;        /* 0 */
   uint64_t expected_n;      /* corpus size the partition is sized for; 0 = rows at prepare() */
   uint64_t seed;            /* seed of the initial centroid choice */
 } tq_bucket_params;
@@ -245,7 +250,7 @@ int tq_bucketed_search(tq_bucketed* h, const float* queries, size_t nq, size_t k
 int tq_bucketed_search_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t k,
                               size_t n_probe, const uint32_t* d_n_probe, float* d_scores,
                               uint64_t* d_ids, size_t* k_eff, void* stream);
-/* Routing only: the top p (<= 256) buckets per query and their scores
+/* Routing only: the top p (<= 2048) buckets per query and their scores
  * <q_hat, routing centroid>, best first (device buffers nq x p). */
 int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t p,
                              float* d_top_scores, uint32_t* d_top_ids, void* stream);

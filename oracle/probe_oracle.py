@@ -1,0 +1,76 @@
+"""Test infrastructure only — the CPU checker of the learned n_probe MLP.
+
+The MLP has no counterpart in the reference, so this checker is not pinned to
+reference code: it restates the network's definition (vectorcache_b200
+tq_probe.cu) in float64 numpy with the same bf16 rounding points — inputs,
+weights and hidden activations are rounded to bf16 exactly where the GPU
+rounds them — and computes the mean softmax cross-entropy and its gradients
+by explicit backpropagation. Only tests/ import it.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def bf16(x) -> np.ndarray:
+    """Round float32 values to the nearest bfloat16 (ties to even), returned as
+    float32 (finite inputs)."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return r.astype(np.uint32).view(np.float32)
+
+
+def unpack(params: np.ndarray, shapes):
+    out, off = [], 0
+    for fi, fo in shapes:
+        w = params[off:off + fi * fo].reshape(fi, fo)
+        off += fi * fo
+        b = params[off:off + fo]
+        off += fo
+        out.append((w, b))
+    return out
+
+
+def inputs(raw: np.ndarray, mean: np.ndarray, std: np.ndarray) -> np.ndarray:
+    """Standardized bf16 inputs: bf16(fp32(fp32(raw - mean) * fp32(1 / std)))."""
+    isd = np.where(std > np.float32(1e-12), np.float32(1.0) / std.astype(np.float32), np.float32(0.0))
+    v = (raw.astype(np.float32) - mean.astype(np.float32)).astype(np.float32) * isd.astype(np.float32)
+    return bf16(v.astype(np.float32))
+
+
+def forward_backward(x: np.ndarray, params: np.ndarray, shapes, labels: np.ndarray, rounding: bool = True):
+    """x: bf16-valued inputs (m x 512). Returns (loss, grads float64, logits).
+    rounding=False drops the bf16 rounding (float64 throughout) for
+    finite-difference checks of the backpropagation itself."""
+    rnd = bf16 if rounding else (lambda a: np.asarray(a, np.float64))
+    layers = unpack(params if not rounding else params.astype(np.float32), shapes)
+    m = x.shape[0]
+    acts = [x.astype(np.float64)]
+    zs = []
+    h = acts[0]
+    for li, (w, b) in enumerate(layers):
+        z = h @ rnd(w).astype(np.float64) + b.astype(np.float64)
+        zs.append(z)
+        if li + 1 < len(layers):
+            h = rnd(np.maximum(z, 0.0).astype(np.float32) if rounding else np.maximum(z, 0.0)).astype(np.float64)
+            acts.append(h)
+    logits = zs[-1]
+    mx = logits.max(axis=1, keepdims=True)
+    e = np.exp(logits - mx)
+    p = e / e.sum(axis=1, keepdims=True)
+    loss = float(np.mean(np.log(e.sum(axis=1)) - (logits[np.arange(m), labels] - mx[:, 0])))
+    dz = p.copy()
+    dz[np.arange(m), labels] -= 1.0
+    dz /= m
+    grads = []
+    for li in range(len(layers) - 1, -1, -1):
+        w, _ = layers[li]
+        gw = acts[li].T @ dz
+        gb = dz.sum(axis=0)
+        grads.append((gw, gb))
+        if li > 0:
+            da = dz @ rnd(w).astype(np.float64).T
+            dz = da * (zs[li - 1] > 0)
+    grads.reverse()
+    flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads])
+    return loss, flat, logits

@@ -142,6 +142,32 @@ def test_search_matches_oracle(oracle, small, bits, k, tq):
 
 
 @pytest.mark.gpu
+def test_rerank_matches_oracle(oracle, small):
+    # rerank_k: the scan's top rerank_k candidates, re-scored with the exact
+    # float <q_hat, x_hat> in the reference's float_rescore_topk order, top k kept.
+    from oracle.oracle import oracle_float_rescore
+
+    db, q, params = small
+    p = vcb.BucketParams(**{**params.__dict__, "rerank_k": 40})
+    idx = _build(db, 4, p)
+    eng = idx.engine()
+    lay = idx.layout()
+    tr = idx.search_trace(q, 40)  # the scan's top-40 (k >= rerank_k: no re-rank)
+    res = idx.search(q, 10)       # re-ranked top-10
+    prep = oracle.prepare_queries(tr["q_hat"], 4)
+    n_probe = np.full(q.shape[0], tr["probes"].shape[1], np.uint32)
+    ns = idx.info()["n_slots"]
+    ws, wi = oracle.ivf_search(prep, eng.codes_flat()[:ns], eng.alpha()[:ns], lay["slot_ids"].astype(np.uint64),
+                               lay["slot_start"].astype(np.int64), lay["bucket_size"].astype(np.int64), tr["probes"],
+                               n_probe, tr["offsets"], 40)
+    assert np.array_equal(tr["ids"], wi)
+    rs, ri = oracle_float_rescore(oracle, tr["q_hat"], idx.rows(), wi)
+    assert np.array_equal(res.ids, ri[:, :10])
+    assert bits_equal(res.scores, rs[:, :10])
+    idx.close()
+
+
+@pytest.mark.gpu
 def test_per_query_probe_counts(small):
     db, q, params = small
     idx = _build(db, 4, params)

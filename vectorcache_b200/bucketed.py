@@ -24,12 +24,15 @@ _P = C.c_void_p
 
 class _Params(C.Structure):
     _fields_ = [("n_probe", C.c_uint32), ("max_bucket_size", C.c_uint32), ("energy_soft", C.c_uint32),
-                ("kmeans_iters", C.c_uint32), ("expected_n", C.c_uint64), ("seed", C.c_uint64)]
+                ("kmeans_iters", C.c_uint32), ("rerank_k", C.c_uint32), ("reserved", C.c_uint32),
+                ("expected_n", C.c_uint64), ("seed", C.c_uint64)]
 
 
 @dataclass
 class BucketParams:
-    """BucketParams of the reference README (README.md:113-120)."""
+    """BucketParams of the reference README (README.md:113-120), plus
+    rerank_k: when larger than k, the scan keeps rerank_k candidates that are
+    re-scored with the exact float inner product before the top k is taken."""
 
     n_probe: int = 64
     max_bucket_size: int = 800
@@ -37,10 +40,11 @@ class BucketParams:
     expected_n: int = 0
     kmeans_iters: int = 4
     seed: int = 0x5EED5EED
+    rerank_k: int = 0
 
     def _c(self) -> _Params:
-        return _Params(self.n_probe, self.max_bucket_size, self.energy_soft, self.kmeans_iters, self.expected_n,
-                       self.seed)
+        return _Params(self.n_probe, self.max_bucket_size, self.energy_soft, self.kmeans_iters, self.rerank_k, 0,
+                       self.expected_n, self.seed)
 
 
 def _declare_bucketed(lib):

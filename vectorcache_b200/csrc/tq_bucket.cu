@@ -172,7 +172,13 @@ __global__ void __launch_bounds__(256) assign_kernel(const float* __restrict__ A
 // ---------------------------------------------------------------------------
 constexpr int kSelThreads = 256;
 constexpr int kSelChunk = 1024;
-constexpr int kSelCap = 2048;  // >= kSelChunk + 256, power of two
+
+// Sort buffer capacity for top-p: a power of two >= kSelChunk + p.
+__host__ __device__ inline int sel_cap(int p) {
+  int c = 2;
+  while (c < kSelChunk + p) c <<= 1;
+  return c;
+}
 
 __device__ void cta_sort(float* s, uint32_t* id, int p) {
   for (int size = 2; size <= p; size <<= 1) {
@@ -198,10 +204,12 @@ __device__ void cta_sort(float* s, uint32_t* id, int p) {
 __global__ void __launch_bounds__(kSelThreads) select_top_kernel(const float* __restrict__ S, long long ld,
                                                                  int ncols, int p, float* __restrict__ out_s,
                                                                  uint32_t* __restrict__ out_i) {
-  __shared__ float buf_s[kSelCap];
-  __shared__ uint32_t buf_i[kSelCap];
-  __shared__ float keep_s[256];
-  __shared__ uint32_t keep_i[256];
+  extern __shared__ __align__(16) unsigned char sel_smem[];
+  const int cap = sel_cap(p);
+  float* buf_s = reinterpret_cast<float*>(sel_smem);
+  uint32_t* buf_i = reinterpret_cast<uint32_t*>(buf_s + cap);
+  float* keep_s = reinterpret_cast<float*>(buf_i + cap);
+  uint32_t* keep_i = reinterpret_cast<uint32_t*>(keep_s + p);
   __shared__ int n_new;
   const long long row = blockIdx.x;
   const float* sr = S + row * ld;
@@ -1021,10 +1029,32 @@ __global__ void gather_rows_kernel(const float* __restrict__ src, const uint32_t
   dst[i] = src[static_cast<long long>(rows[r]) * dim + (i % dim)];
 }
 
+__global__ void take_columns_kernel(const float* __restrict__ src_s, const uint64_t* __restrict__ src_i,
+                                    long long nq, int k_src, int k_out, unsigned long long n_valid,
+                                    float* __restrict__ dst_s, uint64_t* __restrict__ dst_i) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nq * k_out) return;
+  const long long q = t / k_out;
+  const int j = static_cast<int>(t % k_out);
+  const uint64_t id = src_i[q * k_src + j];
+  const bool ok = id < n_valid;
+  dst_s[t] = ok ? src_s[q * k_src + j] : 0.f;
+  dst_i[t] = ok ? id : 0ull;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // Launchers
+cudaError_t launch_take_columns(const float* src_s, const uint64_t* src_i, long long nq, int k_src, int k_out,
+                                unsigned long long n_valid, float* dst_s, uint64_t* dst_i, cudaStream_t stream) {
+  const long long total = nq * k_out;
+  if (total == 0) return cudaSuccess;
+  take_columns_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(src_s, src_i, nq, k_src, k_out,
+                                                                                       n_valid, dst_s, dst_i);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 cudaError_t launch_normalize_rows(const float* x, long long n, int dim_in, int dim, float* out,
                                   cudaStream_t stream) {
@@ -1053,8 +1083,12 @@ cudaError_t launch_assign(const float* A, long long m, const float* B, long long
 cudaError_t launch_select_top(const float* S, long long rows, long long ld, int ncols, int p, float* out_s,
                               uint32_t* out_i, cudaStream_t stream) {
   if (rows == 0) return cudaSuccess;
-  if (p < 1 || p > 256) return cudaErrorInvalidValue;
-  select_top_kernel<<<static_cast<unsigned>(rows), kSelThreads, 0, stream>>>(S, ld, ncols, p, out_s, out_i);
+  if (p < 1 || p > kMaxProbe) return cudaErrorInvalidValue;
+  const size_t smem = static_cast<size_t>(sel_cap(p)) * 8 + static_cast<size_t>(p) * 8;
+  cudaError_t e = cudaFuncSetAttribute(select_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  select_top_kernel<<<static_cast<unsigned>(rows), kSelThreads, smem, stream>>>(S, ld, ncols, p, out_s, out_i);
   return cudaGetLastError();
 }
 

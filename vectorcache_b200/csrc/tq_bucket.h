@@ -38,9 +38,12 @@ cudaError_t launch_gemm_nt(const float* A, long long m, const float* B, long lon
 cudaError_t launch_assign(const float* A, long long m, const float* B, long long nb, int dim,
                           uint32_t* label, float* best, cudaStream_t stream);
 
+// Largest number of buckets one query may probe.
+constexpr int kMaxProbe = 2048;
+
 // Per row of S (row stride ld, ncols valid columns): the top p entries, score
-// descending, equal scores by lower column; p <= 256. Rows with fewer than p
-// columns are padded with (-inf, 0xffffffff).
+// descending, equal scores by lower column; p <= kMaxProbe. Rows with fewer
+// than p columns are padded with (-inf, 0xffffffff).
 cudaError_t launch_select_top(const float* S, long long rows, long long ld, int ncols, int p, float* out_s,
                               uint32_t* out_i, cudaStream_t stream);
 
@@ -90,6 +93,11 @@ cudaError_t launch_relabel(uint32_t* label, long long n, const uint32_t* remap, 
 // dst[r] = src[rows[r]] for n_rows rows of dim floats.
 cudaError_t launch_gather_rows(const float* src, const uint32_t* rows, long long n_rows, int dim, float* dst,
                                cudaStream_t stream);
+
+// dst (nq x k_out) = the first k_out columns of src (nq x k_src); entries whose
+// id is >= n_valid (unfilled slots) become (0, 0).
+cudaError_t launch_take_columns(const float* src_s, const uint64_t* src_i, long long nq, int k_src, int k_out,
+                                unsigned long long n_valid, float* dst_s, uint64_t* dst_i, cudaStream_t stream);
 
 struct PairArgs {
   const uint32_t* probes;    // nq x max_probe bucket ids (routing order)

@@ -61,7 +61,7 @@ struct tq_bucketed {
 
   // search scratch
   vcb::DeviceBuffer s_q, s_qh, s_route, s_top_s, s_top_i, s_counts, s_pstart, s_istart, s_fill, s_pairs, s_off,
-      s_items, s_nitems, s_lcount, s_cand_s, s_cand_i, s_out_s, s_out_i, s_np;
+      s_items, s_nitems, s_lcount, s_cand_s, s_cand_i, s_out_s, s_out_i, s_np, s_rr_s, s_rr_i;
 
   ~tq_bucketed() {
     if (eng) tq_index_destroy(eng);
@@ -370,16 +370,23 @@ struct tq_bucketed {
     });
   }
 
-  size_t pass_queries() const {
+  // Queries per pass: routing scores (nb floats per query) within 256 MiB and
+  // candidate lists (2 * max_probe lists of kscan (score, id) per query)
+  // within 1 GiB.
+  size_t pass_queries(size_t max_probe = 1, size_t kscan = 1) const {
     const size_t by_route = std::max<size_t>(1, (size_t{256} << 20) / (static_cast<size_t>(nb) * 4));
-    return std::min<size_t>(16384, by_route);
+    const size_t by_cand = std::max<size_t>(1, (size_t{1} << 30) / (max_probe * 2 * kscan * 8));
+    return std::min<size_t>({16384, by_route, by_cand});
   }
 
   // Device search: nq raw queries (dim_in floats) -> top k_eff per query.
   void search_device(const float* d_q, size_t nq, size_t ke, int max_probe, const uint32_t* d_np, float* d_scores,
                      uint64_t* d_ids, cudaStream_t s, float* trace_off = nullptr, uint32_t* trace_probe = nullptr,
                      float* trace_qh = nullptr) {
-    const size_t pass = pass_queries();
+    const bool rerank = p.rerank_k > ke;
+    // With re-ranking the scan keeps kscan candidates per query.
+    const size_t kscan = rerank ? std::min<size_t>({static_cast<size_t>(p.rerank_k), n, 256}) : ke;
+    const size_t pass = pass_queries(static_cast<size_t>(max_probe), kscan);
     for (size_t q0 = 0; q0 < nq; q0 += pass) {
       const size_t m = std::min(pass, nq - q0);
       s_qh.reserve(m * dim * 4);
@@ -422,8 +429,8 @@ struct tq_bucketed {
       pa.list_count = s_lcount.as<uint32_t>();
       eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       const size_t lists = m * max_probe * 2;
-      s_cand_s.reserve(lists * ke * 4);
-      s_cand_i.reserve(lists * ke * 4);
+      s_cand_s.reserve(lists * kscan * 4);
+      s_cand_i.reserve(lists * kscan * 4);
       const float* qf = eng->d_qf.as<float>();
       vcb::BucketScanArgs ba{};
       ba.codes = eng->d_codes.as<uint32_t>();
@@ -440,7 +447,7 @@ struct tq_bucketed {
       ba.n_items = pa.n_items;
       ba.nbg = static_cast<int>(nbg);
       ba.bits = static_cast<int>(bits);
-      ba.k = static_cast<int>(ke);
+      ba.k = static_cast<int>(kscan);
       ba.max_probe = max_probe;
       ba.cand_score = s_cand_s.as<float>();
       ba.cand_id = s_cand_i.as<uint32_t>();
@@ -450,12 +457,31 @@ struct tq_bucketed {
       mg.cand_id = ba.cand_id;
       mg.nq = static_cast<long long>(m);
       mg.n_lists = max_probe * 2;
-      mg.k = static_cast<int>(ke);
-      mg.k_out = static_cast<int>(ke);
+      mg.k = static_cast<int>(kscan);
+      mg.k_out = static_cast<int>(kscan);
       mg.out_score = d_scores + q0 * ke;
       mg.out_id = d_ids + q0 * ke;
       mg.list_count = pa.list_count;
+      if (rerank) {
+        s_rr_s.reserve(m * kscan * 4);
+        s_rr_i.reserve(m * kscan * 8);
+        mg.out_score = s_rr_s.as<float>();
+        mg.out_id = s_rr_i.as<uint64_t>();
+        mg.pad_id = ~0ull;  // unfilled slots score -inf in the re-rank
+      }
       eng->launch(tq_index::kMerge, s, "merge kernel", [&] { return vcb::launch_merge(mg, s); });
+      if (rerank) {
+        eng->launch(tq_index::kMerge, s, "rescore kernel", [&] {
+          return vcb::launch_rescore(qh, static_cast<long long>(m), static_cast<int>(dim), d_x.as<float>(),
+                                     static_cast<long long>(n), static_cast<int>(kscan), s_rr_s.as<float>(),
+                                     s_rr_i.as<uint64_t>(), s);
+        });
+        eng->launch(tq_index::kMerge, s, "take kernel", [&] {
+          return vcb::launch_take_columns(s_rr_s.as<float>(), s_rr_i.as<uint64_t>(), static_cast<long long>(m),
+                                          static_cast<int>(kscan), static_cast<int>(ke), n, d_scores + q0 * ke,
+                                          d_ids + q0 * ke, s);
+        });
+      }
       eng->scan_queries += m;
       if (trace_off) {
         vcb::check(cudaMemcpyAsync(trace_off + q0 * max_probe, s_off.get(), m * max_probe * 4,
@@ -474,10 +500,11 @@ namespace {
 using vcb::require;
 
 void check_params(const tq_bucket_params& p) {
-  require(p.n_probe >= 1 && p.n_probe <= 256, TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 256]");
+  require(p.n_probe >= 1 && p.n_probe <= vcb::kMaxProbe, TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 2048]");
   require(p.max_bucket_size >= 2 && p.max_bucket_size <= 8192, TQ_ERR_INVALID_ARGUMENT,
           "max_bucket_size must be in [2, 8192]");
   require(p.energy_soft >= 1, TQ_ERR_INVALID_ARGUMENT, "energy_soft must be >= 1");
+  require(p.rerank_k <= 256, TQ_ERR_INVALID_ARGUMENT, "rerank_k must be <= 256");
 }
 
 tq_bucketed* checked(tq_bucketed* h) {
@@ -496,6 +523,8 @@ void tq_bucket_params_init(tq_bucket_params* p) {
   p->max_bucket_size = 800;
   p->energy_soft = 400;
   p->kmeans_iters = 4;
+  p->rerank_k = 0;
+  p->reserved = 0;
   p->expected_n = 0;
   p->seed = 0x5eed5eedull;
 }
@@ -609,7 +638,7 @@ int tq_bucketed_search_device(tq_bucketed* h, const float* d_queries, size_t nq,
     if (nq == 0 || ke == 0) return;
     require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     const size_t np = n_probe ? n_probe : h->p.n_probe;
-    require(np >= 1 && np <= 256, TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 256]");
+    require(np >= 1 && np <= static_cast<size_t>(vcb::kMaxProbe), TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 2048]");
     vcb::DeviceGuard g(h->device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream();
     h->search_device(d_queries, nq, ke, static_cast<int>(std::min<size_t>(np, h->nb)), d_n_probe, d_scores, d_ids,
@@ -628,7 +657,7 @@ int tq_bucketed_search(tq_bucketed* h, const float* queries, size_t nq, size_t k
     if (nq == 0 || ke == 0) return;
     require(queries && scores && ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     const size_t np = n_probe ? n_probe : h->p.n_probe;
-    require(np >= 1 && np <= 256, TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 256]");
+    require(np >= 1 && np <= static_cast<size_t>(vcb::kMaxProbe), TQ_ERR_INVALID_ARGUMENT, "n_probe must be in [1, 2048]");
     vcb::DeviceGuard g(h->device);
     h->s_q.reserve(nq * h->dim_in * 4);
     h->s_out_s.reserve(nq * ke * 4);
@@ -684,7 +713,7 @@ int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, 
   return vcb::guarded([&] {
     checked(h);
     require(h->prepared, TQ_ERR_STATE, "route before prepare");
-    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    require(p >= 1 && p <= static_cast<size_t>(vcb::kMaxProbe), TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 2048]");
     if (nq == 0) return;
     require(d_queries && d_top_scores && d_top_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     vcb::DeviceGuard g(h->device);

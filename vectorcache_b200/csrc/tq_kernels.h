@@ -106,6 +106,8 @@ struct MergeArgs {
   // Optional: lists actually filled per query (the first list_count[q] of its
   // n_lists); nullptr means all n_lists.
   const uint32_t* list_count = nullptr;
+  // Id written into result slots no candidate filled (their score is 0).
+  uint64_t pad_id = 0;
 };
 
 size_t encode_smem_bytes(int dim, bool tqplus);

@@ -1,0 +1,600 @@
+// Learned n_probe predictor for the bucketed index: a small MLP trained and run
+// on the GPU by this file's own kernels. No counterpart exists in the
+// reference.
+//
+// Input per query: its top-256 routing scores s_1 >= ... >= s_256 and the 255
+// gaps s_i - s_{i+1} (a zero pads the gap vector to 256), standardized per
+// feature with the mean / std of the training set, rounded to bf16. Network:
+// in -> hidden (ReLU) -> hidden (ReLU) -> n_classes logits; one class per
+// candidate n_probe value. Weights are bf16 in every matrix product, with fp32
+// accumulation; the optimizer (Adam) keeps fp32 master weights and rewrites the
+// bf16 copies after each step. Biases, pre-activations and gradients are fp32.
+//
+// Prediction: softmax over the classes (ascending n_probe); the query gets the
+// smallest n_probe whose cumulative probability reaches `coverage`, or the
+// fixed fallback n_probe when the largest class probability is below
+// `min_confidence`.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "../../include/vectorcache_b200.h"
+#include "tq_abi.h"
+#include "tq_index_impl.h"
+
+namespace vcb {
+namespace {
+
+constexpr int kRouteFeatures = 256;  // top routing scores per query
+constexpr int kInputs = 2 * kRouteFeatures;
+constexpr int kMaxClasses = 32;
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ float ld(const float* p, long long i) { return p[i]; }
+__device__ __forceinline__ float ld(const bf16* p, long long i) { return __bfloat162float(p[i]); }
+
+// Raw features -> standardized bf16 inputs. top: m x p (p <= 256) scores
+// best first; missing scores (p < 256 or -inf) repeat the last valid one.
+__global__ void features_kernel(const float* __restrict__ top, long long m, int p, const float* __restrict__ mu,
+                                const float* __restrict__ inv_sd, bf16* __restrict__ x, float* __restrict__ raw) {
+  const long long q = blockIdx.x;
+  if (q >= m) return;
+  __shared__ float s[kRouteFeatures];
+  for (int i = threadIdx.x; i < kRouteFeatures; i += blockDim.x) {
+    s[i] = i < p ? top[q * p + i] : -INFINITY;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float last = s[0] > -INFINITY ? s[0] : 0.f;
+    for (int i = 0; i < kRouteFeatures; ++i) {
+      if (s[i] > -INFINITY) {
+        last = s[i];
+      } else {
+        s[i] = last;
+      }
+    }
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < kInputs; f += blockDim.x) {
+    float v;
+    if (f < kRouteFeatures) {
+      v = s[f];
+    } else {
+      const int i = f - kRouteFeatures;
+      v = i + 1 < kRouteFeatures ? __fsub_rn(s[i], s[i + 1]) : 0.f;
+    }
+    if (raw) raw[q * kInputs + f] = v;
+    x[q * kInputs + f] = __float2bfloat16_rn(__fmul_rn(__fsub_rn(v, mu[f]), inv_sd[f]));
+  }
+}
+
+// C (M x N, fp32, row stride ldc) = A (M x K) . B (K x N), fp32 accumulation in
+// coordinate order. Element (i, k) of A at A[i * a_r + k * a_c]; (k, j) of B at
+// B[k * b_r + j * b_c]. 64 x 64 tile per CTA, 4 x 4 per thread, 32 coordinates
+// per shared-memory stage.
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(256) gemm_kernel(const TA* __restrict__ A, long long a_r, long long a_c,
+                                                   const TB* __restrict__ B, long long b_r, long long b_c,
+                                                   float* __restrict__ C, long long ldc, long long M, int N, int K) {
+  __shared__ float sa[32][64 + 1];
+  __shared__ float sb[32][64 + 1];
+  const long long i0 = static_cast<long long>(blockIdx.y) * 64;
+  const int j0 = blockIdx.x * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += 32) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {
+      const int r = e / 32, c = e % 32;
+      const long long gi = i0 + r;
+      const int gk = k0 + c;
+      sa[c][r] = (gi < M && gk < K) ? ld(A, gi * a_r + gk * a_c) : 0.f;
+      const int gj = j0 + (e % 64);
+      const int gk2 = k0 + e / 64;
+      sb[e / 64][e % 64] = (gj < N && gk2 < K) ? ld(B, gk2 * b_r + static_cast<long long>(gj) * b_c) : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int c = 0; c < 32; ++c) {
+      float av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = sa[c][ty * 4 + a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = sb[c][tx * 4 + b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = __fmaf_rn(av[a], bv[b], acc[a][b]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const long long gi = i0 + ty * 4 + a;
+    if (gi >= M) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int gj = j0 + tx * 4 + b;
+      if (gj < N) C[gi * ldc + gj] = acc[a][b];
+    }
+  }
+}
+
+// Z += bias; optionally A = bf16(relu(Z)).
+__global__ void bias_act_kernel(float* __restrict__ Z, long long M, int N, const float* __restrict__ bias,
+                                bf16* __restrict__ act) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= M * N) return;
+  const float z = __fadd_rn(Z[i], bias[i % N]);
+  Z[i] = z;
+  if (act) act[i] = __float2bfloat16_rn(z > 0.f ? z : 0.f);
+}
+
+// Row-wise softmax cross-entropy: dZ = (softmax - onehot) / M, loss_rows[q].
+__global__ void softmax_xent_kernel(const float* __restrict__ Z, long long M, int N, const uint32_t* __restrict__ label,
+                                    float* __restrict__ dZ, float* __restrict__ loss_rows) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  const float* z = Z + q * N;
+  float mx = -INFINITY;
+  for (int j = 0; j < N; ++j) mx = fmaxf(mx, z[j]);
+  float sum = 0.f;
+  for (int j = 0; j < N; ++j) sum = __fadd_rn(sum, expf(__fsub_rn(z[j], mx)));
+  const float inv_m = 1.f / static_cast<float>(M);
+  const uint32_t y = label[q];
+  for (int j = 0; j < N; ++j) {
+    const float pj = __fdiv_rn(expf(__fsub_rn(z[j], mx)), sum);
+    dZ[q * N + j] = __fmul_rn(__fsub_rn(pj, j == static_cast<int>(y) ? 1.f : 0.f), inv_m);
+  }
+  loss_rows[q] = __fsub_rn(logf(sum), __fsub_rn(z[y], mx));
+}
+
+// dZ *= (Zprev > 0)
+__global__ void relu_grad_kernel(float* __restrict__ dA, const float* __restrict__ Z, long long total) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < total && !(Z[i] > 0.f)) dA[i] = 0.f;
+}
+
+// db[j] = sum_i dZ[i, j] (one thread per column, rows in order).
+__global__ void colsum_kernel(const float* __restrict__ dZ, long long M, int N, float* __restrict__ db) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  float s = 0.f;
+  for (long long i = 0; i < M; ++i) s = __fadd_rn(s, dZ[i * N + j]);
+  db[j] = s;
+}
+
+__global__ void adam_kernel(float* __restrict__ p, float* __restrict__ m1, float* __restrict__ m2,
+                            const float* __restrict__ g, long long n, float lr, float b1, float b2, float eps,
+                            float c1, float c2, bf16* __restrict__ shadow, long long shadow_n) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float a = __fmaf_rn(b1, m1[i], __fmul_rn(1.f - b1, gi));
+  const float v = __fmaf_rn(b2, m2[i], __fmul_rn(1.f - b2, __fmul_rn(gi, gi)));
+  m1[i] = a;
+  m2[i] = v;
+  const float mh = __fdiv_rn(a, c1), vh = __fdiv_rn(v, c2);
+  const float w = __fsub_rn(p[i], __fdiv_rn(__fmul_rn(lr, mh), __fadd_rn(sqrtf(vh), eps)));
+  p[i] = w;
+  if (i < shadow_n) shadow[i] = __float2bfloat16_rn(w);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ src, bf16* __restrict__ dst, long long n) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+// Logits -> n_probe per query (see the file comment).
+__global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, const uint32_t* __restrict__ classes,
+                               float coverage, float min_conf, uint32_t fallback, uint32_t* __restrict__ out,
+                               float* __restrict__ conf_out) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  const float* z = Z + q * N;
+  float mx = -INFINITY;
+  for (int j = 0; j < N; ++j) mx = fmaxf(mx, z[j]);
+  float sum = 0.f;
+  for (int j = 0; j < N; ++j) sum += expf(z[j] - mx);
+  float cum = 0.f, best = 0.f;
+  int pick = N - 1;
+  bool picked = false;
+  for (int j = 0; j < N; ++j) {
+    const float pj = expf(z[j] - mx) / sum;
+    best = fmaxf(best, pj);
+    cum += pj;
+    if (!picked && cum >= coverage) {
+      pick = j;
+      picked = true;
+    }
+  }
+  out[q] = best < min_conf ? fallback : classes[pick];
+  if (conf_out) conf_out[q] = best;
+}
+
+template <typename TA, typename TB>
+cudaError_t gemm(const TA* A, long long a_r, long long a_c, const TB* B, long long b_r, long long b_c, float* C,
+                 long long ldc, long long M, int N, int K, cudaStream_t s) {
+  if (M == 0 || N == 0) return cudaSuccess;
+  dim3 grid(static_cast<unsigned>((N + 63) / 64), static_cast<unsigned>((M + 63) / 64));
+  if (grid.y > 65535) return cudaErrorInvalidValue;
+  gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
+  return cudaGetLastError();
+}
+
+inline unsigned blocks(long long n, int t = 256) { return static_cast<unsigned>((n + t - 1) / t); }
+
+}  // namespace
+}  // namespace vcb
+
+struct tq_probe_mlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int hidden = 128, n_layers = 2, n_classes = 0;
+  std::vector<uint32_t> classes;
+  std::vector<int> fan_in, fan_out;  // per linear layer
+  std::vector<size_t> w_off, b_off;  // offsets into the flat fp32 parameter vector
+  size_t n_params = 0;
+  vcb::DeviceBuffer d_params, d_m1, d_m2, d_grad, d_wbf, d_mu, d_isd, d_classes;
+  std::vector<size_t> wbf_off;
+  size_t n_wbf = 0;
+  int64_t step = 0;
+  // scratch
+  vcb::DeviceBuffer d_x, d_raw, d_top, d_labels, d_loss, d_out;
+  vcb::DeviceBuffer z[5], a[5], dz[5];  // per linear layer (n_layers <= 4)
+
+  ~tq_probe_mlp() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+
+  void sync() { vcb::check(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+  int n_lin() const { return n_layers + 1; }
+
+  void reserve_batch(size_t m) {
+    d_x.reserve(m * vcb::kInputs * 2);
+    for (int l = 0; l < n_lin(); ++l) {
+      z[l].reserve(m * fan_out[l] * 4);
+      a[l].reserve(m * fan_out[l] * 2);
+      dz[l].reserve(m * fan_out[l] * 4);
+    }
+    d_loss.reserve(m * 4);
+  }
+
+  const vcb::bf16* wbf(int l) const { return d_wbf.as<vcb::bf16>() + wbf_off[l]; }
+  const float* bias(int l) const { return d_params.as<float>() + b_off[l]; }
+
+  // features(top) -> d_x; then the forward pass; logits in z[last].
+  void forward(const float* d_top, size_t m, int p, cudaStream_t s) {
+    reserve_batch(m);
+    vcb::features_kernel<<<static_cast<unsigned>(m), 256, 0, s>>>(d_top, static_cast<long long>(m), p,
+                                                                  d_mu.as<float>(), d_isd.as<float>(),
+                                                                  d_x.as<vcb::bf16>(), nullptr);
+    vcb::check(cudaGetLastError(), "features kernel");
+    const vcb::bf16* in = d_x.as<vcb::bf16>();
+    for (int l = 0; l < n_lin(); ++l) {
+      const int K = fan_in[l], N = fan_out[l];
+      vcb::check(vcb::gemm(in, K, 1, wbf(l), N, 1, z[l].as<float>(), N, static_cast<long long>(m), N, K, s),
+                 "mlp gemm");
+      const bool last = l + 1 == n_lin();
+      vcb::bias_act_kernel<<<vcb::blocks(static_cast<long long>(m) * N), 256, 0, s>>>(
+          z[l].as<float>(), static_cast<long long>(m), N, bias(l), last ? nullptr : a[l].as<vcb::bf16>());
+      vcb::check(cudaGetLastError(), "bias kernel");
+      in = a[l].as<vcb::bf16>();
+    }
+  }
+
+  // Gradients of the mean cross-entropy into d_grad; returns the loss.
+  float backward(const uint32_t* d_lab, size_t m, cudaStream_t s) {
+    const long long M = static_cast<long long>(m);
+    const int L = n_lin();
+    vcb::softmax_xent_kernel<<<vcb::blocks(M), 256, 0, s>>>(z[L - 1].as<float>(), M, n_classes, d_lab,
+                                                             dz[L - 1].as<float>(), d_loss.as<float>());
+    vcb::check(cudaGetLastError(), "softmax kernel");
+    float* g = d_grad.as<float>();
+    for (int l = L - 1; l >= 0; --l) {
+      const int K = fan_in[l], N = fan_out[l];
+      const vcb::bf16* in = l == 0 ? d_x.as<vcb::bf16>() : a[l - 1].as<vcb::bf16>();
+      // dW = in^T . dZ  (K x N)
+      vcb::check(vcb::gemm(in, 1, K, dz[l].as<float>(), N, 1, g + w_off[l], N, K, N, static_cast<int>(M), s),
+                 "mlp gemm");
+      vcb::colsum_kernel<<<vcb::blocks(N), 256, 0, s>>>(dz[l].as<float>(), M, N, g + b_off[l]);
+      vcb::check(cudaGetLastError(), "colsum kernel");
+      if (l > 0) {
+        // dA_{l-1} = dZ . W^T (M x K), then the ReLU mask of layer l-1.
+        vcb::check(vcb::gemm(dz[l].as<float>(), N, 1, wbf(l), 1, N, dz[l - 1].as<float>(), K, M, K, N, s),
+                   "mlp gemm");
+        vcb::relu_grad_kernel<<<vcb::blocks(M * K), 256, 0, s>>>(dz[l - 1].as<float>(), z[l - 1].as<float>(),
+                                                                 M * K);
+        vcb::check(cudaGetLastError(), "relu grad kernel");
+      }
+    }
+    std::vector<float> lr(m);
+    vcb::check(cudaMemcpyAsync(lr.data(), d_loss.get(), m * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    double tot = 0.0;
+    for (float v : lr) tot += v;
+    return static_cast<float>(tot / static_cast<double>(m));
+  }
+
+  void adam(float lr, cudaStream_t s) {
+    ++step;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, static_cast<float>(step));
+    const float c2 = 1.f - std::pow(b2, static_cast<float>(step));
+    // Each weight matrix: its fp32 master and its bf16 copy.
+    for (int l = 0; l < n_lin(); ++l) {
+      const long long nw = static_cast<long long>(fan_in[l]) * fan_out[l];
+      vcb::adam_kernel<<<vcb::blocks(nw), 256, 0, s>>>(d_params.as<float>() + w_off[l], d_m1.as<float>() + w_off[l],
+                                                       d_m2.as<float>() + w_off[l], d_grad.as<float>() + w_off[l], nw,
+                                                       lr, b1, b2, 1e-8f, c1, c2, d_wbf.as<vcb::bf16>() + wbf_off[l],
+                                                       nw);
+      vcb::check(cudaGetLastError(), "adam kernel");
+      const long long nbias = fan_out[l];
+      vcb::adam_kernel<<<vcb::blocks(nbias), 256, 0, s>>>(d_params.as<float>() + b_off[l],
+                                                          d_m1.as<float>() + b_off[l], d_m2.as<float>() + b_off[l],
+                                                          d_grad.as<float>() + b_off[l], nbias, lr, b1, b2, 1e-8f, c1,
+                                                          c2, nullptr, 0);
+      vcb::check(cudaGetLastError(), "adam kernel");
+    }
+  }
+
+  void refresh_bf16(cudaStream_t s) {
+    for (int l = 0; l < n_lin(); ++l) {
+      const long long nw = static_cast<long long>(fan_in[l]) * fan_out[l];
+      vcb::to_bf16_kernel<<<vcb::blocks(nw), 256, 0, s>>>(d_params.as<float>() + w_off[l],
+                                                          d_wbf.as<vcb::bf16>() + wbf_off[l], nw);
+      vcb::check(cudaGetLastError(), "bf16 kernel");
+    }
+  }
+};
+
+namespace {
+
+using vcb::require;
+
+tq_probe_mlp* checked(tq_probe_mlp* h) {
+  require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null model");
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tq_probe_mlp_create(size_t hidden, size_t n_layers, const uint32_t* classes, size_t n_classes, uint64_t seed,
+                        int device, tq_probe_mlp** out) {
+  return vcb::guarded([&] {
+    require(out != nullptr, TQ_ERR_INVALID_ARGUMENT, "out must not be NULL");
+    *out = nullptr;
+    require(hidden >= 1 && hidden <= 1024, TQ_ERR_INVALID_ARGUMENT, "hidden must be in [1, 1024]");
+    require(n_layers >= 1 && n_layers <= 4, TQ_ERR_INVALID_ARGUMENT, "n_layers must be in [1, 4]");
+    require(classes != nullptr && n_classes >= 2 && n_classes <= static_cast<size_t>(vcb::kMaxClasses),
+            TQ_ERR_INVALID_ARGUMENT, "need 2..32 classes");
+    for (size_t i = 0; i < n_classes; ++i) {
+      require(classes[i] >= 1 && classes[i] <= 2048 && (i == 0 || classes[i] > classes[i - 1]),
+              TQ_ERR_INVALID_ARGUMENT, "classes must be increasing n_probe values in [1, 2048]");
+    }
+    int count = 0;
+    vcb::check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    require(device >= 0 && device < count, TQ_ERR_INVALID_ARGUMENT, "no such CUDA device");
+    vcb::DeviceGuard g(device);
+    auto h = std::make_unique<tq_probe_mlp>();
+    h->device = device;
+    vcb::check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    h->hidden = static_cast<int>(hidden);
+    h->n_layers = static_cast<int>(n_layers);
+    h->n_classes = static_cast<int>(n_classes);
+    h->classes.assign(classes, classes + n_classes);
+    int in = vcb::kInputs;
+    for (int l = 0; l <= h->n_layers; ++l) {
+      const int o = l == h->n_layers ? h->n_classes : h->hidden;
+      h->fan_in.push_back(in);
+      h->fan_out.push_back(o);
+      h->w_off.push_back(h->n_params);
+      h->n_params += static_cast<size_t>(in) * o;
+      h->b_off.push_back(h->n_params);
+      h->n_params += o;
+      h->wbf_off.push_back(h->n_wbf);
+      h->n_wbf += static_cast<size_t>(in) * o;
+      in = o;
+    }
+    // He-uniform initial weights, zero biases (mt19937_64(seed)).
+    std::vector<float> init(h->n_params, 0.f);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l <= h->n_layers; ++l) {
+      const float lim = std::sqrt(6.f / static_cast<float>(h->fan_in[l]));
+      std::uniform_real_distribution<float> U(-lim, lim);
+      for (size_t i = 0; i < static_cast<size_t>(h->fan_in[l]) * h->fan_out[l]; ++i) init[h->w_off[l] + i] = U(rng);
+    }
+    h->d_params.reserve(h->n_params * 4);
+    h->d_m1.reserve(h->n_params * 4);
+    h->d_m2.reserve(h->n_params * 4);
+    h->d_grad.reserve(h->n_params * 4);
+    h->d_wbf.reserve(h->n_wbf * 2);
+    h->d_mu.reserve(vcb::kInputs * 4);
+    h->d_isd.reserve(vcb::kInputs * 4);
+    h->d_classes.reserve(n_classes * 4);
+    std::vector<float> mu(vcb::kInputs, 0.f), isd(vcb::kInputs, 1.f);
+    vcb::check(cudaMemcpyAsync(h->d_params.get(), init.data(), h->n_params * 4, cudaMemcpyHostToDevice, h->stream),
+               "H2D");
+    vcb::check(cudaMemsetAsync(h->d_m1.get(), 0, h->n_params * 4, h->stream), "memset");
+    vcb::check(cudaMemsetAsync(h->d_m2.get(), 0, h->n_params * 4, h->stream), "memset");
+    vcb::check(cudaMemcpyAsync(h->d_mu.get(), mu.data(), mu.size() * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::check(cudaMemcpyAsync(h->d_isd.get(), isd.data(), isd.size() * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::check(cudaMemcpyAsync(h->d_classes.get(), classes, n_classes * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    h->refresh_bf16(h->stream);
+    h->sync();
+    *out = h.release();
+  });
+}
+
+int tq_probe_mlp_destroy(tq_probe_mlp* h) {
+  return vcb::guarded([&] {
+    if (!h) return;
+    vcb::DeviceGuard g(h->device);
+    delete h;
+  });
+}
+
+int tq_probe_mlp_info(const tq_probe_mlp* h, size_t* n_inputs, size_t* n_params, size_t* n_classes) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null model");
+    if (n_inputs) *n_inputs = vcb::kInputs;
+    if (n_params) *n_params = h->n_params;
+    if (n_classes) *n_classes = static_cast<size_t>(h->n_classes);
+  });
+}
+
+int tq_probe_mlp_features(tq_probe_mlp* h, const float* top_scores, size_t m, size_t p, float* raw) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(top_scores && raw, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    if (m == 0) return;
+    vcb::DeviceGuard g(h->device);
+    vcb::DeviceBuffer top, r, x;
+    top.reserve(m * p * 4);
+    r.reserve(m * vcb::kInputs * 4);
+    x.reserve(m * vcb::kInputs * 2);
+    vcb::check(cudaMemcpyAsync(top.get(), top_scores, m * p * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::features_kernel<<<static_cast<unsigned>(m), 256, 0, h->stream>>>(
+        top.as<float>(), static_cast<long long>(m), static_cast<int>(p), h->d_mu.as<float>(), h->d_isd.as<float>(),
+        x.as<vcb::bf16>(), r.as<float>());
+    vcb::check(cudaGetLastError(), "features kernel");
+    vcb::check(cudaMemcpyAsync(raw, r.get(), m * vcb::kInputs * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_set_normalization(tq_probe_mlp* h, const float* mean, const float* stddev) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(mean && stddev, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    vcb::DeviceGuard g(h->device);
+    std::vector<float> isd(vcb::kInputs);
+    for (int i = 0; i < vcb::kInputs; ++i) isd[i] = stddev[i] > 1e-12f ? 1.f / stddev[i] : 0.f;
+    vcb::check(cudaMemcpyAsync(h->d_mu.get(), mean, vcb::kInputs * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::check(cudaMemcpyAsync(h->d_isd.get(), isd.data(), vcb::kInputs * 4, cudaMemcpyHostToDevice, h->stream),
+               "H2D");
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_get_params(tq_probe_mlp* h, float* params) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(params != nullptr, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    vcb::DeviceGuard g(h->device);
+    vcb::check(cudaMemcpyAsync(params, h->d_params.get(), h->n_params * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_set_params(tq_probe_mlp* h, const float* params) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(params != nullptr, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    vcb::DeviceGuard g(h->device);
+    vcb::check(cudaMemcpyAsync(h->d_params.get(), params, h->n_params * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    h->refresh_bf16(h->stream);
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_forward(tq_probe_mlp* h, const float* top_scores, size_t m, size_t p, float* logits) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(top_scores && logits, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    if (m == 0) return;
+    vcb::DeviceGuard g(h->device);
+    h->d_top.reserve(m * p * 4);
+    vcb::check(cudaMemcpyAsync(h->d_top.get(), top_scores, m * p * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    h->forward(h->d_top.as<float>(), m, static_cast<int>(p), h->stream);
+    vcb::check(cudaMemcpyAsync(logits, h->z[h->n_lin() - 1].get(), m * h->n_classes * 4, cudaMemcpyDeviceToHost,
+                               h->stream),
+               "D2H");
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint32_t* labels, size_t m, size_t p,
+                           float* loss, float* grads) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(top_scores && labels && grads, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
+    for (size_t i = 0; i < m; ++i) {
+      require(labels[i] < static_cast<uint32_t>(h->n_classes), TQ_ERR_INVALID_ARGUMENT, "label out of range");
+    }
+    vcb::DeviceGuard g(h->device);
+    h->d_top.reserve(m * p * 4);
+    h->d_labels.reserve(m * 4);
+    vcb::check(cudaMemcpyAsync(h->d_top.get(), top_scores, m * p * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::check(cudaMemcpyAsync(h->d_labels.get(), labels, m * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    h->forward(h->d_top.as<float>(), m, static_cast<int>(p), h->stream);
+    const float l = h->backward(h->d_labels.as<uint32_t>(), m, h->stream);
+    if (loss) *loss = l;
+    vcb::check(cudaMemcpyAsync(grads, h->d_grad.get(), h->n_params * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+int tq_probe_mlp_train_step_device(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels, size_t m,
+                                   size_t p, float lr, float* loss) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(d_top_scores && d_labels, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
+    vcb::DeviceGuard g(h->device);
+    h->forward(d_top_scores, m, static_cast<int>(p), h->stream);
+    const float l = h->backward(d_labels, m, h->stream);
+    h->adam(lr, h->stream);
+    if (loss) *loss = l;
+  });
+}
+
+int tq_probe_mlp_predict_device(tq_probe_mlp* h, const float* d_top_scores, size_t m, size_t p, float coverage,
+                                float min_confidence, uint32_t fallback, uint32_t* d_n_probe, float* d_confidence,
+                                void* stream) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(d_top_scores && d_n_probe, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    require(fallback >= 1 && fallback <= 2048, TQ_ERR_INVALID_ARGUMENT, "fallback must be in [1, 2048]");
+    if (m == 0) return;
+    vcb::DeviceGuard g(h->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    if (s != h->stream) h->sync();
+    h->forward(d_top_scores, m, static_cast<int>(p), s);
+    vcb::predict_kernel<<<vcb::blocks(static_cast<long long>(m)), 256, 0, s>>>(
+        h->z[h->n_lin() - 1].as<float>(), static_cast<long long>(m), h->n_classes, h->d_classes.as<uint32_t>(),
+        coverage, min_confidence, fallback, d_n_probe, d_confidence);
+    vcb::check(cudaGetLastError(), "predict kernel");
+  });
+}
+
+int tq_probe_mlp_synchronize(tq_probe_mlp* h) {
+  return vcb::guarded([&] {
+    checked(h);
+    vcb::DeviceGuard g(h->device);
+    h->sync();
+  });
+}
+
+}  // extern "C"

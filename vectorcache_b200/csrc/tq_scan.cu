@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   for (int t = threadIdx.x; t < kout; t += blockDim.x) {
     const bool have = t < nbest;
     a.out_score[qi * kout + t] = have ? best_s[t] : 0.f;
-    a.out_id[qi * kout + t] = have ? static_cast<uint64_t>(best_i[t]) : 0ull;
+    a.out_id[qi * kout + t] = have ? static_cast<uint64_t>(best_i[t]) : a.pad_id;
   }
 }
 
