@@ -279,6 +279,105 @@ int tq_bucketed_export_rows(tq_bucketed* h, float* x_hat);
  * alpha, calibration and query LUT exports describe the bucketed layout. */
 int tq_bucketed_engine(tq_bucketed* h, tq_index** engine);
 
+/* ---- learned n_probe predictor ----------------------------------------------
+ * No counterpart in the reference. A small MLP reads a query's top-256
+ * routing scores s_1 >= ... >= s_256 and the gaps s_i - s_{i+1} (512 inputs,
+ * standardized by tq_probe_mlp_set_normalization), n_layers hidden layers of
+ * `hidden` units (ReLU) and one logit per class; class c stands for the
+ * n_probe value classes[c] (increasing, <= 2048). Matrix products use bf16
+ * weights and activations with fp32 accumulation; training (softmax
+ * cross-entropy, Adam) keeps fp32 master weights. Everything runs on the GPU.
+ * Prediction: the smallest class whose cumulative probability reaches
+ * `coverage`, or `fallback` when the largest class probability is below
+ * `min_confidence`. Parameters are flattened as, per layer, W (fan_in x
+ * fan_out, row-major) then b (fan_out). */
+typedef struct tq_probe_mlp tq_probe_mlp;
+
+int tq_probe_mlp_create(size_t hidden, size_t n_layers, const uint32_t* classes, size_t n_classes,
+                        uint64_t seed, int device, tq_probe_mlp** out);
+int tq_probe_mlp_destroy(tq_probe_mlp* h);
+int tq_probe_mlp_info(const tq_probe_mlp* h, size_t* n_inputs, size_t* n_params, size_t* n_classes);
+/* Raw (unstandardized) 512 features of m rows of top routing scores (row
+ * stride p <= 256), host buffers. */
+int tq_probe_mlp_features(tq_probe_mlp* h, const float* top_scores, size_t m, size_t p, float* raw);
+int tq_probe_mlp_set_normalization(tq_probe_mlp* h, const float* mean, const float* stddev);
+int tq_probe_mlp_get_params(tq_probe_mlp* h, float* params);
+int tq_probe_mlp_set_params(tq_probe_mlp* h, const float* params);
+/* Logits (m x n_classes) of host rows. */
+int tq_probe_mlp_forward(tq_probe_mlp* h, const float* top_scores, size_t m, size_t p, float* logits);
+/* Mean cross-entropy and its gradients (n_params floats) for a host batch,
+ * without updating the parameters. */
+int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint32_t* labels, size_t m,
+                           size_t p, float* loss, float* grads);
+/* One Adam step (lr; beta1 0.9, beta2 0.999, eps 1e-8) on a device batch,
+ * queued on `stream` (NULL: the model's own stream); returns when done. */
+int tq_probe_mlp_train_step_device(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels,
+                                   size_t m, size_t p, float lr, float* loss, void* stream);
+/* Per-query n_probe (device, m entries) and optionally the confidence. */
+int tq_probe_mlp_predict_device(tq_probe_mlp* h, const float* d_top_scores, size_t m, size_t p,
+                                float coverage, float min_confidence, uint32_t fallback,
+                                uint32_t* d_n_probe, float* d_confidence, void* stream);
+int tq_probe_mlp_synchronize(tq_probe_mlp* h);
+
+/* Bucketed search with the learned n_probe: one routing pass gives both the
+ * network's input (top-256 routing scores) and the probes; every query scans
+ * its predicted number of buckets (at most fallback_n_probe, which is also the
+ * low-confidence fallback; 0 = the index's n_probe). Device buffers, queued
+ * on `stream`. */
+int tq_bucketed_search_learned_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t k,
+                                      tq_probe_mlp* mlp, float coverage, float min_confidence,
+                                      size_t fallback_n_probe, float* d_scores, uint64_t* d_ids,
+                                      size_t* k_eff, void* stream);
+
+/* ---- serving loop -------------------------------------------------------------
+ * No counterpart in the reference (its tools time single synchronous calls).
+ * Continuous batching over resident indexes on one GPU: requests wait in a
+ * FIFO queue; whenever one of the server's slots (own CUDA stream, pinned
+ * staging, device buffers and search scratch) is free, the oldest request is
+ * launched together with every later waiting request for the same index, k
+ * and n_probe, up to max_batch queries. Batches in different slots overlap on
+ * the device. start() creates slots only while the device memory in use
+ * (resident indexes included) stays within hbm_budget_bytes, and grows each
+ * slot's scratch by one full-size warm-up search per index, so serving
+ * allocates no device memory. A query's result does not depend on the other
+ * queries of its batch. Host buffers of a request must stay valid until
+ * tq_server_wait returns for it. */
+typedef struct tq_server tq_server;
+
+int tq_server_create(int device, size_t hbm_budget_bytes, size_t max_slots, size_t max_batch,
+                     tq_server** out);
+int tq_server_destroy(tq_server* h);
+/* Register an index (prepared, same device) before start(); *target is its id. */
+int tq_server_add_flat(tq_server* h, tq_index* index, size_t max_k, int* target);
+/* mlp (optional): the learned n_probe predictor; requests then scan each
+ * query's predicted number of buckets, at most their n_probe. */
+int tq_server_add_bucketed(tq_server* h, tq_bucketed* index, size_t max_k, size_t max_probe,
+                           tq_probe_mlp* mlp, float coverage, float min_confidence, int* target);
+int tq_server_start(tq_server* h);
+int tq_server_info(tq_server* h, size_t* n_slots, size_t* slot_bytes, size_t* resident_bytes);
+/* Queue a request (nq <= max_batch host rows); scores/ids receive nq x k_eff. */
+int tq_server_submit(tq_server* h, int target, const float* queries, size_t nq, size_t k,
+                     size_t n_probe, float* scores, uint64_t* ids, uint64_t* request);
+/* Block until the request is done; latency from submission to the completion
+ * of its result copy. */
+int tq_server_wait(tq_server* h, uint64_t request, size_t* k_eff, double* latency_us);
+int tq_server_stats(tq_server* h, uint64_t* batches, uint64_t* queries, uint64_t* completed,
+                    size_t* peak_inflight);
+
+/* Open-loop replay of a request trace: each item is submitted at its arrival
+ * time (microseconds after the call starts); latency_us[i] runs from the
+ * scheduled arrival to completion. */
+typedef struct tq_replay_item {
+  double arrival_us;
+  int target;
+  const float* queries;
+  size_t nq, k, n_probe;
+  float* scores;
+  uint64_t* ids;
+} tq_replay_item;
+int tq_server_replay(tq_server* h, const tq_replay_item* items, size_t n, double* latency_us,
+                     double* wall_s);
+
 /* ---- search without device allocation --------------------------------------
  * No counterpart in the reference.
  *

@@ -210,7 +210,18 @@ class SearchResults:
 
 
 def _stream_ptr(stream) -> int | None:
+    """cudaStream_t for a *_device call. With no stream given and torch in use,
+    the caller's current torch stream: device buffers handed over as torch
+    tensors were produced there, so the library's work is ordered after it."""
     if stream is None:
+        import sys
+
+        torch = sys.modules.get("torch")
+        if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+            # torch's default stream is the legacy default stream (handle 0);
+            # pass cudaStreamLegacy (1) for it: a NULL stream would mean the
+            # library's own non-blocking stream, which is not ordered with it.
+            return int(torch.cuda.current_stream().cuda_stream) or 1
         return None
     if isinstance(stream, int):
         return stream
@@ -401,3 +412,7 @@ def _dev(t, n: int | None = None):
 from .bucketed import BucketedTurboQuantIndex, BucketParams  # noqa: E402
 
 __all__ += ["BucketedTurboQuantIndex", "BucketParams"]
+
+from .serving import Server  # noqa: E402
+
+__all__ += ["Server"]

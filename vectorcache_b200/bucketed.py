@@ -237,3 +237,30 @@ class BucketedTurboQuantIndex:
         eng.n_byte_groups = eng.dim // (8 // self.bits)
         eng.close = lambda: None  # owned by the bucketed index
         return eng
+
+
+def _declare_learned(lib):
+    if getattr(lib, "_learned_declared", False):
+        return lib
+    fn = lib.tq_bucketed_search_learned_device
+    fn.restype = C.c_int
+    fn.argtypes = [_P, _P, _SZ, _SZ, _P, C.c_float, C.c_float, _SZ, _P, _P, C.POINTER(_SZ), _P]
+    lib._learned_declared = True
+    return lib
+
+
+def search_learned_device(index: "BucketedTurboQuantIndex", d_queries, k: int, mlp, d_scores, d_ids,
+                          coverage: float = 0.9, min_confidence: float = 0.0, fallback_n_probe: int = 0,
+                          nq: int | None = None, stream=None) -> int:
+    """One routing pass, the learned n_probe per query, then the bucket scan
+    (tq_bucketed_search_learned_device)."""
+    lib = _declare_learned(index._lib)
+    qp, nq = _dev(d_queries, nq)
+    ke = _SZ(0)
+    _check(lib.tq_bucketed_search_learned_device(index._h, qp, nq, k, mlp._h, coverage, min_confidence,
+                                                 fallback_n_probe, _dev(d_scores)[0], _dev(d_ids)[0], C.byref(ke),
+                                                 _stream_ptr(stream)))
+    return ke.value
+
+
+BucketedTurboQuantIndex.search_learned_device = search_learned_device

@@ -649,7 +649,7 @@ __global__ void pair_count_kernel(PairArgs a) {
   const int np = probes_of(a, q);
   if (j == 0) a.list_count[q] = 2u * static_cast<uint32_t>(np);
   if (j >= np) return;
-  const uint32_t b = a.probes[t];
+  const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b < static_cast<uint32_t>(a.nb)) atomicAdd(&a.counts[b], 1u);
 }
 
@@ -659,7 +659,7 @@ __global__ void pair_scatter_kernel(PairArgs a) {
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
   if (j >= probes_of(a, q)) return;
-  const uint32_t b = a.probes[t];
+  const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b >= static_cast<uint32_t>(a.nb)) return;
   const unsigned long long pos = a.pair_start[b] + atomicAdd(&a.fill[b], 1u);
   a.pairs[pos] = static_cast<uint32_t>(t);
@@ -673,7 +673,7 @@ __global__ void pair_offset_kernel(PairArgs a) {
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
   if (j >= probes_of(a, q)) return;
-  const uint32_t b = a.probes[t];
+  const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b >= static_cast<uint32_t>(a.nb)) return;
   const float d = warp_dot(a.q_hat + q * a.dim, a.enc + static_cast<long long>(b) * a.dim, a.dim, lane);
   if (lane == 0) a.offsets[t] = d;

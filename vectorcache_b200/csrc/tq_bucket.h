@@ -100,7 +100,8 @@ cudaError_t launch_take_columns(const float* src_s, const uint64_t* src_i, long 
                                 unsigned long long n_valid, float* dst_s, uint64_t* dst_i, cudaStream_t stream);
 
 struct PairArgs {
-  const uint32_t* probes;    // nq x max_probe bucket ids (routing order)
+  const uint32_t* probes;    // nq rows of bucket ids (routing order), row stride probe_stride
+  int probe_stride = 0;      // 0: max_probe
   const uint32_t* n_probe;   // per query, or nullptr: every query probes `fixed_probe`
   int fixed_probe;
   int max_probe;

@@ -37,6 +37,19 @@
 #include "tq_bucket.h"
 #include "tq_index_impl.h"
 #include "tq_kernels.h"
+#include "tq_probe.h"
+#include "tq_serving_hooks.h"
+
+namespace vcb {
+// Device scratch of one bucketed search (routing, probe pairs, candidate
+// lists, re-rank) plus the flat engine's query scratch.
+struct BucketScratch {
+  DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
+      cand_i, rr_s, rr_i, np;
+  FlatScratchStore flat;
+  ProbeScratch probe;
+};
+}  // namespace vcb
 
 struct tq_bucketed {
   int device = 0;
@@ -60,8 +73,8 @@ struct tq_bucketed {
   bool prepared = false, built_once = false;
 
   // search scratch
-  vcb::DeviceBuffer s_q, s_qh, s_route, s_top_s, s_top_i, s_counts, s_pstart, s_istart, s_fill, s_pairs, s_off,
-      s_items, s_nitems, s_lcount, s_cand_s, s_cand_i, s_out_s, s_out_i, s_np, s_rr_s, s_rr_i;
+  vcb::DeviceBuffer s_q, s_out_s, s_out_i, s_np;  // host-API staging
+  vcb::BucketScratch own;                             // the index's own search scratch
 
   ~tq_bucketed() {
     if (eng) tq_index_destroy(eng);
@@ -356,17 +369,17 @@ struct tq_bucketed {
   }
 
   // Routing of m normalized queries: scores (m x nb) and the top p per query.
-  void route(const float* qh, size_t m, int ptop, cudaStream_t s) {
-    s_route.reserve(m * nb * 4);
-    s_top_s.reserve(m * ptop * 4);
-    s_top_i.reserve(m * ptop * 4);
+  void route(const float* qh, size_t m, int ptop, cudaStream_t s, vcb::BucketScratch& sc) {
+    sc.route.reserve(m * nb * 4);
+    sc.top_s.reserve(m * ptop * 4);
+    sc.top_i.reserve(m * ptop * 4);
     eng->launch(tq_index::kPrep, s, "routing kernel", [&] {
       return vcb::launch_gemm_nt(qh, static_cast<long long>(m), d_route.as<float>(), nb, static_cast<int>(dim),
-                                 s_route.as<float>(), nb, s);
+                                 sc.route.as<float>(), nb, s);
     });
     eng->launch(tq_index::kPrep, s, "select kernel", [&] {
-      return vcb::launch_select_top(s_route.as<float>(), static_cast<long long>(m), nb, nb, ptop, s_top_s.as<float>(),
-                                    s_top_i.as<uint32_t>(), s);
+      return vcb::launch_select_top(sc.route.as<float>(), static_cast<long long>(m), nb, nb, ptop, sc.top_s.as<float>(),
+                                    sc.top_i.as<uint32_t>(), s);
     });
   }
 
@@ -383,34 +396,56 @@ struct tq_bucketed {
   void search_device(const float* d_q, size_t nq, size_t ke, int max_probe, const uint32_t* d_np, float* d_scores,
                      uint64_t* d_ids, cudaStream_t s, float* trace_off = nullptr, uint32_t* trace_probe = nullptr,
                      float* trace_qh = nullptr) {
+    search_device(d_q, nq, ke, max_probe, d_np, d_scores, d_ids, s, own, trace_off, trace_probe, trace_qh);
+  }
+  // Same with caller-owned scratch: searches with distinct scratch may run
+  // concurrently on distinct streams (the index data is only read).
+  void search_device(const float* d_q, size_t nq, size_t ke, int max_probe, const uint32_t* d_np, float* d_scores,
+                     uint64_t* d_ids, cudaStream_t s, vcb::BucketScratch& sc, float* trace_off = nullptr,
+                     uint32_t* trace_probe = nullptr, float* trace_qh = nullptr,
+                     const vcb::LearnedProbe* lp = nullptr) {
+    // With the learned probe, one routing pass serves both the network's
+    // features (top 256 scores) and the probes (top max_probe buckets).
+    const int ptop = lp ? std::max(max_probe, 256) : max_probe;
     const bool rerank = p.rerank_k > ke;
     // With re-ranking the scan keeps kscan candidates per query.
     const size_t kscan = rerank ? std::min<size_t>({static_cast<size_t>(p.rerank_k), n, 256}) : ke;
     const size_t pass = pass_queries(static_cast<size_t>(max_probe), kscan);
     for (size_t q0 = 0; q0 < nq; q0 += pass) {
       const size_t m = std::min(pass, nq - q0);
-      s_qh.reserve(m * dim * 4);
-      float* qh = s_qh.as<float>();
+      sc.qh.reserve(m * dim * 4);
+      float* qh = sc.qh.as<float>();
       eng->launch(tq_index::kPrep, s, "normalize kernel", [&] {
         return vcb::launch_normalize_rows(d_q + q0 * dim_in, static_cast<long long>(m), static_cast<int>(dim_in),
                                           static_cast<int>(dim), qh, s);
       });
-      route(qh, m, max_probe, s);
-      eng->prep_queries(qh, m, s, nullptr);
+      route(qh, m, ptop, s, sc);
+      const uint32_t* np_pass = d_np ? d_np + q0 : nullptr;
+      if (lp) {
+        sc.np.reserve(m * 4);
+        eng->launch(tq_index::kPrep, s, "probe network", [&] {
+          vcb::probe_predict(lp->mlp, sc.top_s.as<float>(), m, ptop, lp->coverage, lp->min_confidence,
+                             static_cast<uint32_t>(max_probe), sc.np.as<uint32_t>(), s, sc.probe);
+          return cudaGetLastError();
+        });
+        np_pass = sc.np.as<uint32_t>();
+      }
+      eng->prep_queries(qh, m, s, nullptr, sc.flat.ref());
       // Pairs and work items.
       const long long items = vcb::max_items(static_cast<long long>(m), max_probe, nb);
-      s_counts.reserve(nb * 4);
-      s_fill.reserve(nb * 4);
-      s_pstart.reserve((nb + 1) * 8);
-      s_istart.reserve((nb + 1) * 8);
-      s_pairs.reserve(m * max_probe * 4);
-      s_off.reserve(m * max_probe * 4);
-      s_items.reserve(static_cast<size_t>(items) * 16);
-      s_nitems.reserve(8);
-      s_lcount.reserve(m * 4);
+      sc.counts.reserve(nb * 4);
+      sc.fill.reserve(nb * 4);
+      sc.pstart.reserve((nb + 1) * 8);
+      sc.istart.reserve((nb + 1) * 8);
+      sc.pairs.reserve(m * max_probe * 4);
+      sc.off.reserve(m * max_probe * 4);
+      sc.items.reserve(static_cast<size_t>(items) * 16);
+      sc.nitems.reserve(8);
+      sc.lcount.reserve(m * 4);
       vcb::PairArgs pa{};
-      pa.probes = s_top_i.as<uint32_t>();
-      pa.n_probe = d_np ? d_np + q0 : nullptr;
+      pa.probes = sc.top_i.as<uint32_t>();
+      pa.probe_stride = ptop;
+      pa.n_probe = np_pass;
       pa.fixed_probe = max_probe;
       pa.max_probe = max_probe;
       pa.nq = static_cast<long long>(m);
@@ -418,27 +453,27 @@ struct tq_bucketed {
       pa.q_hat = qh;
       pa.enc = d_enc.as<float>();
       pa.dim = static_cast<int>(dim);
-      pa.counts = s_counts.as<uint32_t>();
-      pa.pair_start = s_pstart.as<unsigned long long>();
-      pa.item_start = s_istart.as<unsigned long long>();
-      pa.fill = s_fill.as<uint32_t>();
-      pa.pairs = s_pairs.as<uint32_t>();
-      pa.offsets = s_off.as<float>();
-      pa.items = s_items.as<uint4>();
-      pa.n_items = s_nitems.as<unsigned long long>();
-      pa.list_count = s_lcount.as<uint32_t>();
+      pa.counts = sc.counts.as<uint32_t>();
+      pa.pair_start = sc.pstart.as<unsigned long long>();
+      pa.item_start = sc.istart.as<unsigned long long>();
+      pa.fill = sc.fill.as<uint32_t>();
+      pa.pairs = sc.pairs.as<uint32_t>();
+      pa.offsets = sc.off.as<float>();
+      pa.items = sc.items.as<uint4>();
+      pa.n_items = sc.nitems.as<unsigned long long>();
+      pa.list_count = sc.lcount.as<uint32_t>();
       eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       const size_t lists = m * max_probe * 2;
-      s_cand_s.reserve(lists * kscan * 4);
-      s_cand_i.reserve(lists * kscan * 4);
-      const float* qf = eng->d_qf.as<float>();
+      sc.cand_s.reserve(lists * kscan * 4);
+      sc.cand_i.reserve(lists * kscan * 4);
+      const float* qf = sc.flat.qf.as<float>();
       vcb::BucketScanArgs ba{};
       ba.codes = eng->d_codes.as<uint32_t>();
       ba.alpha = eng->d_alpha.as<float>();
       ba.slot_ids = d_slot_ids.as<uint32_t>();
       ba.slot_start = d_slot_start.as<unsigned long long>();
       ba.bucket_size = d_bucket_size.as<uint32_t>();
-      ba.luts = eng->d_luts.as<uint8_t>();
+      ba.luts = sc.flat.luts.as<uint8_t>();
       ba.lut_scale = qf;
       ba.fa_init = qf + 3 * m;
       ba.pairs = pa.pairs;
@@ -449,8 +484,8 @@ struct tq_bucketed {
       ba.bits = static_cast<int>(bits);
       ba.k = static_cast<int>(kscan);
       ba.max_probe = max_probe;
-      ba.cand_score = s_cand_s.as<float>();
-      ba.cand_id = s_cand_i.as<uint32_t>();
+      ba.cand_score = sc.cand_s.as<float>();
+      ba.cand_id = sc.cand_i.as<uint32_t>();
       eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
       vcb::MergeArgs mg{};
       mg.cand_score = ba.cand_score;
@@ -463,32 +498,32 @@ struct tq_bucketed {
       mg.out_id = d_ids + q0 * ke;
       mg.list_count = pa.list_count;
       if (rerank) {
-        s_rr_s.reserve(m * kscan * 4);
-        s_rr_i.reserve(m * kscan * 8);
-        mg.out_score = s_rr_s.as<float>();
-        mg.out_id = s_rr_i.as<uint64_t>();
+        sc.rr_s.reserve(m * kscan * 4);
+        sc.rr_i.reserve(m * kscan * 8);
+        mg.out_score = sc.rr_s.as<float>();
+        mg.out_id = sc.rr_i.as<uint64_t>();
         mg.pad_id = ~0ull;  // unfilled slots score -inf in the re-rank
       }
       eng->launch(tq_index::kMerge, s, "merge kernel", [&] { return vcb::launch_merge(mg, s); });
       if (rerank) {
         eng->launch(tq_index::kMerge, s, "rescore kernel", [&] {
           return vcb::launch_rescore(qh, static_cast<long long>(m), static_cast<int>(dim), d_x.as<float>(),
-                                     static_cast<long long>(n), static_cast<int>(kscan), s_rr_s.as<float>(),
-                                     s_rr_i.as<uint64_t>(), s);
+                                     static_cast<long long>(n), static_cast<int>(kscan), sc.rr_s.as<float>(),
+                                     sc.rr_i.as<uint64_t>(), s);
         });
         eng->launch(tq_index::kMerge, s, "take kernel", [&] {
-          return vcb::launch_take_columns(s_rr_s.as<float>(), s_rr_i.as<uint64_t>(), static_cast<long long>(m),
+          return vcb::launch_take_columns(sc.rr_s.as<float>(), sc.rr_i.as<uint64_t>(), static_cast<long long>(m),
                                           static_cast<int>(kscan), static_cast<int>(ke), n, d_scores + q0 * ke,
                                           d_ids + q0 * ke, s);
         });
       }
       eng->scan_queries += m;
       if (trace_off) {
-        vcb::check(cudaMemcpyAsync(trace_off + q0 * max_probe, s_off.get(), m * max_probe * 4,
+        vcb::check(cudaMemcpyAsync(trace_off + q0 * max_probe, sc.off.get(), m * max_probe * 4,
                                    cudaMemcpyDeviceToHost, s), "D2H");
-        vcb::check(cudaMemcpyAsync(trace_probe + q0 * max_probe, s_top_i.get(), m * max_probe * 4,
+        vcb::check(cudaMemcpyAsync(trace_probe + q0 * max_probe, sc.top_i.get(), m * max_probe * 4,
                                    cudaMemcpyDeviceToHost, s), "D2H");
-        vcb::check(cudaMemcpyAsync(trace_qh + q0 * dim, s_qh.get(), m * dim * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        vcb::check(cudaMemcpyAsync(trace_qh + q0 * dim, sc.qh.get(), m * dim * 4, cudaMemcpyDeviceToHost, s), "D2H");
         vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
       }
     }
@@ -708,6 +743,30 @@ int tq_bucketed_search_trace(tq_bucketed* h, const float* queries, size_t nq, si
   });
 }
 
+int tq_bucketed_search_learned_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t k,
+                                      tq_probe_mlp* mlp, float coverage, float min_confidence,
+                                      size_t fallback_n_probe, float* d_scores, uint64_t* d_ids, size_t* k_eff,
+                                      void* stream) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(mlp != nullptr, TQ_ERR_INVALID_ARGUMENT, "null model");
+    require(h->prepared, TQ_ERR_STATE, "search before prepare");
+    require(k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be <= 256");
+    const size_t ke = std::min(k, h->n);
+    if (k_eff) *k_eff = ke;
+    if (nq == 0 || ke == 0) return;
+    require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t np = fallback_n_probe ? fallback_n_probe : h->p.n_probe;
+    require(np >= 1 && np <= static_cast<size_t>(vcb::kMaxProbe), TQ_ERR_INVALID_ARGUMENT,
+            "fallback n_probe must be in [1, 2048]");
+    vcb::DeviceGuard g(h->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream();
+    const vcb::LearnedProbe lp{mlp, coverage, min_confidence};
+    h->search_device(d_queries, nq, ke, static_cast<int>(std::min<size_t>(np, h->nb)), nullptr, d_scores, d_ids, s,
+                     h->own, nullptr, nullptr, nullptr, &lp);
+  });
+}
+
 int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t p, float* d_top_scores,
                              uint32_t* d_top_ids, void* stream) {
   return vcb::guarded([&] {
@@ -721,16 +780,16 @@ int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, 
     const size_t pass = h->pass_queries();
     for (size_t q0 = 0; q0 < nq; q0 += pass) {
       const size_t m = std::min(pass, nq - q0);
-      h->s_qh.reserve(m * h->dim * 4);
+      h->own.qh.reserve(m * h->dim * 4);
       vcb::check(vcb::launch_normalize_rows(d_queries + q0 * h->dim_in, static_cast<long long>(m),
                                             static_cast<int>(h->dim_in), static_cast<int>(h->dim),
-                                            h->s_qh.as<float>(), s),
+                                            h->own.qh.as<float>(), s),
                  "normalize kernel");
-      h->s_route.reserve(m * h->nb * 4);
-      vcb::check(vcb::launch_gemm_nt(h->s_qh.as<float>(), static_cast<long long>(m), h->d_route.as<float>(), h->nb,
-                                     static_cast<int>(h->dim), h->s_route.as<float>(), h->nb, s),
+      h->own.route.reserve(m * h->nb * 4);
+      vcb::check(vcb::launch_gemm_nt(h->own.qh.as<float>(), static_cast<long long>(m), h->d_route.as<float>(), h->nb,
+                                     static_cast<int>(h->dim), h->own.route.as<float>(), h->nb, s),
                  "routing kernel");
-      vcb::check(vcb::launch_select_top(h->s_route.as<float>(), static_cast<long long>(m), h->nb, h->nb,
+      vcb::check(vcb::launch_select_top(h->own.route.as<float>(), static_cast<long long>(m), h->nb, h->nb,
                                         static_cast<int>(p), d_top_scores + q0 * p, d_top_ids + q0 * p, s),
                  "select kernel");
     }
@@ -745,20 +804,20 @@ int tq_bucketed_route(tq_bucketed* h, const float* queries, size_t nq, float* q_
     require(queries != nullptr, TQ_ERR_INVALID_ARGUMENT, "null queries");
     vcb::DeviceGuard g(h->device);
     h->s_q.reserve(nq * h->dim_in * 4);
-    h->s_qh.reserve(nq * h->dim * 4);
-    h->s_route.reserve(nq * h->nb * 4);
+    h->own.qh.reserve(nq * h->dim * 4);
+    h->own.route.reserve(nq * h->nb * 4);
     h->eng->upload(h->s_q.get(), queries, nq * h->dim_in * 4);
     vcb::check(vcb::launch_normalize_rows(h->s_q.as<float>(), static_cast<long long>(nq), static_cast<int>(h->dim_in),
-                                          static_cast<int>(h->dim), h->s_qh.as<float>(), h->stream()),
+                                          static_cast<int>(h->dim), h->own.qh.as<float>(), h->stream()),
                "normalize kernel");
-    vcb::check(vcb::launch_gemm_nt(h->s_qh.as<float>(), static_cast<long long>(nq), h->d_route.as<float>(), h->nb,
-                                   static_cast<int>(h->dim), h->s_route.as<float>(), h->nb, h->stream()),
+    vcb::check(vcb::launch_gemm_nt(h->own.qh.as<float>(), static_cast<long long>(nq), h->d_route.as<float>(), h->nb,
+                                   static_cast<int>(h->dim), h->own.route.as<float>(), h->nb, h->stream()),
                "routing kernel");
     if (q_hat) {
-      vcb::check(cudaMemcpyAsync(q_hat, h->s_qh.get(), nq * h->dim * 4, cudaMemcpyDeviceToHost, h->stream()), "D2H");
+      vcb::check(cudaMemcpyAsync(q_hat, h->own.qh.get(), nq * h->dim * 4, cudaMemcpyDeviceToHost, h->stream()), "D2H");
     }
     if (scores) {
-      vcb::check(cudaMemcpyAsync(scores, h->s_route.get(), nq * h->nb * 4, cudaMemcpyDeviceToHost, h->stream()),
+      vcb::check(cudaMemcpyAsync(scores, h->own.route.get(), nq * h->nb * 4, cudaMemcpyDeviceToHost, h->stream()),
                  "D2H");
     }
     h->sync();
@@ -834,3 +893,27 @@ int tq_bucketed_engine(tq_bucketed* h, tq_index** engine) {
 }
 
 }  // extern "C"
+
+// ---- hooks for the serving loop (tq_server.cu) ------------------------------
+namespace vcb {
+
+BucketScratch* bucket_scratch_new() { return new BucketScratch(); }
+void bucket_scratch_delete(BucketScratch* sc) { delete sc; }
+
+size_t bucketed_dim_in(const tq_bucketed* h) { return h->dim_in; }
+size_t bucketed_size(const tq_bucketed* h) { return h->n; }
+bool bucketed_prepared(const tq_bucketed* h) { return h->prepared; }
+
+// One search of nq device queries with caller-owned scratch on stream s; the
+// learned probe when lp is not null (n_probe is then its maximum / fallback).
+size_t bucketed_search_with(tq_bucketed* h, const float* d_q, size_t nq, size_t k, size_t n_probe,
+                            const LearnedProbe* lp, float* d_scores, uint64_t* d_ids, cudaStream_t s,
+                            BucketScratch& sc) {
+  const size_t ke = std::min(k, h->n);
+  if (nq == 0 || ke == 0) return ke;
+  const size_t np = std::min<size_t>(n_probe ? n_probe : h->p.n_probe, static_cast<size_t>(h->nb));
+  h->search_device(d_q, nq, ke, static_cast<int>(np), nullptr, d_scores, d_ids, s, sc, nullptr, nullptr, nullptr, lp);
+  return ke;
+}
+
+}  // namespace vcb

@@ -79,6 +79,21 @@ class DeviceGuard {
 
 inline size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
+// Device scratch of one flat search: query LUTs, per-query constants and
+// candidate lists. Grown on demand by the search.
+struct FlatScratch {
+  DeviceBuffer* luts;
+  DeviceBuffer* qf;
+  DeviceBuffer* cand_s;
+  DeviceBuffer* cand_i;
+};
+
+// Owning variant for callers that run searches concurrently (one per stream).
+struct FlatScratchStore {
+  DeviceBuffer luts, qf, cand_s, cand_i;
+  FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i}; }
+};
+
 }  // namespace vcb
 
 struct tq_index;
@@ -235,11 +250,17 @@ struct tq_index {
     n += count;
   }
 
+  // The index's own search scratch (one search at a time on one stream).
+  vcb::FlatScratch own_scratch() { return {&d_luts, &d_qf, &d_cand_s, &d_cand_i}; }
+
   // LUTs and per-query constants for nq device rows.
   void prep_queries(const float* d_q, size_t nq, cudaStream_t s, float* q_rot_out) {
-    d_luts.reserve(nq * nbg * 32);
-    d_qf.reserve(nq * 4 * sizeof(float));
-    float* qf = d_qf.as<float>();
+    prep_queries(d_q, nq, s, q_rot_out, own_scratch());
+  }
+  void prep_queries(const float* d_q, size_t nq, cudaStream_t s, float* q_rot_out, vcb::FlatScratch sc) {
+    sc.luts->reserve(nq * nbg * 32);
+    sc.qf->reserve(nq * 4 * sizeof(float));
+    float* qf = sc.qf->as<float>();
     vcb::QueryPrepArgs a{};
     a.q = d_q;
     a.nq = static_cast<long long>(nq);
@@ -253,7 +274,7 @@ struct tq_index {
     a.tqplus = calibrated;
     a.shift = d_shift.as<float>();
     a.scale = d_scale.as<float>();
-    a.luts = d_luts.as<uint8_t>();
+    a.luts = sc.luts->as<uint8_t>();
     a.lut_scale = qf;
     a.lut_bias = qf + nq;
     a.bias_corr = qf + 2 * nq;
@@ -266,25 +287,31 @@ struct tq_index {
   // Full device search of nq rows at d_q into d_scores/d_ids (stride k_eff).
   void search_device(const float* d_q, size_t nq, size_t k, float* d_scores, uint64_t* d_ids,
                      size_t k_eff, cudaStream_t s) {
+    search_device(d_q, nq, k, d_scores, d_ids, k_eff, s, own_scratch());
+  }
+  // Same with caller-owned scratch: searches with distinct scratch may run
+  // concurrently on distinct streams (the index data is only read).
+  void search_device(const float* d_q, size_t nq, size_t k, float* d_scores, uint64_t* d_ids,
+                     size_t k_eff, cudaStream_t s, vcb::FlatScratch sc) {
     if (nq == 0 || k_eff == 0) return;
     // Bound the scratch per pass: LUTs + candidate lists.
     const size_t max_pass = 1 << 16;
     for (size_t q0 = 0; q0 < nq; q0 += max_pass) {
       const size_t m = std::min(max_pass, nq - q0);
-      prep_queries(d_q + q0 * dim, m, s, nullptr);
+      prep_queries(d_q + q0 * dim, m, s, nullptr, sc);
       vcb::ScanPlan plan;
       if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
                           static_cast<int>(k_eff), sms, &plan)) {
         vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
       }
       const size_t lists = static_cast<size_t>(plan.n_ranges) * plan.lists_per_range;
-      d_cand_s.reserve(m * lists * k_eff * 4);
-      d_cand_i.reserve(m * lists * k_eff * 4);
-      const float* qf = d_qf.as<float>();
+      sc.cand_s->reserve(m * lists * k_eff * 4);
+      sc.cand_i->reserve(m * lists * k_eff * 4);
+      const float* qf = sc.qf->as<float>();
       vcb::ScanArgs a{};
       a.codes = d_codes.as<uint32_t>();
       a.alpha = d_alpha.as<float>();
-      a.luts = d_luts.as<uint8_t>();
+      a.luts = sc.luts->as<uint8_t>();
       a.lut_scale = qf;
       a.fa_init = qf + 3 * m;
       a.n = static_cast<long long>(n);
@@ -296,8 +323,8 @@ struct tq_index {
       a.n_ranges = plan.n_ranges;
       a.lut_chunk_groups = plan.lut_chunk_groups;
       a.bits = static_cast<int>(bits);
-      a.cand_score = d_cand_s.as<float>();
-      a.cand_id = d_cand_i.as<uint32_t>();
+      a.cand_score = sc.cand_s->as<float>();
+      a.cand_id = sc.cand_i->as<uint32_t>();
       launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
       scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
       scan_queries += m;

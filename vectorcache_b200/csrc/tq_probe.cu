@@ -27,6 +27,7 @@
 #include "../../include/vectorcache_b200.h"
 #include "tq_abi.h"
 #include "tq_index_impl.h"
+#include "tq_probe.h"
 
 namespace vcb {
 namespace {
@@ -361,6 +362,40 @@ struct tq_probe_mlp {
   }
 };
 
+namespace vcb {
+
+void probe_predict(tq_probe_mlp* h, const float* d_top, size_t m, int p, float coverage, float min_conf,
+                   uint32_t fallback, uint32_t* d_out, cudaStream_t s, ProbeScratch& sc) {
+  if (m == 0) return;
+  const long long M = static_cast<long long>(m);
+  int widest = 1;
+  for (int l = 0; l < h->n_lin(); ++l) widest = std::max(widest, h->fan_out[l]);
+  sc.x.reserve(m * kInputs * 2);
+  sc.z.reserve(m * widest * 4);
+  sc.act0.reserve(m * widest * 2);
+  sc.act1.reserve(m * widest * 2);
+  features_kernel<<<static_cast<unsigned>(m), 256, 0, s>>>(d_top, M, p, h->d_mu.as<float>(), h->d_isd.as<float>(),
+                                                           sc.x.as<bf16>(), nullptr);
+  check(cudaGetLastError(), "features kernel");
+  const bf16* in = sc.x.as<bf16>();
+  for (int l = 0; l < h->n_lin(); ++l) {
+    const int K = h->fan_in[l], N = h->fan_out[l];
+    check(gemm(in, K, 1, h->wbf(l), N, 1, sc.z.as<float>(), N, M, N, K, s), "mlp gemm");
+    const bool last = l + 1 == h->n_lin();
+    bf16* out = (l & 1) ? sc.act1.as<bf16>() : sc.act0.as<bf16>();
+    bias_act_kernel<<<blocks(M * N), 256, 0, s>>>(sc.z.as<float>(), M, N, h->bias(l), last ? nullptr : out);
+    check(cudaGetLastError(), "bias kernel");
+    in = out;
+  }
+  predict_kernel<<<blocks(M), 256, 0, s>>>(sc.z.as<float>(), M, h->n_classes, h->d_classes.as<uint32_t>(), coverage,
+                                           min_conf, fallback, d_out, nullptr);
+  check(cudaGetLastError(), "predict kernel");
+}
+
+uint32_t probe_max_class(const tq_probe_mlp* h) { return h->classes.back(); }
+
+}  // namespace vcb
+
 namespace {
 
 using vcb::require;
@@ -555,16 +590,21 @@ int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint3
 }
 
 int tq_probe_mlp_train_step_device(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels, size_t m,
-                                   size_t p, float lr, float* loss) {
+                                   size_t p, float lr, float* loss, void* stream) {
   return vcb::guarded([&] {
     checked(h);
     require(d_top_scores && d_labels, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
     require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
     vcb::DeviceGuard g(h->device);
-    h->forward(d_top_scores, m, static_cast<int>(p), h->stream);
-    const float l = h->backward(d_labels, m, h->stream);
-    h->adam(lr, h->stream);
+    // On the caller's stream (where the batch was produced); the step ends
+    // with the loss read back, so it returns with its work complete.
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    if (s != h->stream) h->sync();
+    h->forward(d_top_scores, m, static_cast<int>(p), s);
+    const float l = h->backward(d_labels, m, s);
+    h->adam(lr, s);
+    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     if (loss) *loss = l;
   });
 }

@@ -43,7 +43,7 @@ def _declare_probe(lib):
         "tq_probe_mlp_set_params": (C.c_int, [_P, _P]),
         "tq_probe_mlp_forward": (C.c_int, [_P, _P, _SZ, _SZ, _P]),
         "tq_probe_mlp_gradients": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.POINTER(C.c_float), _P]),
-        "tq_probe_mlp_train_step_device": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.c_float, C.POINTER(C.c_float)]),
+        "tq_probe_mlp_train_step_device": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.c_float, C.POINTER(C.c_float), _P]),
         "tq_probe_mlp_predict_device": (C.c_int, [_P, _P, _SZ, _SZ, C.c_float, C.c_float, C.c_uint32, _P, _P, _P]),
         "tq_probe_mlp_synchronize": (C.c_int, [_P]),
     }
@@ -124,10 +124,10 @@ class ProbeMLP:
                                                 C.byref(loss), _ptr(g)))
         return loss.value, g
 
-    def train_step_device(self, d_top, d_labels, m: int, p: int, lr: float) -> float:
+    def train_step_device(self, d_top, d_labels, m: int, p: int, lr: float, stream=None) -> float:
         loss = C.c_float()
         _check(self._lib.tq_probe_mlp_train_step_device(self._h, _dev(d_top)[0], _dev(d_labels)[0], m, p, lr,
-                                                        C.byref(loss)))
+                                                        C.byref(loss), _stream_ptr(stream)))
         return loss.value
 
     def predict_device(self, d_top, m: int, p: int, d_out, coverage: float = 0.9, min_confidence: float = 0.0,
