@@ -53,9 +53,11 @@ def parse():
     p.add_argument("--recall-queries", type=int, default=1000)
     p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["flat", "bucketed"], default="flat",
+    p.add_argument("--workload", choices=["flat", "bucketed", "serving"], default="flat",
                    help="flat: the 1M x 1536 flat search (default); bucketed: the 1.2M x 100 bucketed index, "
-                        "learned n_probe against fixed n_probe = 64")
+                        "learned n_probe against fixed n_probe; serving: the continuous-batching server over a "
+                        "10M x 768 flat index and the bucketed index")
+    p.add_argument("--serving-flat-n", type=int, default=10_000_000)
     p.add_argument("--bucketed-n", type=int, default=1_200_000)
     p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
     p.add_argument("--rerank", type=int, default=100, help="bucketed: candidates re-ranked exactly (0 = off)")
@@ -615,11 +617,168 @@ def run_bucketed(args, world, rank, local):
     idx.close()
 
 
+SERVING_RATES = (5_000, 20_000, 50_000, 100_000, 200_000)
+
+
+def run_serving(args, world, rank, local):
+    """Serving loop workload: a resident flat index (10M x 768, 3-bit, power-law
+    vectors) plus the bucketed index of the bucketed workload (1.2M x 100 vMF,
+    4-bit, re-rank 100) behind one server (HBM budget 120 GB, 4 slots,
+    max_batch 1024). Requests arrive as a Poisson process in bursts of 1-256
+    queries (k = 10 or 64 at equal odds; 1% of the queries go to the flat
+    index); each rate is replayed open-loop twice: bucketed requests at the
+    fixed n_probe that reaches Recall@10 >= 0.95, then with the learned probe.
+    Reported per rate: p50/p99 latency, achieved QPS, bucketed Recall@10."""
+    import torch
+
+    import vectorcache_b200 as vcb
+    from vectorcache_b200.probe import ProbeMLP, probe_labels, recall_rows
+    from vectorcache_b200.synthetic import power_law_torch, vmf_mixture
+
+    if world > 1:
+        raise SystemExit("--workload serving runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    t0 = time.perf_counter()
+    flat_n, flat_dim = args.serving_flat_n, 768
+    flat = vcb.TurboQuantIndex(flat_dim, 3, device=local)
+    chunk = 1_000_000
+    for s in range(0, flat_n, chunk):
+        x = power_law_torch(min(chunk, flat_n - s), flat_dim, seed=2000 + s // chunk, device=device)
+        if s == 0:
+            flat.calibrate_device(x[:10_000])
+        flat.add_device(x)
+        del x
+    flat.prepare()
+    torch.cuda.empty_cache()
+    flat_q = power_law_torch(2048, flat_dim, seed=77, device=device).cpu().numpy()
+    flat_build_s = time.perf_counter() - t0
+
+    dim, n, nq, k = 100, args.bucketed_n, args.nq, 10
+    db = vmf_mixture(n, dim, seed=31)
+    test_q = vmf_mixture(nq, dim, seed=32)
+    train_q = vmf_mixture(args.bucketed_train, dim, seed=33)
+    bkt = vcb.BucketedTurboQuantIndex(dim, 4, vcb.BucketParams(max_bucket_size=800, energy_soft=400, expected_n=n,
+                                                               rerank_k=args.rerank), device=local)
+    bkt.add(db)
+    bkt.prepare()
+    x = torch.from_numpy(db).to(device)
+
+    def exact(q):
+        out = []
+        for s in range(0, q.shape[0], 4096):
+            qq = torch.from_numpy(q[s:s + 4096]).to(device)
+            out.append(torch.topk(qq @ x.T, k, dim=1).indices.cpu().numpy())
+        return np.concatenate(out)
+
+    ex_test, ex_train = exact(test_q), exact(train_q)
+    del x
+    torch.cuda.empty_cache()
+    # fixed operating point: smallest n_probe with Recall@10 >= 0.95
+    p_op = FIXED_PROBES[-1]
+    for p in FIXED_PROBES:
+        if recall_rows(bkt.search(test_q, k, n_probe=p).ids, ex_test, k).mean() >= RECALL_TARGET:
+            p_op = p
+            break
+    classes = tuple(c for c in PROBE_CLASSES if c <= p_op)
+    labels, _ = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
+    mlp = ProbeMLP(classes=classes, hidden=128, layers=2, seed=17, device=local)
+    d_train = torch.from_numpy(train_q).to(device)
+    tr_s = torch.empty((train_q.shape[0], 256), dtype=torch.float32, device=device)
+    tr_i = torch.empty((train_q.shape[0], 256), dtype=torch.int32, device=device)
+    bkt.route_device(d_train, 256, tr_s, tr_i)
+    torch.cuda.synchronize()
+    raw = mlp.features(tr_s.cpu().numpy())
+    mlp.set_normalization(raw.mean(axis=0), raw.std(axis=0) + 1e-6)
+    d_lab = torch.from_numpy(labels.astype(np.int32)).to(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(5)
+    for epoch in range(args.epochs):
+        perm = torch.randperm(train_q.shape[0], device=device, generator=gen)
+        for s in range(0, train_q.shape[0], 512):
+            sel = perm[s:s + 512]
+            mlp.train_step_device(tr_s[sel].contiguous(), d_lab[sel].contiguous(), sel.numel(), 256, 2e-3)
+    # learned operating point: the lowest coverage whose Recall@10 reaches the target
+    cov_op = 0.98
+    d_q = torch.from_numpy(test_q).to(device)
+    d_s = torch.empty((nq, k), dtype=torch.float32, device=device)
+    d_i = torch.empty((nq, k), dtype=torch.int64, device=device)
+    for cov in (0.7, 0.8, 0.9, 0.95, 0.98):
+        bkt.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=cov, fallback_n_probe=p_op)
+        torch.cuda.synchronize()
+        if recall_rows(d_i.cpu().numpy(), ex_test, k).mean() >= RECALL_TARGET:
+            cov_op = cov
+            break
+
+    srv = vcb.Server(device=local, hbm_budget_bytes=120 << 30, max_slots=4, max_batch=1024)
+    t_flat = srv.add_flat(flat, 64)
+    t_fixed = srv.add_bucketed(bkt, 64, p_op)
+    t_learn = srv.add_bucketed(bkt, 64, p_op, mlp=mlp, coverage=cov_op)
+    srv.start()
+    info = srv.info()
+    rng = np.random.default_rng(11)
+    per_rate = []
+    for rate in SERVING_RATES:
+        budget_q = min(40_000, int(rate * 2.0))
+        t, base = 0.0, []
+        total = 0
+        while total < budget_q:
+            nb_q = int(rng.integers(1, 257))
+            t += rng.exponential(nb_q / rate * 1e6)
+            kk = int(rng.choice([10, 64]))
+            if rng.random() < 0.01:
+                rows = rng.integers(0, flat_q.shape[0], nb_q)
+                base.append((t, "flat", rows, kk))
+            else:
+                rows = rng.integers(0, nq, nb_q)
+                base.append((t, "bkt", rows, kk))
+            total += nb_q
+        row = {"rate_qps": rate, "queries": total, "requests": len(base)}
+        for mode, target in (("fixed", t_fixed), ("learned", t_learn)):
+            trace = [(tt, t_flat if kind == "flat" else target, (flat_q if kind == "flat" else test_q)[rows], kk,
+                      0 if kind == "flat" else p_op) for tt, kind, rows, kk in base]
+            lat, wall, results = srv.replay(trace)
+            lat_ms = lat / 1e3
+            is_b = np.array([kind == "bkt" for _, kind, _, _ in base])
+            hits = tot = 0
+            for (tt, kind, rows, kk), (s_, i_) in zip(base, results):
+                if kind == "bkt":
+                    hits += recall_rows(i_[:, :k], ex_test[rows], k).sum() * k
+                    tot += rows.size * k
+            row[mode] = {"qps": total / wall, "wall_s": wall, "p50_ms": float(np.percentile(lat_ms, 50)),
+                         "p99_ms": float(np.percentile(lat_ms, 99)),
+                         "bucketed_p50_ms": float(np.percentile(lat_ms[is_b], 50)),
+                         "bucketed_p99_ms": float(np.percentile(lat_ms[is_b], 99)),
+                         "flat_p99_ms": float(np.percentile(lat_ms[~is_b], 99)) if (~is_b).any() else None,
+                         "bucketed_recall_at_10": hits / max(tot, 1)}
+        per_rate.append(row)
+    best = max(per_rate, key=lambda r: r["learned"]["qps"])
+    line = {
+        "metric": "serving QPS and p50/p99 latency (10Mx768 3-bit flat + 1.2Mx100 bucketed, Poisson bursts 1-256)",
+        "value": best["learned"]["qps"], "unit": "queries/s", "n_gpus": 1, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"serving: flat {flat_n}x{flat_dim} 3-bit + bucketed {n}x{dim} 4-bit, HBM budget "
+                               f"120 GB, rates {list(SERVING_RATES)} q/s", "slots": info["slots"],
+                   "slot_bytes": info["slot_bytes"], "resident_bytes": info["resident_bytes"],
+                   "fixed_n_probe": p_op, "learned_coverage": cov_op, "flat_build_s": flat_build_s},
+        "per_rate": per_rate, "server_stats": srv.stats(),
+    }
+    print(json.dumps(line), flush=True)
+    srv.close()
+    mlp.close()
+    bkt.close()
+    flat.close()
+
+
 def main():
     args = parse()
     if args.workload == "bucketed":
         world, rank, local = dist_setup(args)
         run_bucketed(args, world, rank, local)
+        return
+    if args.workload == "serving":
+        world, rank, local = dist_setup(args)
+        run_serving(args, world, rank, local)
         return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
