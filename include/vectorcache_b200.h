@@ -378,6 +378,38 @@ typedef struct tq_replay_item {
 int tq_server_replay(tq_server* h, const tq_replay_item* items, size_t n, double* latency_us,
                      double* wall_s);
 
+/* ---- multi-index launch -----------------------------------------------------
+ * No counterpart in the reference. One persistent scan launch serves many
+ * prepared flat indexes (same device; any n, dim, bits) with per-index batch
+ * sizes and k: work items (index, vector range, up to 8 queries) are pulled
+ * from a global counter by a fixed grid of CTAs. tq_multi_plan fixes the batch
+ * size nq[i] and k[i] of every index, sizes all scratch, optionally autotunes
+ * the item range length and resident CTAs per SM (timed on the planned
+ * workload), and captures query-LUT kernels + scan + merges into one CUDA
+ * graph; tq_multi_launch replays it. Queries go into the device buffers given
+ * by tq_multi_buffers (nq[i] x dim_i floats) before a launch; results come out
+ * as nq[i] x k_eff rows, identical to tq_index_search on each index. */
+typedef struct tq_multi tq_multi;
+
+int tq_multi_create(tq_index* const* indexes, size_t n_indexes, tq_multi** out);
+int tq_multi_destroy(tq_multi* h);
+int tq_multi_plan(tq_multi* h, const size_t* nq, const size_t* k, int autotune);
+int tq_multi_buffers(tq_multi* h, size_t i, float** d_queries, float** d_scores, uint64_t** d_ids,
+                     size_t* k_eff);
+/* Graph launch on `stream` (NULL: the multi-index object's stream). */
+int tq_multi_launch(tq_multi* h, void* stream);
+/* The same sequence issued kernel by kernel (no graph), for comparison. */
+int tq_multi_run_uncaptured(tq_multi* h, void* stream);
+int tq_multi_synchronize(tq_multi* h);
+/* Chosen configuration; tuned_ms receives up to *n_tuned candidate timings
+ * (on return *n_tuned = candidates timed). */
+int tq_multi_config(tq_multi* h, long long* range_vectors, int* ctas, size_t* n_items, size_t* smem_bytes,
+                    double* tuned_ms, size_t* n_tuned);
+/* Synchronous copies into / out of the library's device buffers (for callers
+ * without their own CUDA runtime). */
+int tq_copy_to_device(void* d_dst, const void* src, size_t bytes);
+int tq_copy_to_host(void* dst, const void* d_src, size_t bytes);
+
 /* ---- search without device allocation --------------------------------------
  * No counterpart in the reference.
  *

@@ -20,7 +20,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libvectorcache_b200.so"
 SOURCES = ["tq_host_math.cpp", "tq_formats.cpp", "tq_encode.cu", "tq_query.cu", "tq_scan.cu", "tq_bigdim.cu",
-           "tq_bucket.cu", "tq_bucketed.cu", "tq_probe.cu", "tq_server.cu",
+           "tq_bucket.cu", "tq_bucketed.cu", "tq_probe.cu", "tq_server.cu", "tq_multi.cu",
            "tq_rescore.cu", "tq_index.cu"]
 HEADERS = ["tq_host_math.h", "tq_kernels.h", "tq_device.cuh", "tq_abi.h", "tq_index_impl.h", "tq_bucket.h",
            "tq_probe.h", "tq_serving_hooks.h"]

@@ -725,42 +725,40 @@ __device__ __forceinline__ float lane_jth_largest(const float (&sc)[8], unsigned
   return out;
 }
 
+// One scan work item: up to kItemQueries queries against one range of slots
+// of a scan layout (a probed bucket, or a vector range of a flat index).
+struct ItemView {
+  const uint32_t* codes;
+  const float* alpha;
+  const uint32_t* slot_ids;  // original id per slot; nullptr: the id is the slot
+  long long slot0;           // multiple of kBucketSlotAlign
+  int size;                  // slots of the range
+  int nbg;
+  const uint8_t* luts;       // LUT rows (nbg x 32 bytes each)
+  int k;
+  int pc;                    // queries of the item
+  float* cand_s;
+  uint32_t* cand_i;
+};
+
+// The item's queries, in shared memory (filled by the calling kernel).
+struct ItemQueries {
+  int q[kItemQueries];           // LUT row (-1: no query)
+  long long list[kItemQueries];  // candidate list written by tile set 0 (tile set 1: list + 1)
+  float scale[kItemQueries], init[kItemQueries], off[kItemQueries];
+};
+
+// Scans one item with the CTA's 4 warps (2 query quads x 2 tile sets) and
+// writes one sorted candidate list of k per (query, tile set).
 template <bool NIBBLE8>
-__global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_q[kItemQueries];
-  __shared__ uint32_t s_pair[kItemQueries];
-  __shared__ float s_scale[kItemQueries], s_init[kItemQueries], s_off[kItemQueries];
-  if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
-  const uint4 it = a.items[blockIdx.x];
-  const int b = static_cast<int>(it.x);
-  const int pc = static_cast<int>(it.z);
-  const int nbg = a.nbg, k = a.k;
+__device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& iq, unsigned char* smem) {
+  const int nbg = v.nbg, k = v.k, pc = v.pc;
   const int chunk = nbg < kFlushGroups ? nbg : kFlushGroups;
   const bool resident = chunk >= nbg;
-  if (threadIdx.x < kItemQueries) {
-    const int t = threadIdx.x;
-    if (t < pc) {
-      const uint32_t pr = a.pairs[it.y + t];
-      const int q = static_cast<int>(pr / static_cast<uint32_t>(a.max_probe));
-      s_q[t] = q;
-      s_pair[t] = pr;
-      s_scale[t] = a.lut_scale[q];
-      s_init[t] = a.fa_init[q];
-      s_off[t] = a.offsets[pr];
-    } else {
-      s_q[t] = -1;
-      s_pair[t] = 0u;
-      s_scale[t] = 0.f;
-      s_init[t] = 0.f;
-      s_off[t] = 0.f;
-    }
-  }
-  __syncthreads();
 
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [kItemQueries][chunk][2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int kmax = a.k <= 32 ? 32 : (a.k <= 64 ? 64 : 256);
+  const int kmax = k <= 32 ? 32 : (k <= 64 ? 64 : 256);
   // Per-warp top-k lists and sort buffer after the LUT area.
   unsigned char* warp_area = smem + static_cast<size_t>(kItemQueries) * chunk * 32 +
                              warp * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
@@ -774,8 +772,8 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
     for (int t = threadIdx.x; t < kItemQueries * halves; t += blockDim.x) {
       const int q = t / halves, r = t % halves;
       LutHalf h = {{0u, 0u, 0u, 0u}};
-      if (s_q[q] >= 0) {
-        h = *reinterpret_cast<const LutHalf*>(a.luts + (static_cast<long long>(s_q[q]) * nbg + g_first) * 32LL +
+      if (iq.q[q] >= 0) {
+        h = *reinterpret_cast<const LutHalf*>(v.luts + (static_cast<long long>(iq.q[q]) * nbg + g_first) * 32LL +
                                               r * 16LL);
       }
       s_lut[q * chunk * 2 + r] = h;
@@ -788,17 +786,17 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
 
   const int quad = warp & 1, tset = warp >> 1;
   const bool quad_ok = quad * 4 < pc;
-  const unsigned long long slot0 = a.slot_start[b];
-  const int size = static_cast<int>(a.bucket_size[b]);
+  const unsigned long long slot0 = static_cast<unsigned long long>(v.slot0);
+  const int size = v.size;
   const int n_sub = (size + kBucketSlotAlign - 1) / kBucketSlotAlign;
   float scale[4], init[4], off[4], thr_s[4];
   uint32_t thr_i[4];
   int cnt[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    scale[q] = s_scale[quad * 4 + q];
-    init[q] = s_init[quad * 4 + q];
-    off[q] = s_off[quad * 4 + q];
+    scale[q] = iq.scale[quad * 4 + q];
+    init[q] = iq.init[quad * 4 + q];
+    off[q] = iq.off[quad * 4 + q];
     thr_s[q] = -FLT_MAX;
     thr_i[q] = 0xffffffffu;
     cnt[q] = 0;
@@ -814,7 +812,7 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
     const long long sub = static_cast<long long>(slot0 / kBucketSlotAlign) + st;
     const long long tile = sub >> 1;
     const int half = static_cast<int>(sub & 1);
-    const uint2* wp = reinterpret_cast<const uint2*>(a.codes + tile * nbg * kTileWords + half * 64) + lane;
+    const uint2* wp = reinterpret_cast<const uint2*>(v.codes + tile * nbg * kTileWords + half * 64) + lane;
     const long long vbase = sub * kBucketSlotAlign + 8 * lane;
     float fa[4][8];
     uint32_t acc[4][8];
@@ -914,14 +912,19 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
     float al[8];
     uint32_t ids[8];
     {
-      const float4 x0 = *reinterpret_cast<const float4*>(a.alpha + vbase);
-      const float4 x1 = *reinterpret_cast<const float4*>(a.alpha + vbase + 4);
+      const float4 x0 = *reinterpret_cast<const float4*>(v.alpha + vbase);
+      const float4 x1 = *reinterpret_cast<const float4*>(v.alpha + vbase + 4);
       al[0] = x0.x; al[1] = x0.y; al[2] = x0.z; al[3] = x0.w;
       al[4] = x1.x; al[5] = x1.y; al[6] = x1.z; al[7] = x1.w;
-      const uint4 i0 = *reinterpret_cast<const uint4*>(a.slot_ids + vbase);
-      const uint4 i1 = *reinterpret_cast<const uint4*>(a.slot_ids + vbase + 4);
-      ids[0] = i0.x; ids[1] = i0.y; ids[2] = i0.z; ids[3] = i0.w;
-      ids[4] = i1.x; ids[5] = i1.y; ids[6] = i1.z; ids[7] = i1.w;
+      if (v.slot_ids) {
+        const uint4 i0 = *reinterpret_cast<const uint4*>(v.slot_ids + vbase);
+        const uint4 i1 = *reinterpret_cast<const uint4*>(v.slot_ids + vbase + 4);
+        ids[0] = i0.x; ids[1] = i0.y; ids[2] = i0.z; ids[3] = i0.w;
+        ids[4] = i1.x; ids[5] = i1.y; ids[6] = i1.z; ids[7] = i1.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) ids[j] = static_cast<uint32_t>(vbase + j);
+      }
     }
     unsigned valid = 0;
 #pragma unroll
@@ -1000,18 +1003,98 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
       __syncwarp();
     }
   }
-  // Publish: list (pair * 2 + tile set) of every valid query of this warp.
+  // Publish the list (tile set 0's list + tile set) of every valid query of this warp.
   if (!quad_ok) return;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     if (quad * 4 + q >= pc) break;
-    const long long list = static_cast<long long>(s_pair[quad * 4 + q]) * 2 + tset;
-    float* os = a.cand_score + list * k;
-    uint32_t* oi = a.cand_id + list * k;
+    const long long list = iq.list[quad * 4 + q] + tset;
+    float* os = v.cand_s + list * k;
+    uint32_t* oi = v.cand_i + list * k;
     for (int t = lane; t < k; t += kWarp) {
       const bool have = t < cnt[q];
       os[t] = have ? list_s[q * kmax + t] : -INFINITY;
       oi[t] = have ? list_i[q * kmax + t] : 0xffffffffu;
+    }
+  }
+}
+
+template <bool NIBBLE8>
+__global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ ItemQueries iq;
+  if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
+  const uint4 it = a.items[blockIdx.x];
+  const int b = static_cast<int>(it.x);
+  const int pc = static_cast<int>(it.z);
+  if (threadIdx.x < kItemQueries) {
+    const int t = threadIdx.x;
+    if (t < pc) {
+      const uint32_t pr = a.pairs[it.y + t];
+      const int q = static_cast<int>(pr / static_cast<uint32_t>(a.max_probe));
+      iq.q[t] = q;
+      iq.list[t] = static_cast<long long>(pr) * 2;
+      iq.scale[t] = a.lut_scale[q];
+      iq.init[t] = a.fa_init[q];
+      iq.off[t] = a.offsets[pr];
+    } else {
+      iq.q[t] = -1;
+      iq.list[t] = 0;
+      iq.scale[t] = 0.f;
+      iq.init[t] = 0.f;
+      iq.off[t] = 0.f;
+    }
+  }
+  __syncthreads();
+  const ItemView v{a.codes, a.alpha, a.slot_ids, static_cast<long long>(a.slot_start[b]),
+                   static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id};
+  scan_item<NIBBLE8>(v, iq, smem);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-index persistent scan: a fixed grid of CTAs pulls work items — (flat
+// index, vector range, up to 8 of its queries) — from a global counter until
+// none is left, so one launch serves indexes of any n, dim and bits.
+// ---------------------------------------------------------------------------
+template <bool ANY3, bool ANY24>
+__global__ void __launch_bounds__(kBsWarps * 32) multi_scan_kernel(MultiScanArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ ItemQueries iq;
+  __shared__ long long s_item;
+  while (true) {
+    __syncthreads();  // the previous item is done with iq and the LUT area
+    if (threadIdx.x == 0) s_item = static_cast<long long>(atomicAdd(a.next_item, 1ull));
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= a.n_items) return;
+    const MultiItem it = a.items[item];
+    const MultiIndexDesc d = a.indexes[it.index];
+    if (threadIdx.x < kItemQueries) {
+      const int t = threadIdx.x;
+      if (t < it.n_queries) {
+        const int q = it.first_query + t;
+        iq.q[t] = q;
+        iq.list[t] = (static_cast<long long>(q) * d.n_ranges + it.range) * 2;
+        iq.scale[t] = d.lut_scale[q];
+        iq.init[t] = d.fa_init[q];
+        iq.off[t] = 0.f;
+      } else {
+        iq.q[t] = -1;
+        iq.list[t] = 0;
+        iq.scale[t] = 0.f;
+        iq.init[t] = 0.f;
+        iq.off[t] = 0.f;
+      }
+    }
+    __syncthreads();
+    const long long slot0 = static_cast<long long>(it.range) * d.range_vectors;
+    const long long left = d.n - slot0;
+    const int size = static_cast<int>(left < d.range_vectors ? left : d.range_vectors);
+    const ItemView v{d.codes, d.alpha, nullptr, slot0, size, d.nbg, d.luts, d.k, it.n_queries, d.cand_s, d.cand_i};
+    if (ANY3 && d.bits == 3) {
+      scan_item<true>(v, iq, smem);
+    } else if (ANY24) {
+      scan_item<false>(v, iq, smem);
     }
   }
 }
@@ -1208,6 +1291,37 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   item_build_kernel<<<static_cast<unsigned>((a.nb + 255) / 256), 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+size_t multi_scan_smem_bytes(int max_nbg, int max_k) {
+  const int chunk = max_nbg < kFlushGroups ? max_nbg : kFlushGroups;
+  const int kmax = max_k <= 32 ? 32 : (max_k <= 64 ? 64 : 256);
+  return static_cast<size_t>(kItemQueries) * chunk * 32 +
+         static_cast<size_t>(kBsWarps) * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
+}
+
+int multi_scan_ctas_per_sm(size_t smem_bytes, bool any3) {
+  int blocks = 0;
+  auto kern = any3 ? multi_scan_kernel<true, true> : multi_scan_kernel<false, true>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes)) !=
+      cudaSuccess) {
+    return 0;
+  }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kBsWarps * 32, smem_bytes) != cudaSuccess) {
+    return 0;
+  }
+  return blocks;
+}
+
+cudaError_t launch_multi_scan(const MultiScanArgs& a, int ctas, size_t smem_bytes, bool any3, bool any24,
+                              cudaStream_t stream) {
+  if (a.n_items <= 0 || ctas <= 0) return cudaSuccess;
+  auto kern = any3 ? (any24 ? multi_scan_kernel<true, true> : multi_scan_kernel<true, false>)
+                   : multi_scan_kernel<false, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes));
+  if (e != cudaSuccess) return e;
+  kern<<<ctas, kBsWarps * 32, smem_bytes, stream>>>(a);
   return cudaGetLastError();
 }
 

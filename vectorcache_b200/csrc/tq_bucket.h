@@ -144,4 +144,41 @@ struct BucketScanArgs {
 };
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
 
+// ---- multi-index persistent scan (tq_multi.cu) -----------------------------
+// One flat index of a multi-index launch: its scan layout, its queries' LUTs
+// and constants, and where its candidate lists go: list ((q * n_ranges +
+// range) * 2 + tile set), k entries each.
+struct MultiIndexDesc {
+  const uint32_t* codes;
+  const float* alpha;
+  long long n;
+  long long range_vectors;  // multiple of kBucketSlotAlign
+  int n_ranges;
+  int nbg, bits, k;
+  const uint8_t* luts;
+  const float* lut_scale;
+  const float* fa_init;
+  float* cand_s;
+  uint32_t* cand_i;
+};
+struct MultiItem {
+  int index;
+  int range;
+  int first_query;
+  int n_queries;  // <= kItemQueries
+};
+struct MultiScanArgs {
+  const MultiIndexDesc* indexes;
+  const MultiItem* items;
+  long long n_items;
+  unsigned long long* next_item;  // zeroed before the launch
+};
+// Persistent launch: `ctas` CTAs pull items until none is left. smem_bytes:
+// multi_scan_smem_bytes of the largest nbg and k among the indexes.
+size_t multi_scan_smem_bytes(int max_nbg, int max_k);
+cudaError_t launch_multi_scan(const MultiScanArgs& a, int ctas, size_t smem_bytes, bool any3, bool any24,
+                              cudaStream_t stream);
+// Resident CTAs per SM of the multi-index scan for a given shared-memory size.
+int multi_scan_ctas_per_sm(size_t smem_bytes, bool any3);
+
 }  // namespace vcb
