@@ -53,10 +53,11 @@ def parse():
     p.add_argument("--recall-queries", type=int, default=1000)
     p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["flat", "bucketed", "serving"], default="flat",
+    p.add_argument("--workload", choices=["flat", "bucketed", "serving", "multi"], default="flat",
                    help="flat: the 1M x 1536 flat search (default); bucketed: the 1.2M x 100 bucketed index, "
                         "learned n_probe against fixed n_probe; serving: the continuous-batching server over a "
-                        "10M x 768 flat index and the bucketed index")
+                        "10M x 768 flat index and the bucketed index; multi: 32 flat indexes in one persistent "
+                        "graph-captured launch")
     p.add_argument("--serving-flat-n", type=int, default=10_000_000)
     p.add_argument("--bucketed-n", type=int, default=1_200_000)
     p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
@@ -770,8 +771,109 @@ def run_serving(args, world, rank, local):
     flat.close()
 
 
+def run_multi(args, world, rank, local):
+    """Multi-index workload: 32 flat indexes with n log-uniform in [10k, 2M],
+    dim in {128, 384, 768, 1536}, bits in {2, 3, 4} (power-law vectors at each
+    dim), query batches log-uniform in [1, 4096], k in {10, 64}. One step =
+    one search of every index's batch: (a) index by index on one stream, (b)
+    the one persistent graph-captured multi-index launch (autotuned). Results
+    of (b) are checked against (a) for every index."""
+    import torch
+
+    import vectorcache_b200 as vcb
+    from vectorcache_b200.multi import MultiIndex
+    from vectorcache_b200.synthetic import power_law_torch
+
+    if world > 1:
+        raise SystemExit("--workload multi runs on one GPU")
+    device = torch.device("cuda", local)
+    rng = np.random.default_rng(3)
+    n_idx = 32
+    specs = []
+    for j in range(n_idx):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        dim = int(rng.choice([128, 384, 768, 1536]))
+        bits = int(rng.choice([2, 3, 4]))
+        nq = int(np.exp(rng.uniform(0.0, np.log(4096))))
+        k = int(rng.choice([10, 64]))
+        specs.append((n, dim, bits, nq, k))
+    t0 = time.perf_counter()
+    idxs, queries = [], []
+    for j, (n, dim, bits, nq, k) in enumerate(specs):
+        idx = vcb.TurboQuantIndex(dim, bits, device=local)
+        for s in range(0, n, 1 << 20):
+            x = power_law_torch(min(1 << 20, n - s), dim, seed=5000 + 97 * j + s, device=device)
+            idx.add_device(x)
+            del x
+        idx.prepare()
+        idxs.append(idx)
+        queries.append(power_law_torch(nq, dim, seed=9000 + j, device=device))
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    total_q = sum(s[3] for s in specs)
+    stream = torch.cuda.Stream(device=device)
+    torch.cuda.set_stream(stream)
+    outs = [(torch.empty((s[3], s[4]), dtype=torch.float32, device=device),
+             torch.empty((s[3], s[4]), dtype=torch.int64, device=device)) for s in specs]
+
+    def seq_step():
+        for idx, q, (o_s, o_i), s in zip(idxs, queries, outs, specs):
+            idx.search_device(q, s[4], o_s, o_i, stream=stream)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    seq_ms = timed(seq_step)
+    multi = MultiIndex(idxs)
+    t0 = time.perf_counter()
+    multi.plan([s[3] for s in specs], [s[4] for s in specs], autotune=True)
+    plan_s = time.perf_counter() - t0
+    for j, q in enumerate(queries):
+        multi.set_queries(j, q.cpu().numpy())
+    multi_ms = timed(lambda: multi.launch(stream=stream))
+    # exactness: every index's result equals its own search
+    seq_step()
+    torch.cuda.synchronize()
+    exact = True
+    for j, (o_s, o_i) in enumerate(outs):
+        ms_, mi_ = multi.results(j)
+        exact &= bool(np.array_equal(mi_, o_i.cpu().numpy().view(np.uint64)))
+        exact &= bool(np.array_equal(ms_.view(np.uint32), o_s.cpu().numpy().view(np.uint32)))
+    cfg = multi.config()
+    line = {
+        "metric": "multi-index QPS (32 flat indexes, uneven n/dim/bits/batches, one persistent graph launch)",
+        "value": total_q / (multi_ms / 1e3), "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": multi_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "32 flat TurboQuant indexes: n log-uniform [1e4, 2e6], dim {128,384,768,1536}, "
+                               "bits {2,3,4}, batches log-uniform [1, 4096], k {10,64}",
+                   "indexes": [{"n": s[0], "dim": s[1], "bits": s[2], "nq": s[3], "k": s[4]} for s in specs],
+                   "total_queries": total_q, "total_vectors": sum(s[0] for s in specs), "build_s": build_s,
+                   "plan_and_autotune_s": plan_s, "autotuned": cfg},
+        "per_index_sequential": {"ms_per_step": seq_ms, "qps": total_q / (seq_ms / 1e3)},
+        "speedup_vs_sequential": seq_ms / multi_ms, "identical_to_per_index_search": exact,
+    }
+    print(json.dumps(line), flush=True)
+    multi.close()
+    for idx in idxs:
+        idx.close()
+
+
 def main():
     args = parse()
+    if args.workload == "multi":
+        world, rank, local = dist_setup(args)
+        run_multi(args, world, rank, local)
+        return
     if args.workload == "bucketed":
         world, rank, local = dist_setup(args)
         run_bucketed(args, world, rank, local)

@@ -405,6 +405,10 @@ int tq_multi_synchronize(tq_multi* h);
  * (on return *n_tuned = candidates timed). */
 int tq_multi_config(tq_multi* h, long long* range_vectors, int* ctas, size_t* n_items, size_t* smem_bytes,
                     double* tuned_ms, size_t* n_tuned);
+/* The autotuner's third pass may route the heaviest index batches (by nq x n
+ * x byte groups) to the single-index scan kernels, inside the same graph;
+ * flags[i] = 1 marks those (n_indexes entries). */
+int tq_multi_direct(tq_multi* h, size_t* n_direct, uint8_t* flags);
 /* Synchronous copies into / out of the library's device buffers (for callers
  * without their own CUDA runtime). */
 int tq_copy_to_device(void* d_dst, const void* src, size_t bytes);

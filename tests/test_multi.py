@@ -55,7 +55,7 @@ def test_multi_launch_equals_per_index_search(indexes, autotune):
     cfg = multi.config()
     assert cfg["items"] > 0 and cfg["ctas"] > 0
     if autotune:
-        assert len(cfg["tuned_ms"]) >= 4
+        assert len(cfg["tuned_ms"]) >= 4 and 0 <= cfg["direct_indexes"] <= len(SPECS)
     for rep in range(2):  # the graph is replayed with new queries
         qs = [_queries(j, s[0], s[3], rep) for j, s in enumerate(SPECS)]
         for j, q in enumerate(qs):

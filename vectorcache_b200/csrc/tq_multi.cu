@@ -13,9 +13,11 @@
 // id asc) top-k are those of the flat search, so results equal the per-index
 // search bit for bit.
 //
-// The autotuner picks the vector-range length of a work item and the number of
-// resident CTAs by timing the candidates on the planned workload itself
-// (CUDA events, median of 3), then captures the graph with the fastest.
+// The autotuner times candidates on the planned workload itself (CUDA events,
+// one untimed and one timed run each), in three passes: the vector-range
+// length of a work item, the resident CTAs per SM, and how many of the
+// heaviest index batches run the single-index scan kernels (inside the same
+// graph) instead of the persistent launch; then it captures the graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +38,8 @@ struct tq_multi {
   std::vector<tq_index*> idx;
   // plan
   std::vector<size_t> nq, k, ke;
+  std::vector<char> direct;  // index runs the single-index kernels instead of the persistent launch
+  size_t n_direct = 0;
   std::vector<std::unique_ptr<vcb::FlatScratchStore>> scratch;
   std::vector<std::unique_ptr<vcb::DeviceBuffer>> d_q, d_s, d_i;
   vcb::DeviceBuffer d_desc, d_items, d_counter;
@@ -92,7 +96,7 @@ struct tq_multi {
       d.cand_s = sc.cand_s.as<float>();
       d.cand_i = sc.cand_i.as<uint32_t>();
       descs.push_back(d);
-      if (nq[i] == 0 || ke[i] == 0) continue;
+      if (nq[i] == 0 || ke[i] == 0 || direct[i]) continue;
       max_nbg = std::max(max_nbg, d.nbg);
       max_k = std::max(max_k, d.k);
       (d.bits == 3 ? any3 : any24) = true;
@@ -123,10 +127,17 @@ struct tq_multi {
     vcb::check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
   }
 
-  // The whole multi-index search on stream s (what the graph captures).
+  // The whole multi-index search on stream s (what the graph captures):
+  // indexes marked `direct` run the single-index scan kernels (best for the
+  // heaviest index batches), all others share the one persistent launch.
   void run(cudaStream_t s) {
     for (size_t i = 0; i < idx.size(); ++i) {
-      if (nq[i] == 0 || ke[i] == 0) continue;
+      if (nq[i] == 0 || ke[i] == 0 || !direct[i]) continue;
+      idx[i]->search_device(d_q[i]->as<float>(), nq[i], k[i], d_s[i]->as<float>(), d_i[i]->as<uint64_t>(), ke[i], s,
+                            scratch[i]->ref());
+    }
+    for (size_t i = 0; i < idx.size(); ++i) {
+      if (nq[i] == 0 || ke[i] == 0 || direct[i]) continue;
       idx[i]->prep_queries(d_q[i]->as<float>(), nq[i], s, nullptr, scratch[i]->ref());
     }
     vcb::check(cudaMemsetAsync(d_counter.get(), 0, 8, s), "cudaMemsetAsync");
@@ -137,7 +148,7 @@ struct tq_multi {
     a.next_item = d_counter.as<unsigned long long>();
     vcb::check(vcb::launch_multi_scan(a, ctas, smem, any3, any24, s), "multi scan kernel");
     for (size_t i = 0; i < idx.size(); ++i) {
-      if (nq[i] == 0 || ke[i] == 0) continue;
+      if (nq[i] == 0 || ke[i] == 0 || direct[i]) continue;
       vcb::MergeArgs mg{};
       mg.cand_score = descs[i].cand_s;
       mg.cand_id = descs[i].cand_i;
@@ -248,6 +259,8 @@ int tq_multi_plan(tq_multi* h, const size_t* nq, const size_t* k, int autotune) 
     h->nq.assign(nq, nq + m);
     h->k.assign(k, k + m);
     h->ke.resize(m);
+    h->direct.assign(m, 0);
+    h->n_direct = 0;
     h->scratch.clear();
     h->d_q.clear();
     h->d_s.clear();
@@ -265,38 +278,76 @@ int tq_multi_plan(tq_multi* h, const size_t* nq, const size_t* k, int autotune) 
       vcb::check(cudaMemsetAsync(h->d_q[i]->get(), 0, std::max<size_t>(nq[i], 1) * h->idx[i]->dim * 4, h->stream),
                  "cudaMemsetAsync");
     }
-    // Candidates: range length x resident CTAs per SM.
-    const long long ranges[] = {4096, 8192, 16384, 32768};
-    std::vector<std::pair<long long, int>> cands;
+    // Autotuner, two passes over the planned workload itself: the item range
+    // length at the most resident CTAs, then the resident CTAs per SM at that
+    // length. Each candidate: one untimed run (grows scratch, loads kernels),
+    // one timed run (CUDA events).
     h->tuned_ms.clear();
+    long long best_rv = 8192;
     if (autotune) {
+      const long long ranges[] = {4096, 8192, 16384, 32768};
+      double best = -1.0;
       for (long long rv : ranges) {
         h->build_items(rv);
-        const int per_sm = std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
-        for (int c = 1; c <= per_sm; ++c) cands.push_back({rv, c});
-      }
-    } else {
-      cands.push_back({8192, 0});
-    }
-    double best = -1.0;
-    std::pair<long long, int> pick = cands.front();
-    for (const auto& cd : cands) {
-      h->build_items(cd.first);
-      const int per_sm = std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
-      h->ctas = h->sms * (cd.second ? std::min(cd.second, per_sm) : per_sm);
-      if (!autotune) break;
-      h->time_ms(1);  // warm-up: grows the scratch, loads the kernels
-      const double ms = h->time_ms(3);
-      h->tuned_ms.push_back(ms);
-      if (best < 0 || ms < best) {
-        best = ms;
-        pick = cd;
+        h->ctas = h->sms * std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
+        h->time_ms(1);
+        const double ms = h->time_ms(1);
+        h->tuned_ms.push_back(ms);
+        if (best < 0 || ms < best) {
+          best = ms;
+          best_rv = rv;
+        }
       }
     }
+    h->build_items(best_rv);
+    const int per_sm = std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
+    int best_c = per_sm;
+    if (autotune && per_sm > 1) {
+      double best = -1.0;
+      for (int c = 1; c <= per_sm; ++c) {
+        h->ctas = h->sms * c;
+        const double ms = h->time_ms(1);
+        h->tuned_ms.push_back(ms);
+        if (best < 0 || ms < best) {
+          best = ms;
+          best_c = c;
+        }
+      }
+    }
+    h->ctas = h->sms * best_c;
+    // Third pass: how many of the heaviest index batches (nq x n x byte groups)
+    // go to the single-index kernels instead of the persistent launch.
     if (autotune) {
-      h->build_items(pick.first);
-      const int per_sm = std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
-      h->ctas = h->sms * std::min(pick.second, per_sm);
+      std::vector<size_t> order(m);
+      std::iota(order.begin(), order.end(), size_t{0});
+      auto work = [&](size_t i) {
+        return static_cast<double>(h->nq[i]) * static_cast<double>(h->idx[i]->n) * static_cast<double>(h->idx[i]->nbg);
+      };
+      std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work(a) > work(b); });
+      auto set_direct = [&](size_t d) {
+        h->direct.assign(m, 0);
+        for (size_t t = 0; t < d; ++t) h->direct[order[t]] = 1;
+        h->n_direct = d;
+        h->build_items(best_rv);
+        const int ps = std::max(1, vcb::multi_scan_ctas_per_sm(h->smem, h->any3));
+        h->ctas = h->sms * std::min(best_c, ps);
+      };
+      set_direct(0);
+      double best = h->time_ms(1);
+      size_t best_d = 0;
+      for (size_t d : {size_t{1}, size_t{2}, size_t{4}, size_t{8}, size_t{16}, m}) {
+        if (d > m || d == 0) continue;
+        set_direct(d);
+        h->time_ms(1);
+        const double ms = h->time_ms(1);
+        h->tuned_ms.push_back(ms);
+        if (ms < best) {
+          best = ms;
+          best_d = d;
+        }
+        if (d == m) break;
+      }
+      set_direct(best_d);
     }
     h->capture();
     h->planned = true;
@@ -378,3 +429,14 @@ int tq_copy_to_host(void* dst, const void* d_src, size_t bytes) {
 }
 
 }  // extern "C"
+
+extern "C" int tq_multi_direct(tq_multi* h, size_t* n_direct, uint8_t* flags) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(h->planned, TQ_ERR_STATE, "plan() first");
+    if (n_direct) *n_direct = h->n_direct;
+    if (flags) {
+      for (size_t i = 0; i < h->direct.size(); ++i) flags[i] = static_cast<uint8_t>(h->direct[i]);
+    }
+  });
+}

@@ -33,6 +33,7 @@ def _declare_multi(lib):
         "tq_multi_synchronize": (C.c_int, [_P]),
         "tq_multi_config": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(_SZ),
                                       C.POINTER(_SZ), _P, C.POINTER(_SZ)]),
+        "tq_multi_direct": (C.c_int, [_P, C.POINTER(_SZ), _P]),
         "tq_copy_to_device": (C.c_int, [_P, _P, _SZ]),
         "tq_copy_to_host": (C.c_int, [_P, _P, _SZ]),
     }
@@ -108,6 +109,10 @@ class MultiIndex:
         nt = _SZ(64)
         _check(self._lib.tq_multi_config(self._h, C.byref(rv), C.byref(ctas), C.byref(ni), C.byref(sm),
                                           _ptr(tuned), C.byref(nt)))
+        nd = _SZ()
+        flags = np.zeros(len(self.indexes), np.uint8)
+        _check(self._lib.tq_multi_direct(self._h, C.byref(nd), _ptr(flags)))
         return {"range_vectors": rv.value, "ctas": ctas.value, "items": ni.value, "smem_bytes": sm.value,
-                "tuned_ms": tuned[: nt.value].tolist()}
+                "tuned_ms": tuned[: nt.value].tolist(), "direct_indexes": int(nd.value),
+                "direct_flags": flags.tolist()}
 
