@@ -699,6 +699,9 @@ constexpr int kBsWarps = 4;
 constexpr int kBsPrefetch = 4;
 constexpr int kBsBuf = 512;  // per-warp sort buffer: up to 256 new + 256 kept
 
+// Per-warp top-k list capacity for k (k <= 256).
+__host__ __device__ inline int kmax_of(int k) { return k <= 32 ? 32 : (k <= 64 ? 64 : (k <= 128 ? 128 : 256)); }
+
 // j-th largest (1-based, j <= 8) of the lane's valid scores, -inf if fewer.
 __device__ __forceinline__ float lane_jth_largest(const float (&sc)[8], unsigned ok, int j) {
   float v[8];
@@ -758,7 +761,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
 
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [kItemQueries][chunk][2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int kmax = k <= 32 ? 32 : (k <= 64 ? 64 : 256);
+  const int kmax = kmax_of(k);
   // Per-warp top-k lists and sort buffer after the LUT area.
   unsigned char* warp_area = smem + static_cast<size_t>(kItemQueries) * chunk * 32 +
                              warp * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
@@ -789,14 +792,12 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   const unsigned long long slot0 = static_cast<unsigned long long>(v.slot0);
   const int size = v.size;
   const int n_sub = (size + kBucketSlotAlign - 1) / kBucketSlotAlign;
-  float scale[4], init[4], off[4], thr_s[4];
+  // per-query constants stay in shared memory (iq): fewer live registers
+  float thr_s[4];
   uint32_t thr_i[4];
   int cnt[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    scale[q] = iq.scale[quad * 4 + q];
-    init[q] = iq.init[quad * 4 + q];
-    off[q] = iq.off[quad * 4 + q];
     thr_s[q] = -FLT_MAX;
     thr_i[q] = 0xffffffffu;
     cnt[q] = 0;
@@ -820,7 +821,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        fa[q][j] = init[q];
+        fa[q][j] = iq.init[quad * 4 + q];
         acc[q][j] = 0u;
       }
     for (int gb = 0; gb < nbg; gb += kFlushGroups) {
@@ -903,7 +904,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          fa[q][j] = __fmaf_rn(scale[q], __uint2float_rn(acc[q][j]), fa[q][j]);
+          fa[q][j] = __fmaf_rn(iq.scale[quad * 4 + q], __uint2float_rn(acc[q][j]), fa[q][j]);
           acc[q][j] = 0u;
         }
     }
@@ -938,7 +939,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       unsigned ok = 0;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), off[q]);
+        sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), iq.off[quad * 4 + q]);
         if ((valid >> j & 1u) && sc[j] > -INFINITY) ok |= 1u << j;
       }
       unsigned pass = 0;
@@ -1020,7 +1021,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
 }
 
 template <bool NIBBLE8>
-__global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanArgs a) {
+__global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketScanArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ ItemQueries iq;
   if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
@@ -1057,7 +1058,7 @@ __global__ void __launch_bounds__(kBsWarps * 32) bucket_scan_kernel(BucketScanAr
 // none is left, so one launch serves indexes of any n, dim and bits.
 // ---------------------------------------------------------------------------
 template <bool ANY3, bool ANY24>
-__global__ void __launch_bounds__(kBsWarps * 32) multi_scan_kernel(MultiScanArgs a) {
+__global__ void __launch_bounds__(kBsWarps * 32, 4) multi_scan_kernel(MultiScanArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ ItemQueries iq;
   __shared__ long long s_item;
@@ -1296,7 +1297,7 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
 
 size_t multi_scan_smem_bytes(int max_nbg, int max_k) {
   const int chunk = max_nbg < kFlushGroups ? max_nbg : kFlushGroups;
-  const int kmax = max_k <= 32 ? 32 : (max_k <= 64 ? 64 : 256);
+  const int kmax = kmax_of(max_k);
   return static_cast<size_t>(kItemQueries) * chunk * 32 +
          static_cast<size_t>(kBsWarps) * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
 }
@@ -1329,7 +1330,7 @@ cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStre
   if (grid <= 0) return cudaSuccess;
   if (a.k < 1 || a.k > kMaxK) return cudaErrorInvalidValue;
   const int chunk = a.nbg < kFlushGroups ? a.nbg : kFlushGroups;
-  const int kmax = a.k <= 32 ? 32 : (a.k <= 64 ? 64 : 256);
+  const int kmax = kmax_of(a.k);
   const size_t smem = static_cast<size_t>(kItemQueries) * chunk * 32 +
                       static_cast<size_t>(kBsWarps) * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
   cudaError_t e;
