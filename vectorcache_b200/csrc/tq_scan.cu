@@ -28,7 +28,6 @@ namespace {
 
 constexpr int kScanWarps = 8;
 constexpr int kMergeBuf = 512;  // per-warp sort buffer: 256 new + up to 256 kept
-constexpr int kPrefetch = 4;    // byte groups of codes in flight per thread
 constexpr int kRegTopK = 32;    // k up to this is kept in registers, one entry per lane
 
 // Running top-k of one warp for one query, one entry per lane (k <= 32),
@@ -95,10 +94,54 @@ struct RegTopK {
       if (better(cs, ci, thr_s, thr_i)) insert(cs, ci, k, lane);
     }
   }
+
+  // offer() for candidates with arbitrary ids (merging candidate lists).
+  __device__ __forceinline__ void offer_ids(const float (&sc)[8], const uint32_t (&id)[8], unsigned valid, int k,
+                                            int lane) {
+    unsigned pass = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if ((valid >> j & 1u) && better(sc[j], id[j], thr_s, thr_i)) pass |= 1u << j;
+    }
+    if (!(thr_s > -INFINITY)) {
+      float mx = -INFINITY;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (pass >> j & 1u) mx = fmaxf(mx, sc[j]);
+      }
+      const float bound = warp_kth_largest(mx, k, lane);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if ((pass >> j & 1u) && sc[j] < bound) pass &= ~(1u << j);
+      }
+    }
+    unsigned any = __ballot_sync(full_mask(), pass != 0);
+    while (any) {
+      const int src = __ffs(any) - 1;
+      const int my_j = __ffs(pass) - 1;
+      float my_s = sc[0];
+      uint32_t my_i = id[0];
+#pragma unroll
+      for (int j = 1; j < 8; ++j) {
+        if (j == my_j) {
+          my_s = sc[j];
+          my_i = id[j];
+        }
+      }
+      const float cs = __shfl_sync(full_mask(), my_s, src);
+      const uint32_t ci = __shfl_sync(full_mask(), my_i, src);
+      if (lane == src) pass &= pass - 1;
+      any = __ballot_sync(full_mask(), pass != 0);
+      if (better(cs, ci, thr_s, thr_i)) insert(cs, ci, k, lane);
+    }
+  }
 };
 
-template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8>
+// PF: byte groups of codes in flight per thread. Few queries per CTA leave
+// the kernel memory-bound, where a deeper ring keeps more bytes in flight.
+template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
+  static_assert(PF % 2 == 0, "byte groups are consumed in pairs");
   constexpr bool kReg = KMAX <= kRegTopK;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nbg = a.nbg;
@@ -189,17 +232,17 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         __syncthreads();
       }
       const int chunk_base = resident ? 0 : (gb / chunk) * chunk;
-      uint2 ring[kPrefetch];
+      uint2 ring[PF];
 #pragma unroll
-      for (int u = 0; u < kPrefetch; ++u) {
+      for (int u = 0; u < PF; ++u) {
         ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
       }
-      for (int g = gb; g < g_stop; g += kPrefetch) {
-        uint2 cur[kPrefetch];
+      for (int g = gb; g < g_stop; g += PF) {
+        uint2 cur[PF];
 #pragma unroll
-        for (int u = 0; u < kPrefetch; ++u) {
+        for (int u = 0; u < PF; ++u) {
           cur[u] = ring[u];
-          const int gn = g + kPrefetch + u;
+          const int gn = g + PF + u;
           ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
         }
         // Byte groups in pairs (nbg and every 256-group batch are even): the
@@ -207,7 +250,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         // (<= 2 * 127), the first-half lookups into another; one prmt
         // interleaves the two bytes of each vector so a single dp4a adds both.
 #pragma unroll
-        for (int u = 0; u < kPrefetch; u += 2) {
+        for (int u = 0; u < PF; u += 2) {
           if (g + u >= g_stop) break;
           const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
           const uint32_t a0h = a0 >> 16, a1h = a1 >> 16, b0h = b0 >> 16, b1h = b1 >> 16;
@@ -488,6 +531,55 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   }
 }
 
+// k_out <= 32: one CTA per query, every warp keeps a register top-k over a
+// strided share of the candidates (8 consecutive entries per lane, the
+// first-block prefilter bounds the work), then one warp merges the 8 lists.
+// Same result as merge_kernel: best k_out by (score desc, id asc), -inf and
+// NaN never admitted, unfilled slots (0, pad_id).
+__global__ void __launch_bounds__(kMergeThreads) merge_reg_kernel(MergeArgs a) {
+  constexpr int kWarps = kMergeThreads / kWarp;
+  __shared__ float m_s[kMergeThreads];
+  __shared__ uint32_t m_i[kMergeThreads];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long qi = blockIdx.x;
+  const long long stride = static_cast<long long>(a.n_lists) * a.k;
+  const long long total = (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
+                                        : static_cast<long long>(a.n_lists)) * a.k;
+  const float* cs = a.cand_score + qi * stride;
+  const uint32_t* ci = a.cand_id + qi * stride;
+  const int kout = a.k_out;
+  RegTopK top;
+  for (long long base = static_cast<long long>(warp) * kWarp * 8; base < total;
+       base += static_cast<long long>(kWarps) * kWarp * 8) {
+    float sc[8];
+    uint32_t id[8];
+    unsigned ok = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const long long idx = base + lane * 8 + j;
+      sc[j] = -INFINITY;
+      id[j] = 0xffffffffu;
+      if (idx < total) {
+        sc[j] = cs[idx];
+        id[j] = ci[idx];
+        if (sc[j] > -INFINITY) ok |= 1u << j;
+      }
+    }
+    top.offer_ids(sc, id, ok, kout, lane);
+  }
+  m_s[threadIdx.x] = lane < kout ? top.s : -INFINITY;
+  m_i[threadIdx.x] = lane < kout ? top.i : 0xffffffffu;
+  __syncthreads();
+  if (warp == 0) {
+    warp_sort_best_first(m_s, m_i, kMergeThreads, lane);
+    if (lane < kout) {
+      const bool have = m_s[lane] > -INFINITY;
+      a.out_score[qi * kout + lane] = have ? m_s[lane] : 0.f;
+      a.out_id[qi * kout + lane] = have ? static_cast<uint64_t>(m_i[lane]) : a.pad_id;
+    }
+  }
+}
+
 // Dense integer / float scores for parity checks: one thread per (query, vector).
 __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const float* __restrict__ alpha,
                                     const uint8_t* __restrict__ luts, const float* __restrict__ lut_scale,
@@ -516,15 +608,20 @@ __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const fl
   if (out_score) out_score[idx] = __fadd_rn(__fmul_rn(fa, alpha[v]), 0.f);
 }
 
-template <int Q, int KMAX, int MINB, bool N8>
+template <int Q, int KMAX, int MINB, bool N8, int PF>
 cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB, N8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB, N8, PF>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(plan.smem_bytes));
   if (e != cudaSuccess) return e;
   dim3 grid(static_cast<unsigned>((a.nq + Q - 1) / Q), static_cast<unsigned>(plan.n_ranges));
-  scan_kernel<Q, KMAX, MINB, N8><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
+  scan_kernel<Q, KMAX, MINB, N8, PF><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
   return cudaGetLastError();
 }
+
+// Prefetch depth per queries-per-CTA: the one-query kernel is memory-bound and
+// keeps 16 byte groups in flight per thread, the 4-query kernel is issue-bound.
+constexpr int prefetch_for(int q) { return q == 1 ? 16 : (q == 2 ? 8 : 4); }
 
 size_t scan_warp_bytes(int q, int kmax) {
   if (kmax <= kRegTopK) return 0;
@@ -600,8 +697,8 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
   const bool n8 = a.bits == 3;  // 3-bit codes never set a nibble's top bit
 #define VCB_SCAN(QQ, KK, MB)                                                             \
   if (q == QQ && km == KK) {                                                             \
-    return n8 ? launch_scan_t<QQ, KK, MB, true>(a, plan, stream)                         \
-              : launch_scan_t<QQ, KK, MB, false>(a, plan, stream);                       \
+    return n8 ? launch_scan_t<QQ, KK, MB, true, prefetch_for(QQ)>(a, plan, stream)       \
+              : launch_scan_t<QQ, KK, MB, false, prefetch_for(QQ)>(a, plan, stream);     \
   }
   VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
   VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
@@ -612,6 +709,10 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
 
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream) {
   if (a.nq == 0 || a.k_out == 0) return cudaSuccess;
+  if (a.k_out <= kRegTopK) {
+    merge_reg_kernel<<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+  }
   merge_kernel<<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
