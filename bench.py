@@ -349,11 +349,14 @@ def run_ours(args, world, rank, local):
 
     # Latency of small batches (device-resident queries): p50 / p99 over repeats.
     latency = {}
+    one_query = None
     if world == 1:
         for bsz, reps in ((1, 50), (16, 30), (256, 15)):
             times = []
             sub = q[:bsz]
             for r in range(reps + 3):
+                if r == 3:
+                    index.read_profile()  # per-kernel times of the timed repeats only
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 index.search_device(sub, k, d_scores, d_ids, stream=stream)
@@ -361,10 +364,18 @@ def run_ours(args, world, rank, local):
                 e1.synchronize()
                 if r >= 3:
                     times.append(e0.elapsed_time(e1))
+            p = index.read_profile()
             latency[f"nq={bsz}"] = {"p50_ms": float(np.percentile(times, 50)),
                                     "p99_ms": float(np.percentile(times, 99)),
-                                    "qps": bsz / (float(np.median(times)) / 1e3)}
-        index.read_profile()
+                                    "qps": bsz / (float(np.median(times)) / 1e3),
+                                    "kernel_ms": {"prep": p["prep_ms"] / reps, "scan": p["scan_ms"] / reps,
+                                                  "merge": p["merge_ms"] / reps}}
+            if bsz == 1 and p["scan_launches"]:
+                # One query per pass: the scan's memory-bound regime.
+                ms = p["scan_ms"] / p["scan_launches"]
+                gbs = args.n * (args.dim // (8 // args.bits) + 4) / (ms / 1e3) / 1e9
+                one_query = {"kernel": "scan_kernel (1 query per pass)", "bound": "hbm", "achieved": gbs,
+                             "unit": "GB/s", "ms_per_launch": ms}
 
     # End to end through the public host-buffer API: pinned host queries in,
     # host top-k out, copies inside the timed region.
@@ -456,7 +467,11 @@ def run_ours(args, world, rank, local):
             "roofline": {"kernel": "scan_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": tr,
                          "bytes_per_launch": bytes_per_launch, "ms_per_launch": scan_ms_avg,
-                         "share_of_kernel_time": prof["scan_ms"] / total_kernel_ms if total_kernel_ms else None},
+                         "share_of_kernel_time": prof["scan_ms"] / total_kernel_ms if total_kernel_ms else None,
+                         "nibble_lookups_per_s": lookups * args.steps / (prof["scan_ms"] / 1e3)
+                         if prof["scan_ms"] else None,
+                         "one_query_pass": (dict(one_query, peak=peak, frac=one_query["achieved"] / peak)
+                                            if one_query else None)},
             "cpu_baseline": cpu_base,
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * args.dim * 4,
                     "d2h_bytes_per_step": args.nq * k * 12},
@@ -586,12 +601,15 @@ def run_bucketed(args, world, rank, local):
     learned_sweep = []
     for cov in (0.5, 0.7, 0.8, 0.9, 0.95, 0.98):
         def learned_step(cov=cov):
-            idx.route_device(d_q, 256, te_s, te_i, stream=stream)
-            mlp.predict_device(te_s, nq, 256, npq, coverage=cov, min_confidence=0.0, fallback=p_op, stream=stream)
-            idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, d_n_probe=npq, stream=stream)
+            # one routing pass feeds the network and the probes
+            idx.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=cov, min_confidence=0.0,
+                                      fallback_n_probe=p_op, stream=stream)
 
         ms = timed(learned_step)
         r = float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())
+        # the per-query probe counts of that search (recomputed outside the timed region)
+        idx.route_device(d_q, 256, te_s, te_i, stream=stream)
+        mlp.predict_device(te_s, nq, 256, npq, coverage=cov, min_confidence=0.0, fallback=p_op, stream=stream)
         mean_probe = float(npq.float().mean().item())
         cand = {"coverage": cov, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
                 "mean_n_probe": mean_probe}
@@ -599,6 +617,26 @@ def run_bucketed(args, world, rank, local):
         if r >= min(RECALL_TARGET, recall_fixed) and (best is None or cand["qps"] > best["qps"]):
             best = cand
     qps_fixed = nq / (fixed_ms / 1e3)
+
+    # Device time per kernel class of one search at each operating point.
+    eng = idx.engine()
+
+    def kernel_ms(step_fn):
+        step_fn()
+        torch.cuda.synchronize()
+        eng.set_profiling(True)
+        eng.read_profile()
+        step_fn()
+        torch.cuda.synchronize()
+        prof = eng.read_profile()
+        eng.set_profiling(False)
+        return {"prep_route_pairs": prof["prep_ms"], "bucket_scan": prof["scan_ms"], "merge_rerank": prof["merge_ms"]}
+
+    fixed["kernel_ms"] = kernel_ms(lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, stream=stream))
+    if best:
+        best["kernel_ms"] = kernel_ms(lambda: idx.search_learned_device(
+            d_q, k, mlp, d_s, d_i, coverage=best["coverage"], min_confidence=0.0, fallback_n_probe=p_op,
+            stream=stream))
     line = {
         "metric": BUCKETED_METRIC, "value": best["qps"] if best else None, "unit": "queries/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",

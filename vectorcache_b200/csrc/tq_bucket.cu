@@ -641,14 +641,18 @@ __device__ __forceinline__ int probes_of(const PairArgs& a, long long q) {
   return np < a.max_probe ? np : a.max_probe;
 }
 
+// Probe position j of query q gets a pair in this build.
+__device__ __forceinline__ bool pair_in_range(const PairArgs& a, long long q, int j) {
+  return j >= a.probe_begin && j < a.probe_end && j < probes_of(a, q);
+}
+
 __global__ void pair_count_kernel(PairArgs a) {
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= a.nq * a.max_probe) return;
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
-  const int np = probes_of(a, q);
-  if (j == 0) a.list_count[q] = 2u * static_cast<uint32_t>(np);
-  if (j >= np) return;
+  if (j == 0) a.list_count[q] = 2u * static_cast<uint32_t>(probes_of(a, q));
+  if (!pair_in_range(a, q, j)) return;
   const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b < static_cast<uint32_t>(a.nb)) atomicAdd(&a.counts[b], 1u);
 }
@@ -658,7 +662,7 @@ __global__ void pair_scatter_kernel(PairArgs a) {
   if (t >= a.nq * a.max_probe) return;
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
-  if (j >= probes_of(a, q)) return;
+  if (!pair_in_range(a, q, j)) return;
   const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b >= static_cast<uint32_t>(a.nb)) return;
   const unsigned long long pos = a.pair_start[b] + atomicAdd(&a.fill[b], 1u);
@@ -672,7 +676,7 @@ __global__ void pair_offset_kernel(PairArgs a) {
   if (t >= a.nq * a.max_probe) return;
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
-  if (j >= probes_of(a, q)) return;
+  if (!pair_in_range(a, q, j)) return;
   const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b >= static_cast<uint32_t>(a.nb)) return;
   const float d = warp_dot(a.q_hat + q * a.dim, a.enc + static_cast<long long>(b) * a.dim, a.dim, lane);
@@ -749,6 +753,7 @@ struct ItemQueries {
   int q[kItemQueries];           // LUT row (-1: no query)
   long long list[kItemQueries];  // candidate list written by tile set 0 (tile set 1: list + 1)
   float scale[kItemQueries], init[kItemQueries], off[kItemQueries];
+  float floor[kItemQueries];     // scores below it are not kept (-inf: keep all)
 };
 
 // Scans one item with the CTA's 4 warps (2 query quads x 2 tile sets) and
@@ -937,10 +942,11 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       if (quad * 4 + q >= pc) break;  // warp-uniform
       float sc[8];
       unsigned ok = 0;
+      const float fl = iq.floor[quad * 4 + q];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), iq.off[quad * 4 + q]);
-        if ((valid >> j & 1u) && sc[j] > -INFINITY) ok |= 1u << j;
+        if ((valid >> j & 1u) && sc[j] > -INFINITY && !(sc[j] < fl)) ok |= 1u << j;
       }
       unsigned pass = 0;
       if (cnt[q] == k) {
@@ -1038,12 +1044,14 @@ __global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketSca
       iq.scale[t] = a.lut_scale[q];
       iq.init[t] = a.fa_init[q];
       iq.off[t] = a.offsets[pr];
+      iq.floor[t] = a.floor ? a.floor[q] : -INFINITY;
     } else {
       iq.q[t] = -1;
       iq.list[t] = 0;
       iq.scale[t] = 0.f;
       iq.init[t] = 0.f;
       iq.off[t] = 0.f;
+      iq.floor[t] = -INFINITY;
     }
   }
   __syncthreads();
@@ -1086,6 +1094,7 @@ __global__ void __launch_bounds__(kBsWarps * 32, 4) multi_scan_kernel(MultiScanA
         iq.init[t] = 0.f;
         iq.off[t] = 0.f;
       }
+      iq.floor[t] = -INFINITY;
     }
     __syncthreads();
     const long long slot0 = static_cast<long long>(it.range) * d.range_vectors;
@@ -1292,6 +1301,28 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   item_build_kernel<<<static_cast<unsigned>((a.nb + 255) / 256), 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+__global__ void probe_floor_kernel(const float* __restrict__ cand_score, const uint32_t* __restrict__ list_count,
+                                   long long nq, int max_probe, int k, float* __restrict__ floor) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  float f = -INFINITY;
+  if (list_count[q] >= 2u) {
+    const long long l0 = q * max_probe * 2;  // probe 0, tile sets 0 and 1
+    const float a = cand_score[l0 * k + (k - 1)];
+    const float b = cand_score[(l0 + 1) * k + (k - 1)];
+    f = fmaxf(a, b);  // -inf pads when a tile set holds fewer than k candidates
+  }
+  floor[q] = f;
+}
+
+cudaError_t launch_probe_floor(const float* cand_score, const uint32_t* list_count, long long nq, int max_probe,
+                               int k, float* floor, cudaStream_t stream) {
+  if (nq <= 0) return cudaSuccess;
+  probe_floor_kernel<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, stream>>>(cand_score, list_count, nq,
+                                                                                   max_probe, k, floor);
   return cudaGetLastError();
 }
 

@@ -120,6 +120,10 @@ struct PairArgs {
   uint4* items;              // (bucket, first pair, pair count, 0)
   unsigned long long* n_items;
   uint32_t* list_count;      // nq: 2 * n_probe (candidate lists per query)
+  // Probe positions [probe_begin, probe_end) of each query get pairs (the
+  // search scans probe 0 first to bound the rest; list_count always counts all).
+  int probe_begin = 0;
+  int probe_end = 1 << 30;
 };
 // Groups the (query, probe) pairs by bucket and builds the scan work items.
 cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);
@@ -141,8 +145,16 @@ struct BucketScanArgs {
   int nbg, bits, k, max_probe;
   float* cand_score;         // (nq * max_probe * 2) lists of k
   uint32_t* cand_id;
+  // Optional per query: scores below floor[q] cannot reach the query's top k
+  // and are not kept (nullptr: no floor).
+  const float* floor = nullptr;
 };
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
+// floor[q] = the larger k-th score of the two lists of probe 0 (each list is
+// the exact top k of its tile set, so either k-th score is a lower bound of
+// the k-th best over all probes); -inf for queries without probes.
+cudaError_t launch_probe_floor(const float* cand_score, const uint32_t* list_count, long long nq, int max_probe,
+                               int k, float* floor, cudaStream_t stream);
 
 // ---- multi-index persistent scan (tq_multi.cu) -----------------------------
 // One flat index of a multi-index launch: its scan layout, its queries' LUTs

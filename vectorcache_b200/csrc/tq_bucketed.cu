@@ -45,7 +45,7 @@ namespace vcb {
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
   DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
-      cand_i, rr_s, rr_i, np;
+      cand_i, rr_s, rr_i, np, floor;
   FlatScratchStore flat;
   ProbeScratch probe;
 };
@@ -462,10 +462,10 @@ struct tq_bucketed {
       pa.items = sc.items.as<uint4>();
       pa.n_items = sc.nitems.as<unsigned long long>();
       pa.list_count = sc.lcount.as<uint32_t>();
-      eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       const size_t lists = m * max_probe * 2;
       sc.cand_s.reserve(lists * kscan * 4);
       sc.cand_i.reserve(lists * kscan * 4);
+      sc.floor.reserve(m * 4);
       const float* qf = sc.flat.qf.as<float>();
       vcb::BucketScanArgs ba{};
       ba.codes = eng->d_codes.as<uint32_t>();
@@ -486,6 +486,25 @@ struct tq_bucketed {
       ba.max_probe = max_probe;
       ba.cand_score = sc.cand_s.as<float>();
       ba.cand_id = sc.cand_i.as<uint32_t>();
+      // Probe 0 first: the k-th best score of a query's best-routed bucket is a
+      // lower bound of its k-th best over all probes, so the scan of probes
+      // 1.. keeps only scores at or above it (fewer list insertions, sparse
+      // lists for the merge). The kept top k is the same.
+      const bool two_phase = max_probe > 1;
+      if (two_phase) {
+        pa.probe_begin = 0;
+        pa.probe_end = 1;
+        eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
+        eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
+        eng->launch(tq_index::kPrep, s, "floor kernel", [&] {
+          return vcb::launch_probe_floor(ba.cand_score, pa.list_count, static_cast<long long>(m), max_probe,
+                                         static_cast<int>(kscan), sc.floor.as<float>(), s);
+        });
+        pa.probe_begin = 1;
+        pa.probe_end = max_probe;
+        ba.floor = sc.floor.as<float>();
+      }
+      eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
       vcb::MergeArgs mg{};
       mg.cand_score = ba.cand_score;

@@ -4,10 +4,11 @@
 // Follows the reference's prepare_queries / build_query_lut
 // (src/search/search.cpp:149-219, :762-860) bit for bit.
 //
-// One CTA of 4 warps prepares 4 queries: the rows are staged in shared memory,
-// warp 0 runs the 8 sequential norm chains of all 4 rows, warp w rotates query
-// w in registers, and then all 128 threads build the 4 queries' LUTs together
-// (so a single query still gets the whole CTA for its byte groups).
+// One CTA of 8 warps prepares 4 queries: the rows are staged in shared memory,
+// warp 0 runs the 8 sequential norm chains of all 4 rows, warp w < 4 rotates
+// query w in registers, and then all 256 threads divide by the TQ+ scale and
+// build the 4 queries' LUTs together (so a single query still gets the whole
+// CTA for its divides and byte groups).
 #include <cfloat>
 
 #include "tq_kernels.h"
@@ -16,8 +17,8 @@
 namespace vcb {
 namespace {
 
-constexpr int kPrepWarps = 4;  // = queries per CTA
-constexpr int kPrepThreads = kPrepWarps * 32;
+constexpr int kPrepQueries = 4;  // queries per CTA; warp w < 4 rotates query w
+constexpr int kPrepThreads = 256;  // all 8 warps share the TQ+ divides and the LUT passes
 
 // The 16 entries of one LUT half: entry nv = sum over the cpn codes packed in
 // nibble value nv (first code in the high bits) of q[c] * centroid[code], each
@@ -52,7 +53,7 @@ __device__ __forceinline__ void half_min_max(const float (&v)[16], float* mn, fl
 }
 
 template <int R, int BITS>
-__global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs a) {
+__global__ void __launch_bounds__(kPrepThreads, 2) query_prep_kernel(QueryPrepArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int dim = a.dim, nbg = a.nbg;
   constexpr int kCpb = 8 / BITS;      // codes per byte group
@@ -61,36 +62,69 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
   float* s_shift = reinterpret_cast<float*>(s_perm + dim);
   float* s_scale = s_shift + (a.tqplus ? dim : 0);
   float* s_rows = s_scale + (a.tqplus ? dim : 0);   // 4 x dim
-  float* s_gmin = s_rows + kPrepWarps * dim;         // 4 x nbg
+  float* s_gmin = s_rows + kPrepQueries * dim;         // 4 x nbg
   __shared__ float s_cen[16];
-  __shared__ float s_norm[kPrepWarps];
-  __shared__ float s_bias_corr[kPrepWarps];
-  __shared__ unsigned s_span_bits[kPrepWarps];
-  __shared__ float s_inv[kPrepWarps];
-  __shared__ float s_lut_scale[kPrepWarps];
+  __shared__ float s_norm[kPrepQueries];
+  __shared__ float s_bias_corr[kPrepQueries];
+  __shared__ unsigned s_span_bits[kPrepQueries];
+  __shared__ float s_inv[kPrepQueries];
+  __shared__ float s_lut_scale[kPrepQueries];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  for (int i = threadIdx.x; i < dim; i += blockDim.x) {
-    s_perm[i] = a.perm_sign[i];
-    if (a.tqplus) {
-      s_shift[i] = a.shift[i];
-      s_scale[i] = a.scale[i];
+  // Tables in 16-byte pieces (dim is a multiple of 8), four pieces per thread
+  // loaded before any is stored so their latencies overlap.
+  const int n4 = dim >> 2;
+  for (int i0 = threadIdx.x; i0 < n4; i0 += 4 * kPrepThreads) {
+    uint4 p[4];
+    float4 sh[4], sc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * kPrepThreads;
+      if (i < n4) {
+        p[u] = __ldg(reinterpret_cast<const uint4*>(a.perm_sign) + i);
+        if (a.tqplus) {
+          sh[u] = __ldg(reinterpret_cast<const float4*>(a.shift) + i);
+          sc[u] = __ldg(reinterpret_cast<const float4*>(a.scale) + i);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * kPrepThreads;
+      if (i < n4) {
+        reinterpret_cast<uint4*>(s_perm)[i] = p[u];
+        if (a.tqplus) {
+          reinterpret_cast<float4*>(s_shift)[i] = sh[u];
+          reinterpret_cast<float4*>(s_scale)[i] = sc[u];
+        }
+      }
     }
   }
   if (threadIdx.x < 16) s_cen[threadIdx.x] = a.centroids[threadIdx.x];
 
-  for (long long q0 = static_cast<long long>(blockIdx.x) * kPrepWarps; q0 < a.nq;
-       q0 += static_cast<long long>(gridDim.x) * kPrepWarps) {
-    const int nloc = static_cast<int>(min(static_cast<long long>(kPrepWarps), a.nq - q0));
+  for (long long q0 = static_cast<long long>(blockIdx.x) * kPrepQueries; q0 < a.nq;
+       q0 += static_cast<long long>(gridDim.x) * kPrepQueries) {
+    const int nloc = static_cast<int>(min(static_cast<long long>(kPrepQueries), a.nq - q0));
     __syncthreads();
     // Stage the rows (coalesced 16-byte loads).
     const int vec_per_row = dim / 4;
-    for (int t = threadIdx.x; t < nloc * vec_per_row; t += blockDim.x) {
-      const int r = t / vec_per_row, c = t % vec_per_row;
-      reinterpret_cast<float4*>(s_rows + r * dim)[c] =
-          __ldg(reinterpret_cast<const float4*>(a.q + (q0 + r) * static_cast<long long>(dim)) + c);
+    for (int t0 = threadIdx.x; t0 < nloc * vec_per_row; t0 += 4 * kPrepThreads) {
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * kPrepThreads;
+        if (t < nloc * vec_per_row) {
+          const int r = t / vec_per_row, c = t % vec_per_row;
+          v[u] = __ldg(reinterpret_cast<const float4*>(a.q + (q0 + r) * static_cast<long long>(dim)) + c);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * kPrepThreads;
+        if (t < nloc * vec_per_row) reinterpret_cast<float4*>(s_rows)[t] = v[u];
+      }
     }
-    if (threadIdx.x < kPrepWarps) s_span_bits[threadIdx.x] = 0u;
+    if (threadIdx.x < kPrepQueries) s_span_bits[threadIdx.x] = 0u;
     __syncthreads();
 
     // Norms: lane 8v + c of warp 0 runs chain c of row v (encode.cpp:16-26).
@@ -99,7 +133,15 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
       float s = 0.f;
       if (v < nloc) {
         const float* row = s_rows + v * dim;
-        for (int j = c; j < dim; j += 8) s = __fmaf_rn(row[j], row[j], s);
+        int j = c;
+        for (; j + 56 < dim; j += 64) {  // 8 loads ahead of the chain's FMAs, same order
+          float x[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) x[u] = row[j + 8 * u];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) s = __fmaf_rn(x[u], x[u], s);
+        }
+        for (; j < dim; j += 8) s = __fmaf_rn(row[j], row[j], s);
       }
       s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 1));
       s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 2));
@@ -151,11 +193,6 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
           bias_corr = __double2float_rn(__shfl_sync(full_mask(), bc, 0));
           if (lane == 0 && a.replay_count) atomicAdd(a.replay_count, 1ull);
         }
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int i = lane + kWarp * r;
-          if (i < dim) y[r] = __fdiv_rn(y[r], s_scale[i]);
-        }
       }
       __syncwarp();
 #pragma unroll
@@ -163,15 +200,36 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
         const int i = lane + kWarp * r;
         if (i < dim) {
           row[i] = y[r];
-          if (a.q_rot) a.q_rot[qi * dim + i] = y[r];
+          if (a.q_rot && !a.tqplus) a.q_rot[qi * dim + i] = y[r];
         }
       }
       if (lane == 0) s_bias_corr[warp] = bias_corr;
     }
     __syncthreads();
+    if (a.tqplus) {
+      // q_rot_d = y_d / scale_d (search.cpp:792-797), spread over the whole CTA.
+      const int total = nloc * dim;
+      for (int t0 = threadIdx.x; t0 < total; t0 += 4 * kPrepThreads) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int t = t0 + u * kPrepThreads;
+          v[u] = (t < total) ? __fdiv_rn(s_rows[t], s_scale[t % dim]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int t = t0 + u * kPrepThreads;
+          if (t < total) {
+            s_rows[t] = v[u];
+            if (a.q_rot) a.q_rot[q0 * dim + t] = v[u];
+          }
+        }
+      }
+      __syncthreads();
+    }
 
     // LUT pass 1: per-group minima and per-query largest span (search.cpp:163-199).
-    float span[kPrepWarps] = {0.f, 0.f, 0.f, 0.f};
+    float span[kPrepQueries] = {0.f, 0.f, 0.f, 0.f};
     for (int t = threadIdx.x; t < nloc * nbg; t += blockDim.x) {
       const int r = t / nbg, g = t % nbg;
       const float* qd = s_rows + r * dim + g * kCpb;
@@ -184,13 +242,13 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
       float sp = (0.f < d0) ? d0 : 0.f;
       sp = (sp < d1) ? d1 : sp;
 #pragma unroll
-      for (int rr = 0; rr < kPrepWarps; ++rr) {
+      for (int rr = 0; rr < kPrepQueries; ++rr) {
         if (rr == r) span[rr] = (span[rr] < sp) ? sp : span[rr];
       }
       s_gmin[r * nbg + g] = __fadd_rn(mn0, mn1);
     }
 #pragma unroll
-    for (int rr = 0; rr < kPrepWarps; ++rr) {
+    for (int rr = 0; rr < kPrepQueries; ++rr) {
       const float m = warp_max_f(span[rr]);
       // Spans are >= 0, so their IEEE bit patterns order like the values.
       if (lane == 0 && rr < nloc) atomicMax(&s_span_bits[rr], __float_as_uint(m));
@@ -244,7 +302,16 @@ __global__ void __launch_bounds__(kPrepThreads) query_prep_kernel(QueryPrepArgs 
     if (threadIdx.x < nloc) {
       const int r = threadIdx.x;
       float bias = 0.f;
-      for (int g = 0; g < nbg; ++g) bias = __fadd_rn(bias, s_gmin[r * nbg + g]);
+      const float* gm = s_gmin + r * nbg;
+      int g = 0;
+      for (; g + 8 <= nbg; g += 8) {  // loads ahead of the in-order adds
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = gm[g + u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) bias = __fadd_rn(bias, v[u]);
+      }
+      for (; g < nbg; ++g) bias = __fadd_rn(bias, gm[g]);
       const long long qi = q0 + r;
       a.lut_scale[qi] = s_lut_scale[r];
       a.lut_bias[qi] = bias;
@@ -293,8 +360,8 @@ cudaError_t launch_query_prep(const QueryPrepArgs& a, int sms, cudaStream_t stre
   if (a.dim > kRegisterRowMaxDim) return launch_query_prep_big(a, sms, stream);
   const int r = rows_template_q(a.dim);
   const size_t smem = static_cast<size_t>(a.dim) * 4 * (a.tqplus ? 3 : 1) +
-                      static_cast<size_t>(kPrepWarps) * (a.dim + a.nbg) * 4;
-  long long grid = (a.nq + kPrepWarps - 1) / kPrepWarps;
+                      static_cast<size_t>(kPrepQueries) * (a.dim + a.nbg) * 4;
+  long long grid = (a.nq + kPrepQueries - 1) / kPrepQueries;
   if (grid > static_cast<long long>(sms) * 16) grid = static_cast<long long>(sms) * 16;
   const unsigned g = static_cast<unsigned>(grid);
   switch (r) {

@@ -481,17 +481,28 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   int nbest = 0;
   float thr_s = -FLT_MAX;
   uint32_t thr_i = 0xffffffffu;
+  constexpr int kPer = kMergeChunk / kMergeThreads;
   for (long long base = 0; base < total; base += kMergeChunk) {
+    // Scores first: a chunk with nothing at or above the current k-th best
+    // (padding, or candidates of far probes) costs one barrier.
+    float s[kPer];
+    bool any = false;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const long long idx = base + threadIdx.x + u * kMergeThreads;
+      s[u] = idx < total ? cs[idx] : -INFINITY;
+      any |= s[u] > -INFINITY && (nbest < kout || !(s[u] < thr_s));
+    }
+    if (!__syncthreads_or(any)) continue;
     if (threadIdx.x == 0) n_new = 0;
     __syncthreads();
-    for (int t = threadIdx.x; t < kMergeChunk; t += blockDim.x) {
-      const long long idx = base + t;
-      if (idx < total) {
-        const float s = cs[idx];
-        const uint32_t id = ci[idx];
-        if (s > -INFINITY && (nbest < kout || better(s, id, thr_s, thr_i))) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      if (s[u] > -INFINITY && (nbest < kout || !(s[u] < thr_s))) {
+        const uint32_t id = ci[base + threadIdx.x + u * kMergeThreads];
+        if (nbest < kout || better(s[u], id, thr_s, thr_i)) {
           const int pos = atomicAdd(&n_new, 1);
-          buf_s[pos] = s;
+          buf_s[pos] = s[u];
           buf_i[pos] = id;
         }
       }
@@ -548,8 +559,11 @@ __global__ void __launch_bounds__(kMergeThreads) merge_reg_kernel(MergeArgs a) {
   const float* cs = a.cand_score + qi * stride;
   const uint32_t* ci = a.cand_id + qi * stride;
   const int kout = a.k_out;
+  // Warps that receive candidates (one warp covers 256 per round); the same
+  // value in every thread of the CTA.
+  const int active = static_cast<int>(min(static_cast<long long>(kWarps), (total + kWarp * 8 - 1) / (kWarp * 8)));
   RegTopK top;
-  for (long long base = static_cast<long long>(warp) * kWarp * 8; base < total;
+  for (long long base = static_cast<long long>(warp) * kWarp * 8; warp < active && base < total;
        base += static_cast<long long>(kWarps) * kWarp * 8) {
     float sc[8];
     uint32_t id[8];
@@ -567,11 +581,22 @@ __global__ void __launch_bounds__(kMergeThreads) merge_reg_kernel(MergeArgs a) {
     }
     top.offer_ids(sc, id, ok, kout, lane);
   }
+  if (active <= 1) {
+    // Warp 0's list (sorted best first) is the answer.
+    if (warp == 0 && lane < kout) {
+      const bool have = top.s > -INFINITY;
+      a.out_score[qi * kout + lane] = have ? top.s : 0.f;
+      a.out_id[qi * kout + lane] = have ? static_cast<uint64_t>(top.i) : a.pad_id;
+    }
+    return;  // taken by the whole CTA (active is CTA-uniform)
+  }
   m_s[threadIdx.x] = lane < kout ? top.s : -INFINITY;
   m_i[threadIdx.x] = lane < kout ? top.i : 0xffffffffu;
   __syncthreads();
   if (warp == 0) {
-    warp_sort_best_first(m_s, m_i, kMergeThreads, lane);
+    int p = kWarp * 2;
+    while (p < kWarp * active) p <<= 1;  // lists of warps >= active are all empty
+    warp_sort_best_first(m_s, m_i, p, lane);
     if (lane < kout) {
       const bool have = m_s[lane] > -INFINITY;
       a.out_score[qi * kout + lane] = have ? m_s[lane] : 0.f;
