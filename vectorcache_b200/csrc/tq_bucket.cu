@@ -948,6 +948,36 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
         sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), iq.off[quad * 4 + q]);
         if ((valid >> j & 1u) && sc[j] > -INFINITY && !(sc[j] < fl)) ok |= 1u << j;
       }
+      if (!__any_sync(full_mask(), ok != 0u)) continue;  // nothing at or above the floor
+      if (r == rounds - 1) {
+        // Last block and every admissible score fits in the list: append them
+        // all, unsorted (published lists need not be ordered; the merge
+        // selects and sorts), without the prefilter.
+        const int n_ok = __popc(ok);
+        int incl_ok = n_ok;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+          const int t = __shfl_up_sync(full_mask(), incl_ok, o);
+          if (lane >= o) incl_ok += t;
+        }
+        const int total_ok = __shfl_sync(full_mask(), incl_ok, kWarp - 1);
+        if (cnt[q] + total_ok <= k) {
+          float* ls = list_s + q * kmax;
+          uint32_t* li = list_i + q * kmax;
+          int at = cnt[q] + incl_ok - n_ok;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (ok >> j & 1u) {
+              ls[at] = sc[j];
+              li[at] = ids[j];
+              ++at;
+            }
+          }
+          cnt[q] += total_ok;
+          __syncwarp();
+          continue;
+        }
+      }
       unsigned pass = 0;
       if (cnt[q] == k) {
 #pragma unroll
@@ -973,6 +1003,23 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       }
       const int total = __shfl_sync(full_mask(), incl, kWarp - 1);
       if (total == 0) continue;
+      float* ls = list_s + q * kmax;
+      uint32_t* li = list_i + q * kmax;
+      if (r == rounds - 1 && cnt[q] + total <= k) {
+        // Last block and the prefiltered scores fit: append without sorting.
+        int at = cnt[q] + incl - n_mine;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (pass >> j & 1u) {
+            ls[at] = sc[j];
+            li[at] = ids[j];
+            ++at;
+          }
+        }
+        cnt[q] += total;
+        __syncwarp();
+        continue;
+      }
       int pos = incl - n_mine;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -982,8 +1029,6 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
           ++pos;
         }
       }
-      float* ls = list_s + q * kmax;
-      uint32_t* li = list_i + q * kmax;
       for (int t = lane; t < cnt[q]; t += kWarp) {
         buf_s[total + t] = ls[t];
         buf_i[total + t] = li[t];
@@ -1304,25 +1349,18 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-__global__ void probe_floor_kernel(const float* __restrict__ cand_score, const uint32_t* __restrict__ list_count,
-                                   long long nq, int max_probe, int k, float* __restrict__ floor) {
+__global__ void probe_floor_kernel(const float* __restrict__ top_s, const uint64_t* __restrict__ top_i,
+                                   long long nq, int k, uint64_t pad, float* __restrict__ floor) {
   const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (q >= nq) return;
-  float f = -INFINITY;
-  if (list_count[q] >= 2u) {
-    const long long l0 = q * max_probe * 2;  // probe 0, tile sets 0 and 1
-    const float a = cand_score[l0 * k + (k - 1)];
-    const float b = cand_score[(l0 + 1) * k + (k - 1)];
-    f = fmaxf(a, b);  // -inf pads when a tile set holds fewer than k candidates
-  }
-  floor[q] = f;
+  const long long last = q * k + (k - 1);
+  floor[q] = top_i[last] != pad ? top_s[last] : -INFINITY;
 }
 
-cudaError_t launch_probe_floor(const float* cand_score, const uint32_t* list_count, long long nq, int max_probe,
-                               int k, float* floor, cudaStream_t stream) {
+cudaError_t launch_probe_floor(const float* top_s, const uint64_t* top_i, long long nq, int k, uint64_t pad,
+                               float* floor, cudaStream_t stream) {
   if (nq <= 0) return cudaSuccess;
-  probe_floor_kernel<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, stream>>>(cand_score, list_count, nq,
-                                                                                   max_probe, k, floor);
+  probe_floor_kernel<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, stream>>>(top_s, top_i, nq, k, pad, floor);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,8 @@ cudaError_t launch_assign(const float* A, long long m, const float* B, long long
 
 // Largest number of buckets one query may probe.
 constexpr int kMaxProbe = 2048;
+// Probes scanned before the rest to bound the candidates kept from the rest.
+constexpr int kFloorProbes = 8;
 
 // Per row of S (row stride ld, ncols valid columns): the top p entries, score
 // descending, equal scores by lower column; p <= kMaxProbe. Rows with fewer
@@ -150,11 +152,11 @@ struct BucketScanArgs {
   const float* floor = nullptr;
 };
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
-// floor[q] = the larger k-th score of the two lists of probe 0 (each list is
-// the exact top k of its tile set, so either k-th score is a lower bound of
-// the k-th best over all probes); -inf for queries without probes.
-cudaError_t launch_probe_floor(const float* cand_score, const uint32_t* list_count, long long nq, int max_probe,
-                               int k, float* floor, cudaStream_t stream);
+// floor[q] = the k-th score of the merged top k of the first probes (a lower
+// bound of the k-th best over all probes), -inf when that top k is not full
+// (its k-th id is `pad`).
+cudaError_t launch_probe_floor(const float* top_s, const uint64_t* top_i, long long nq, int k, uint64_t pad,
+                               float* floor, cudaStream_t stream);
 
 // ---- multi-index persistent scan (tq_multi.cu) -----------------------------
 // One flat index of a multi-index launch: its scan layout, its queries' LUTs

@@ -45,7 +45,7 @@ namespace vcb {
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
   DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
-      cand_i, rr_s, rr_i, np, floor;
+      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i;
   FlatScratchStore flat;
   ProbeScratch probe;
 };
@@ -486,21 +486,39 @@ struct tq_bucketed {
       ba.max_probe = max_probe;
       ba.cand_score = sc.cand_s.as<float>();
       ba.cand_id = sc.cand_i.as<uint32_t>();
-      // Probe 0 first: the k-th best score of a query's best-routed bucket is a
-      // lower bound of its k-th best over all probes, so the scan of probes
-      // 1.. keeps only scores at or above it (fewer list insertions, sparse
-      // lists for the merge). The kept top k is the same.
-      const bool two_phase = max_probe > 1;
+      // The best-routed buckets first: the k-th best score over a query's
+      // first kFloorProbes probes is a lower bound of its k-th best over all
+      // probes, so the scan of the remaining probes keeps only scores at or
+      // above it (few list insertions, mostly empty lists for the merge). The
+      // kept top k is the same.
+      const int first = std::min(vcb::kFloorProbes, max_probe);
+      const bool two_phase = max_probe > first;
       if (two_phase) {
         pa.probe_begin = 0;
-        pa.probe_end = 1;
+        pa.probe_end = first;
         eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
         eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
-        eng->launch(tq_index::kPrep, s, "floor kernel", [&] {
-          return vcb::launch_probe_floor(ba.cand_score, pa.list_count, static_cast<long long>(m), max_probe,
-                                         static_cast<int>(kscan), sc.floor.as<float>(), s);
+        sc.fl_s.reserve(m * kscan * 4);
+        sc.fl_i.reserve(m * kscan * 8);
+        vcb::MergeArgs fm{};
+        fm.cand_score = ba.cand_score;
+        fm.cand_id = ba.cand_id;
+        fm.nq = static_cast<long long>(m);
+        fm.n_lists = 2 * first;
+        fm.list_stride = 2 * max_probe;
+        fm.k = static_cast<int>(kscan);
+        fm.k_out = static_cast<int>(kscan);
+        fm.out_score = sc.fl_s.as<float>();
+        fm.out_id = sc.fl_i.as<uint64_t>();
+        fm.list_count = pa.list_count;
+        fm.pad_id = ~0ull;
+        eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
+          cudaError_t e = vcb::launch_merge(fm, s);
+          if (e != cudaSuccess) return e;
+          return vcb::launch_probe_floor(fm.out_score, fm.out_id, static_cast<long long>(m),
+                                         static_cast<int>(kscan), ~0ull, sc.floor.as<float>(), s);
         });
-        pa.probe_begin = 1;
+        pa.probe_begin = first;
         pa.probe_end = max_probe;
         ba.floor = sc.floor.as<float>();
       }
@@ -516,6 +534,7 @@ struct tq_bucketed {
       mg.out_score = d_scores + q0 * ke;
       mg.out_id = d_ids + q0 * ke;
       mg.list_count = pa.list_count;
+      mg.sparse_lists = two_phase;  // past probe 0 most lists hold nothing above the floor
       if (rerank) {
         sc.rr_s.reserve(m * kscan * 4);
         sc.rr_i.reserve(m * kscan * 8);
