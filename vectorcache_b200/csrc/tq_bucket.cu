@@ -746,6 +746,11 @@ struct ItemView {
   int pc;                    // queries of the item
   float* cand_s;
   uint32_t* cand_i;
+  // nullptr: each (query, tile set) writes its own list of k entries at
+  // ItemQueries::list, -inf padded. Otherwise ItemQueries::list is the start
+  // (in lists of k) of the query's candidate region and the kept candidates
+  // are appended there at append_count[query] (atomically), unpadded.
+  uint32_t* append_count = nullptr;
 };
 
 // The item's queries, in shared memory (filled by the calling kernel).
@@ -1057,6 +1062,23 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   }
   // Publish the list (tile set 0's list + tile set) of every valid query of this warp.
   if (!quad_ok) return;
+  if (v.append_count) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (quad * 4 + q >= pc) break;
+      const int c = cnt[q];
+      if (c == 0) continue;  // warp-uniform
+      unsigned at = 0;
+      if (lane == 0) at = atomicAdd(v.append_count + iq.q[quad * 4 + q], static_cast<unsigned>(c));
+      at = __shfl_sync(full_mask(), at, 0);
+      const long long base = iq.list[quad * 4 + q] * k + at;
+      for (int t = lane; t < c; t += kWarp) {
+        v.cand_s[base + t] = list_s[q * kmax + t];
+        v.cand_i[base + t] = list_i[q * kmax + t];
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     if (quad * 4 + q >= pc) break;
@@ -1085,7 +1107,8 @@ __global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketSca
       const uint32_t pr = a.pairs[it.y + t];
       const int q = static_cast<int>(pr / static_cast<uint32_t>(a.max_probe));
       iq.q[t] = q;
-      iq.list[t] = static_cast<long long>(pr) * 2;
+      // (query, probe) lists, or the query's region when appending
+      iq.list[t] = a.append_count ? static_cast<long long>(q) * a.max_probe * 2 : static_cast<long long>(pr) * 2;
       iq.scale[t] = a.lut_scale[q];
       iq.init[t] = a.fa_init[q];
       iq.off[t] = a.offsets[pr];
@@ -1101,7 +1124,8 @@ __global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketSca
   }
   __syncthreads();
   const ItemView v{a.codes, a.alpha, a.slot_ids, static_cast<long long>(a.slot_start[b]),
-                   static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id};
+                   static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id,
+                   a.append_count};
   scan_item<NIBBLE8>(v, iq, smem);
 }
 

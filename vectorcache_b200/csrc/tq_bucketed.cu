@@ -45,7 +45,7 @@ namespace vcb {
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
   DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
-      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i;
+      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount;
   FlatScratchStore flat;
   ProbeScratch probe;
 };
@@ -486,12 +486,18 @@ struct tq_bucketed {
       ba.max_probe = max_probe;
       ba.cand_score = sc.cand_s.as<float>();
       ba.cand_id = sc.cand_i.as<uint32_t>();
+      // Every (query, probe, tile set) appends its kept candidates to the
+      // query's region; the merges read exactly those.
+      sc.acount.reserve(m * 4);
+      vcb::check(cudaMemsetAsync(sc.acount.get(), 0, m * 4, s), "cudaMemsetAsync");
+      ba.append_count = sc.acount.as<uint32_t>();
       // The best-routed buckets first: the k-th best score over a query's
-      // first kFloorProbes probes is a lower bound of its k-th best over all
+      // first 8 (16 from 256 probes) probes is a lower bound of its k-th best over all
       // probes, so the scan of the remaining probes keeps only scores at or
-      // above it (few list insertions, mostly empty lists for the merge). The
-      // kept top k is the same.
-      const int first = std::min(vcb::kFloorProbes, max_probe);
+      // above it (few insertions, few candidates for the merge). The kept top
+      // k is the same.
+      const int first =
+          std::min(max_probe >= vcb::kFloorWideFrom ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
       const bool two_phase = max_probe > first;
       if (two_phase) {
         pa.probe_begin = 0;
@@ -510,7 +516,7 @@ struct tq_bucketed {
         fm.k_out = static_cast<int>(kscan);
         fm.out_score = sc.fl_s.as<float>();
         fm.out_id = sc.fl_i.as<uint64_t>();
-        fm.list_count = pa.list_count;
+        fm.entry_count = ba.append_count;
         fm.pad_id = ~0ull;
         eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
           cudaError_t e = vcb::launch_merge(fm, s);
@@ -533,8 +539,7 @@ struct tq_bucketed {
       mg.k_out = static_cast<int>(kscan);
       mg.out_score = d_scores + q0 * ke;
       mg.out_id = d_ids + q0 * ke;
-      mg.list_count = pa.list_count;
-      mg.sparse_lists = two_phase;  // past probe 0 most lists hold nothing above the floor
+      mg.entry_count = ba.append_count;
       if (rerank) {
         sc.rr_s.reserve(m * kscan * 4);
         sc.rr_i.reserve(m * kscan * 8);

@@ -108,11 +108,11 @@ struct MergeArgs {
   const uint32_t* list_count = nullptr;
   // Id written into result slots no candidate filled (their score is 0).
   uint64_t pad_id = 0;
-  // Each list holds its candidates first, then -inf padding, and most lists
-  // are empty: the merge skips lists whose first entry is -inf.
-  bool sparse_lists = false;
   // Lists per query in memory when only the first n_lists are merged (0: n_lists).
   int list_stride = 0;
+  // Optional per query: its candidates are the first entry_count[q] entries of
+  // its region (list_stride * k entries), unpadded; list_count is then unused.
+  const uint32_t* entry_count = nullptr;
 };
 
 size_t encode_smem_bytes(int dim, bool tqplus);

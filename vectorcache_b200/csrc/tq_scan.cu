@@ -443,7 +443,6 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
 constexpr int kMergeThreads = 256;
 constexpr int kMergeChunk = 1024;
 constexpr int kMergeCap = 2048;  // >= kMergeChunk + kMaxK, power of two
-constexpr int kMergeMaxLists = 4096;  // sparse merge: lists per query (2 per probe, <= 2048 probes)
 
 __device__ void cta_sort_best_first(float* s, uint32_t* id, int p) {
   for (int size = 2; size <= p; size <<= 1) {
@@ -466,42 +465,20 @@ __device__ void cta_sort_best_first(float* s, uint32_t* id, int p) {
   }
 }
 
-// SPARSE: most lists are empty (their first entry is -inf); the CTA first
-// collects the non-empty ones and then reads only those.
-template <bool SPARSE>
 __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   __shared__ float buf_s[kMergeCap];
   __shared__ uint32_t buf_i[kMergeCap];
   __shared__ float best_s[kMaxK];
   __shared__ uint32_t best_i[kMaxK];
   __shared__ int n_new;
-  __shared__ uint32_t live[SPARSE ? kMergeMaxLists : 1];
-  __shared__ int n_live;
   const long long qi = blockIdx.x;
   const long long stride = static_cast<long long>(a.list_stride ? a.list_stride : a.n_lists) * a.k;
-  const int lists = a.list_count ? static_cast<int>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
-                                 : a.n_lists;
+  const long long total =
+      a.entry_count ? static_cast<long long>(a.entry_count[qi])
+                    : (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
+                                    : static_cast<long long>(a.n_lists)) * a.k;
   const float* cs = a.cand_score + qi * stride;
   const uint32_t* ci = a.cand_id + qi * stride;
-  const int k = a.k;
-  long long total = static_cast<long long>(lists) * k;
-  if constexpr (SPARSE) {
-    if (threadIdx.x == 0) n_live = 0;
-    __syncthreads();
-    for (int l = threadIdx.x; l < lists; l += blockDim.x) {
-      if (cs[static_cast<long long>(l) * k] > -INFINITY) live[atomicAdd(&n_live, 1)] = static_cast<uint32_t>(l);
-    }
-    __syncthreads();
-    total = static_cast<long long>(n_live) * k;
-  }
-  // Position in the candidate arrays of the v-th entry considered.
-  auto entry = [&](long long v) -> long long {
-    if constexpr (SPARSE) {
-      return static_cast<long long>(live[v / k]) * k + v % k;
-    } else {
-      return v;
-    }
-  };
   const int kout = a.k_out;
   int nbest = 0;
   float thr_s = -FLT_MAX;
@@ -515,7 +492,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       const long long v = base + threadIdx.x + u * kMergeThreads;
-      s[u] = v < total ? cs[entry(v)] : -INFINITY;
+      s[u] = v < total ? cs[v] : -INFINITY;
       any |= s[u] > -INFINITY && (nbest < kout || !(s[u] < thr_s));
     }
     if (!__syncthreads_or(any)) continue;
@@ -524,7 +501,7 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       if (s[u] > -INFINITY && (nbest < kout || !(s[u] < thr_s))) {
-        const uint32_t id = ci[entry(base + threadIdx.x + u * kMergeThreads)];
+        const uint32_t id = ci[base + threadIdx.x + u * kMergeThreads];
         if (nbest < kout || better(s[u], id, thr_s, thr_i)) {
           const int pos = atomicAdd(&n_new, 1);
           buf_s[pos] = s[u];
@@ -579,8 +556,10 @@ __global__ void __launch_bounds__(kMergeThreads) merge_reg_kernel(MergeArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long qi = blockIdx.x;
   const long long stride = static_cast<long long>(a.list_stride ? a.list_stride : a.n_lists) * a.k;
-  const long long total = (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
-                                        : static_cast<long long>(a.n_lists)) * a.k;
+  const long long total =
+      a.entry_count ? static_cast<long long>(a.entry_count[qi])
+                    : (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
+                                    : static_cast<long long>(a.n_lists)) * a.k;
   const float* cs = a.cand_score + qi * stride;
   const uint32_t* ci = a.cand_id + qi * stride;
   const int kout = a.k_out;
@@ -763,11 +742,7 @@ cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream) {
     merge_reg_kernel<<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
     return cudaGetLastError();
   }
-  if (a.sparse_lists && a.n_lists <= kMergeMaxLists) {
-    merge_kernel<true><<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
-    return cudaGetLastError();
-  }
-  merge_kernel<false><<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
+  merge_kernel<<<static_cast<unsigned>(a.nq), kMergeThreads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
