@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
     p.add_argument("--rerank", type=int, default=100, help="bucketed: candidates re-ranked exactly (0 = off)")
     p.add_argument("--epochs", type=int, default=30)
+    p.add_argument("--bucketed-fixed-only", type=int, default=0,
+                   help="bucketed: time the plain path at this n_probe only (no sweep, no learned probe)")
     return p.parse_args()
 
 
@@ -558,10 +560,15 @@ def run_bucketed(args, world, rank, local):
     # The plain path at fixed n_probe: QPS and Recall@10 per n_probe; the
     # operating point is the smallest n_probe reaching the recall target.
     sweep = {}
-    for p in FIXED_PROBES:
+    for p in ([args.bucketed_fixed_only] if args.bucketed_fixed_only else FIXED_PROBES):
         ms = timed(lambda p=p: idx.search_device(d_q, k, d_s, d_i, n_probe=p, stream=stream))
         sweep[p] = {"n_probe": p, "ms_per_step": ms, "qps": nq / (ms / 1e3),
                     "recall_at_10": float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())}
+    if args.bucketed_fixed_only:
+        # the plain path at one n_probe only (profiling runs)
+        print(json.dumps({"metric": BUCKETED_METRIC, "fixed_only": sweep[args.bucketed_fixed_only]}), flush=True)
+        idx.close()
+        return
     reach = [p for p in FIXED_PROBES if sweep[p]["recall_at_10"] >= RECALL_TARGET]
     p_op = reach[0] if reach else FIXED_PROBES[-1]
     fixed = sweep[p_op]
