@@ -254,6 +254,14 @@ int tq_bucketed_search_device(tq_bucketed* h, const float* d_queries, size_t nq,
  * <q_hat, routing centroid>, best first (device buffers nq x p). */
 int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t p,
                              float* d_top_scores, uint32_t* d_top_ids, void* stream);
+/* The selection the routing uses, on any device score matrix (rows x ncols,
+ * row stride ld floats): per row the top p (<= 2048) columns, score
+ * descending, equal scores by lower column; -inf and NaN are never selected
+ * and rows with fewer than p selectable columns end in (-inf, 0xffffffff).
+ * Outputs rows x p. No counterpart in the reference (its probe order is the
+ * heap order of the same key). */
+int tq_select_top_device(const float* d_scores, size_t rows, size_t ld, size_t ncols, size_t p,
+                         float* d_top_scores, uint32_t* d_top_ids, int device, void* stream);
 
 /* Introspection for parity checks. */
 int tq_bucketed_info(const tq_bucketed* h, size_t* dim, size_t* dim_padded, size_t* bits, size_t* n,

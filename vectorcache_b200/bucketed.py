@@ -264,3 +264,18 @@ def search_learned_device(index: "BucketedTurboQuantIndex", d_queries, k: int, m
 
 
 BucketedTurboQuantIndex.search_learned_device = search_learned_device
+
+
+def select_top_device(d_scores, p: int, d_top_scores, d_top_ids, ncols: int | None = None, device: int = 0,
+                      stream=None) -> None:
+    """Per row of a device score matrix (torch CUDA tensor, rows x ld floats),
+    the top p columns, score descending, equal scores by lower column; -inf and
+    NaN are never selected (tq_select_top_device, the routing's selection).
+    d_top_scores (float32) and d_top_ids (int32 / uint32) are rows x p."""
+    lib = load_library()
+    fn = lib.tq_select_top_device
+    fn.restype = C.c_int
+    fn.argtypes = [_P, _SZ, _SZ, _SZ, _SZ, _P, _P, C.c_int, _P]
+    rows, ld = int(d_scores.shape[0]), int(d_scores.stride(0))
+    _check(fn(_dev(d_scores)[0], rows, ld, int(ncols if ncols is not None else d_scores.shape[1]), p,
+              _dev(d_top_scores)[0], _dev(d_top_ids)[0], device, _stream_ptr(stream)))

@@ -201,6 +201,153 @@ __device__ void cta_sort(float* s, uint32_t* id, int p) {
   }
 }
 
+// Top-p by radix selection, for rows that fit in shared memory: the row's
+// scores become order-preserving 32-bit keys, four 8-bit histogram passes find
+// the p-th largest key T, every key above T and the lowest columns holding T
+// are gathered, and only those p entries are sorted. Same output as
+// select_top_kernel (a score order with ties by column; -inf and NaN never
+// selected).
+constexpr int kRadixThreads = 256;
+constexpr int kRadixMaxCols = 32768;
+
+// Scores that can be selected map to keys > 0 ordered like the scores (-0 as +0).
+__device__ __forceinline__ uint32_t select_key(float v) {
+  if (!(v > -INFINITY)) return 0u;
+  uint32_t u = __float_as_uint(v);
+  if (u == 0x80000000u) u = 0u;
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void __launch_bounds__(kRadixThreads) select_radix_kernel(const float* __restrict__ S, long long ld,
+                                                                     int ncols, int p, float* __restrict__ out_s,
+                                                                     uint32_t* __restrict__ out_i) {
+  extern __shared__ __align__(16) unsigned char rad_smem[];
+  int p2 = 2;
+  while (p2 < p) p2 <<= 1;
+  float* bs = reinterpret_cast<float*>(rad_smem);
+  uint32_t* bi = reinterpret_cast<uint32_t*>(bs + p2);
+  uint32_t* keys = bi + p2;  // ncols
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_valid, s_eq, s_n, s_bin, s_above, s_warp[kRadixThreads / kWarp];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long row = blockIdx.x;
+  const float* sr = S + row * ld;
+  if (threadIdx.x == 0) {
+    s_valid = 0u;
+    s_eq = 0u;
+    s_n = 0u;
+  }
+  __syncthreads();
+  unsigned mine = 0;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    const uint32_t k = select_key(sr[c]);
+    keys[c] = k;
+    mine += k != 0u;
+  }
+  atomicAdd(&s_valid, mine);
+  __syncthreads();
+  const unsigned n_valid = s_valid;
+  // T: the p-th largest key (0 when every valid key is taken); rank: how many
+  // keys equal to T belong to the top p.
+  uint32_t T = 0u, mask = 0u;
+  unsigned rank = 0u;
+  if (n_valid > static_cast<unsigned>(p)) {
+    rank = static_cast<unsigned>(p);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      hist[threadIdx.x] = 0u;  // blockDim.x == 256
+      __syncthreads();
+      for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+        const uint32_t k = keys[c];
+        if (k != 0u && (k & mask) == T) atomicAdd(&hist[(k >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // lane l holds bins 255 - 8l .. 248 - 8l (highest first)
+        unsigned c8[8], sum = 0u;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          c8[j] = hist[255 - (lane * 8 + j)];
+          sum += c8[j];
+        }
+        unsigned incl = sum;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+          const unsigned t = __shfl_up_sync(full_mask(), incl, o);
+          if (lane >= o) incl += t;
+        }
+        const unsigned excl = incl - sum;
+        if (excl < rank && rank <= incl) {
+          unsigned acc = excl;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (acc + c8[j] >= rank) {
+              s_bin = 255u - static_cast<unsigned>(lane * 8 + j);
+              s_above = acc;
+              break;
+            }
+            acc += c8[j];
+          }
+        }
+      }
+      __syncthreads();
+      T |= s_bin << shift;
+      mask |= 0xffu << shift;
+      rank -= s_above;
+      __syncthreads();  // s_bin / s_above are rewritten by the next pass
+    }
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+      if (keys[c] == T) atomicAdd(&s_eq, 1u);
+    }
+    __syncthreads();
+  }
+  const unsigned n_eq = s_eq;
+  // Every key above T (all valid keys when T = 0), and the keys equal to T
+  // when all of them belong to the top p.
+  const bool all_eq = n_eq <= rank;
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    const uint32_t k = keys[c];
+    if (k > T || (k == T && k != 0u && all_eq)) {
+      const unsigned pos = atomicAdd(&s_n, 1u);
+      bs[pos] = sr[c];
+      bi[pos] = static_cast<uint32_t>(c);
+    }
+  }
+  if (!all_eq) {
+    // More keys equal T than fit: the lowest `rank` columns, in column order.
+    unsigned base = 0u;
+    for (int c0 = 0; c0 < ncols; c0 += blockDim.x) {
+      const int c = c0 + threadIdx.x;
+      const bool eq = c < ncols && keys[c] == T;
+      const unsigned bal = __ballot_sync(full_mask(), eq);
+      __syncthreads();
+      if (lane == 0) s_warp[warp] = __popc(bal);
+      __syncthreads();
+      unsigned before = base;
+      for (int w = 0; w < warp; ++w) before += s_warp[w];
+      before += __popc(bal & ((1u << lane) - 1u));
+      if (eq && before < rank) {
+        const unsigned pos = atomicAdd(&s_n, 1u);
+        bs[pos] = sr[c];
+        bi[pos] = static_cast<uint32_t>(c);
+      }
+      for (int w = 0; w < kRadixThreads / kWarp; ++w) base += s_warp[w];
+    }
+  }
+  __syncthreads();
+  const int n = static_cast<int>(s_n);
+  for (int t = n + threadIdx.x; t < p2; t += blockDim.x) {
+    bs[t] = -INFINITY;
+    bi[t] = 0xffffffffu;
+  }
+  __syncthreads();
+  cta_sort(bs, bi, p2);
+  for (int t = threadIdx.x; t < p; t += blockDim.x) {
+    const bool have = t < n;
+    out_s[row * p + t] = have ? bs[t] : -INFINITY;
+    out_i[row * p + t] = have ? bi[t] : 0xffffffffu;
+  }
+}
+
 __global__ void __launch_bounds__(kSelThreads) select_top_kernel(const float* __restrict__ S, long long ld,
                                                                  int ncols, int p, float* __restrict__ out_s,
                                                                  uint32_t* __restrict__ out_i) {
@@ -1246,6 +1393,16 @@ cudaError_t launch_select_top(const float* S, long long rows, long long ld, int 
                               uint32_t* out_i, cudaStream_t stream) {
   if (rows == 0) return cudaSuccess;
   if (p < 1 || p > kMaxProbe) return cudaErrorInvalidValue;
+  if (ncols <= kRadixMaxCols) {
+    int p2 = 2;
+    while (p2 < p) p2 <<= 1;
+    const size_t rsmem = static_cast<size_t>(p2) * 8 + static_cast<size_t>(ncols) * 4;
+    cudaError_t e = cudaFuncSetAttribute(select_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(rsmem));
+    if (e != cudaSuccess) return e;
+    select_radix_kernel<<<static_cast<unsigned>(rows), kRadixThreads, rsmem, stream>>>(S, ld, ncols, p, out_s, out_i);
+    return cudaGetLastError();
+  }
   const size_t smem = static_cast<size_t>(sel_cap(p)) * 8 + static_cast<size_t>(p) * 8;
   cudaError_t e = cudaFuncSetAttribute(select_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));

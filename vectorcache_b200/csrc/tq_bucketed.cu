@@ -810,6 +810,22 @@ int tq_bucketed_search_learned_device(tq_bucketed* h, const float* d_queries, si
   });
 }
 
+int tq_select_top_device(const float* d_scores, size_t rows, size_t ld, size_t ncols, size_t p, float* d_top_scores,
+                         uint32_t* d_top_ids, int device, void* stream) {
+  return vcb::guarded([&] {
+    require(p >= 1 && p <= static_cast<size_t>(vcb::kMaxProbe), TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 2048]");
+    require(ncols <= ld || rows <= 1, TQ_ERR_INVALID_ARGUMENT, "ncols must be <= ld");
+    require(ncols <= 0x7fffffffu, TQ_ERR_INVALID_ARGUMENT, "ncols too large");
+    if (rows == 0) return;
+    require(d_scores && d_top_scores && d_top_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    vcb::DeviceGuard g(device);
+    vcb::check(vcb::launch_select_top(d_scores, static_cast<long long>(rows), static_cast<long long>(ld),
+                                      static_cast<int>(ncols), static_cast<int>(p), d_top_scores, d_top_ids,
+                                      static_cast<cudaStream_t>(stream)),
+               "select kernel");
+  });
+}
+
 int tq_bucketed_route_device(tq_bucketed* h, const float* d_queries, size_t nq, size_t p, float* d_top_scores,
                              uint32_t* d_top_ids, void* stream) {
   return vcb::guarded([&] {
