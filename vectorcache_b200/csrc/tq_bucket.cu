@@ -830,6 +830,19 @@ __global__ void pair_offset_kernel(PairArgs a) {
   if (lane == 0) a.offsets[t] = d;
 }
 
+// One thread per (query, probe): the offset read from the precomputed
+// q_hat . enc^T matrix.
+__global__ void pair_offset_gather_kernel(PairArgs a) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= a.nq * a.max_probe) return;
+  const long long q = t / a.max_probe;
+  const int j = static_cast<int>(t % a.max_probe);
+  if (!pair_in_range(a, q, j)) return;
+  const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
+  if (b >= static_cast<uint32_t>(a.nb)) return;
+  a.offsets[t] = a.enc_scores[q * a.enc_ld + b];
+}
+
 __global__ void item_build_kernel(PairArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.nb) return;
@@ -1523,7 +1536,11 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
   if (total > 0) {
     pair_scatter_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    pair_offset_kernel<<<static_cast<unsigned>((total * kWarp + 255) / 256), 256, 0, stream>>>(a);
+    if (a.enc_scores) {
+      pair_offset_gather_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
+    } else {
+      pair_offset_kernel<<<static_cast<unsigned>((total * kWarp + 255) / 256), 256, 0, stream>>>(a);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   item_build_kernel<<<static_cast<unsigned>((a.nb + 255) / 256), 256, 0, stream>>>(a);

@@ -131,6 +131,10 @@ struct PairArgs {
   // search scans probe 0 first to bound the rest; list_count always counts all).
   int probe_begin = 0;
   int probe_end = 1 << 30;
+  // Optional: q_hat . enc^T (nq rows, row stride enc_ld) computed beforehand;
+  // offsets are then read from it instead of one dot product per pair.
+  const float* enc_scores = nullptr;
+  long long enc_ld = 0;
 };
 // Groups the (query, probe) pairs by bucket and builds the scan work items.
 cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);

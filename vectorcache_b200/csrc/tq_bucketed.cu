@@ -45,7 +45,7 @@ namespace vcb {
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
   DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
-      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount;
+      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount, encs;
   FlatScratchStore flat;
   ProbeScratch probe;
 };
@@ -462,6 +462,15 @@ struct tq_bucketed {
       pa.items = sc.items.as<uint4>();
       pa.n_items = sc.nitems.as<unsigned long long>();
       pa.list_count = sc.lcount.as<uint32_t>();
+      // Offsets <q_hat, encode_c> of every probed bucket: one q_hat . enc^T
+      // product per pass, gathered per pair.
+      sc.encs.reserve(m * nb * 4);
+      eng->launch(tq_index::kPrep, s, "offset kernel", [&] {
+        return vcb::launch_gemm_nt(qh, static_cast<long long>(m), d_enc.as<float>(), nb, static_cast<int>(dim),
+                                   sc.encs.as<float>(), nb, s);
+      });
+      pa.enc_scores = sc.encs.as<float>();
+      pa.enc_ld = nb;
       const size_t lists = m * max_probe * 2;
       sc.cand_s.reserve(lists * kscan * 4);
       sc.cand_i.reserve(lists * kscan * 4);
