@@ -102,3 +102,11 @@ def test_against_oracle(oracle, case):
         ws, wi = oracle.topk(want_scores, k)
         assert np.array_equal(res.ids, wi), k
         assert bits_equal(res.scores, ws), k
+    # One and two queries: with several 256-group batches (dim > 512 at 3/4
+    # bits, > 1024 at 2 bits) the scan splits the work by batch.
+    for m in (1, 2):
+        for k in (1, 10):
+            res = idx.search(q[:m], k)
+            ws, wi = oracle.topk(want_scores[:m], k)
+            assert np.array_equal(res.ids, wi), (m, k)
+            assert bits_equal(res.scores, ws), (m, k)

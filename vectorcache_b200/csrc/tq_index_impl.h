@@ -80,18 +80,20 @@ class DeviceGuard {
 inline size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
 // Device scratch of one flat search: query LUTs, per-query constants and
-// candidate lists. Grown on demand by the search.
+// candidate lists, and (optional) the batch-split scan's integer sums. Grown
+// on demand by the search.
 struct FlatScratch {
   DeviceBuffer* luts;
   DeviceBuffer* qf;
   DeviceBuffer* cand_s;
   DeviceBuffer* cand_i;
+  DeviceBuffer* partial = nullptr;  // nullptr: the scan does not split
 };
 
 // Owning variant for callers that run searches concurrently (one per stream).
 struct FlatScratchStore {
-  DeviceBuffer luts, qf, cand_s, cand_i;
-  FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i}; }
+  DeviceBuffer luts, qf, cand_s, cand_i, partial;
+  FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i, &partial}; }
 };
 
 }  // namespace vcb
@@ -120,7 +122,7 @@ struct tq_index {
   vcb::DeviceBuffer d_perm_sign, d_bnd, d_cen, d_shift, d_scale, d_inv_scale;
   vcb::DeviceBuffer d_codes, d_alpha, d_staged, d_flat, d_counter;
   // search scratch
-  vcb::DeviceBuffer d_queries, d_luts, d_qf, d_cand_s, d_cand_i, d_out_s, d_out_i, d_qrot;
+  vcb::DeviceBuffer d_queries, d_luts, d_qf, d_cand_s, d_cand_i, d_out_s, d_out_i, d_qrot, d_partial;
 
   // Optional per-launch timing (tq_index_set_profiling).
   enum Kind { kPrep = 0, kScan = 1, kMerge = 2, kEncode = 3 };
@@ -251,7 +253,7 @@ struct tq_index {
   }
 
   // The index's own search scratch (one search at a time on one stream).
-  vcb::FlatScratch own_scratch() { return {&d_luts, &d_qf, &d_cand_s, &d_cand_i}; }
+  vcb::FlatScratch own_scratch() { return {&d_luts, &d_qf, &d_cand_s, &d_cand_i, &d_partial}; }
 
   // LUTs and per-query constants for nq device rows.
   void prep_queries(const float* d_q, size_t nq, cudaStream_t s, float* q_rot_out) {
@@ -325,6 +327,12 @@ struct tq_index {
       a.bits = static_cast<int>(bits);
       a.cand_score = sc.cand_s->as<float>();
       a.cand_id = sc.cand_i->as<uint32_t>();
+      if (plan.split_batches > 1 && sc.partial) {
+        sc.partial->reserve(m * static_cast<size_t>(plan.split_batches) * cap * 4);
+        a.partial = sc.partial->as<uint32_t>();
+        a.partial_stride = static_cast<long long>(cap);
+        a.partial_batches = plan.split_batches;
+      }
       launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
       scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
       scan_queries += m;

@@ -92,6 +92,13 @@ struct ScanArgs {
   int bits = 4;            // 3 selects the lookup that skips nibble values >= 8
   float* cand_score;       // nq x n_ranges x k
   uint32_t* cand_id;
+  // Optional scratch for the batch-split scan of one or two queries (used
+  // when the plan asks for it): integer sums [query][batch][partial_stride]
+  // over partial_batches 256-group batches; partial_stride >= the layout
+  // capacity. nullptr: the scan never splits.
+  uint32_t* partial = nullptr;
+  long long partial_stride = 0;
+  int partial_batches = 0;
 };
 
 struct MergeArgs {
@@ -143,6 +150,10 @@ struct ScanPlan {
   int lut_chunk_groups = 0;
   size_t smem_bytes = 0;
   int lists_per_range = 1;  // candidate lists each (query, range) publishes
+  // > 1: batches of the batch-split scan, which pays off for one or two
+  // queries over few blocks (whole blocks per CTA would leave the last wave
+  // of CTAs part-full); it needs ScanArgs::partial.
+  int split_batches = 0;
 };
 bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan);
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);

@@ -13,7 +13,8 @@
 // callback queued after the copy. Slots are created at start() only while the
 // device memory in use (resident indexes included) stays within the HBM
 // budget; each slot's scratch is grown there, by one full-size warm-up search
-// per index, so serving itself allocates nothing.
+// per index (and a two-query one for the batch-split scan of small flat
+// batches), so serving itself allocates nothing.
 //
 // Every query's result is computed independently of the other queries of its
 // batch (per-query LUTs and an exact top-k), so a result is the same whether
@@ -279,6 +280,9 @@ struct tq_server {
         if (t.flat) {
           t.flat->search_device(q.as<float>(), m, t.max_k, sc_s.as<float>(), sc_i.as<uint64_t>(),
                                 std::min(t.max_k, t.flat->n), nullptr, fs.ref());
+          // one- and two-query searches may take the batch-split scan kernels
+          t.flat->search_device(q.as<float>(), std::min<size_t>(m, 2), t.max_k, sc_s.as<float>(),
+                                sc_i.as<uint64_t>(), std::min(t.max_k, t.flat->n), nullptr, fs.ref());
         } else {
           const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
           vcb::bucketed_search_with(t.bkt, q.as<float>(), m, t.max_k, t.max_probe, t.mlp ? &lp : nullptr,
@@ -308,6 +312,9 @@ struct tq_server {
           const size_t ke = std::min(t.max_k, t.flat->n);
           t.flat->search_device(sl->d_q.as<float>(), max_batch, t.max_k, sl->d_s.as<float>(), sl->d_i.as<uint64_t>(),
                                 ke, sl->stream, sl->flat.ref());
+          // grows the batch-split scratch that one- and two-query batches use
+          t.flat->search_device(sl->d_q.as<float>(), std::min<size_t>(max_batch, 2), t.max_k, sl->d_s.as<float>(),
+                                sl->d_i.as<uint64_t>(), ke, sl->stream, sl->flat.ref());
         } else {
           const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
           vcb::bucketed_search_with(t.bkt, sl->d_q.as<float>(), max_batch, t.max_k, t.max_probe,
