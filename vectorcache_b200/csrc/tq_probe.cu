@@ -78,54 +78,56 @@ __global__ void features_kernel(const float* __restrict__ top, long long m, int 
 
 // C (M x N, fp32, row stride ldc) = A (M x K) . B (K x N), fp32 accumulation in
 // coordinate order. Element (i, k) of A at A[i * a_r + k * a_c]; (k, j) of B at
-// B[k * b_r + j * b_c]. 64 x 64 tile per CTA, 4 x 4 per thread, 32 coordinates
-// per shared-memory stage.
-template <typename TA, typename TB>
+// B[k * b_r + j * b_c]. T x T tile per CTA (T = 64, or 32 when 64-wide tiles
+// would leave most SMs idle), (T/16)^2 per thread, 32 coordinates per
+// shared-memory stage. Every element is the same FMA chain for either T.
+template <typename TA, typename TB, int T>
 __global__ void __launch_bounds__(256) gemm_kernel(const TA* __restrict__ A, long long a_r, long long a_c,
                                                    const TB* __restrict__ B, long long b_r, long long b_c,
                                                    float* __restrict__ C, long long ldc, long long M, int N, int K) {
-  __shared__ float sa[32][64 + 1];
-  __shared__ float sb[32][64 + 1];
-  const long long i0 = static_cast<long long>(blockIdx.y) * 64;
-  const int j0 = blockIdx.x * 64;
+  constexpr int R = T / 16;
+  __shared__ float sa[32][T + 1];
+  __shared__ float sb[32][T + 1];
+  const long long i0 = static_cast<long long>(blockIdx.y) * T;
+  const int j0 = blockIdx.x * T;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  float acc[4][4];
+  float acc[R][R];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < R; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+    for (int b = 0; b < R; ++b) acc[a][b] = 0.f;
   for (int k0 = 0; k0 < K; k0 += 32) {
     __syncthreads();
-    for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {
+    for (int e = threadIdx.x; e < T * 32; e += blockDim.x) {
       const int r = e / 32, c = e % 32;
       const long long gi = i0 + r;
       const int gk = k0 + c;
       sa[c][r] = (gi < M && gk < K) ? ld(A, gi * a_r + gk * a_c) : 0.f;
-      const int gj = j0 + (e % 64);
-      const int gk2 = k0 + e / 64;
-      sb[e / 64][e % 64] = (gj < N && gk2 < K) ? ld(B, gk2 * b_r + static_cast<long long>(gj) * b_c) : 0.f;
+      const int gj = j0 + (e % T);
+      const int gk2 = k0 + e / T;
+      sb[e / T][e % T] = (gj < N && gk2 < K) ? ld(B, gk2 * b_r + static_cast<long long>(gj) * b_c) : 0.f;
     }
     __syncthreads();
 #pragma unroll 8
     for (int c = 0; c < 32; ++c) {
-      float av[4], bv[4];
+      float av[R], bv[R];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) av[a] = sa[c][ty * 4 + a];
+      for (int a = 0; a < R; ++a) av[a] = sa[c][ty * R + a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) bv[b] = sb[c][tx * 4 + b];
+      for (int b = 0; b < R; ++b) bv[b] = sb[c][tx * R + b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < R; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = __fmaf_rn(av[a], bv[b], acc[a][b]);
+        for (int b = 0; b < R; ++b) acc[a][b] = __fmaf_rn(av[a], bv[b], acc[a][b]);
     }
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const long long gi = i0 + ty * 4 + a;
+  for (int a = 0; a < R; ++a) {
+    const long long gi = i0 + ty * R + a;
     if (gi >= M) continue;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int gj = j0 + tx * 4 + b;
+    for (int b = 0; b < R; ++b) {
+      const int gj = j0 + tx * R + b;
       if (gj < N) C[gi * ldc + gj] = acc[a][b];
     }
   }
@@ -227,9 +229,16 @@ template <typename TA, typename TB>
 cudaError_t gemm(const TA* A, long long a_r, long long a_c, const TB* B, long long b_r, long long b_c, float* C,
                  long long ldc, long long M, int N, int K, cudaStream_t s) {
   if (M == 0 || N == 0) return cudaSuccess;
+  const long long tiles64 = ((N + 63) / 64) * ((M + 63) / 64);
+  if (tiles64 < 2 * 148) {  // e.g. 1,310 x 128 outputs: 42 tiles of 64 x 64, 164 of 32 x 32
+    dim3 grid(static_cast<unsigned>((N + 31) / 32), static_cast<unsigned>((M + 31) / 32));
+    if (grid.y > 65535) return cudaErrorInvalidValue;
+    gemm_kernel<TA, TB, 32><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
+    return cudaGetLastError();
+  }
   dim3 grid(static_cast<unsigned>((N + 63) / 64), static_cast<unsigned>((M + 63) / 64));
   if (grid.y > 65535) return cudaErrorInvalidValue;
-  gemm_kernel<TA, TB><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
+  gemm_kernel<TA, TB, 64><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
   return cudaGetLastError();
 }
 
