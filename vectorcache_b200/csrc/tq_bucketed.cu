@@ -509,10 +509,6 @@ struct tq_bucketed {
           std::min(max_probe >= vcb::kFloorWideFrom ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
       const bool two_phase = max_probe > first;
       if (two_phase) {
-        pa.probe_begin = 0;
-        pa.probe_end = first;
-        eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
-        eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
         sc.fl_s.reserve(m * kscan * 4);
         sc.fl_i.reserve(m * kscan * 8);
         vcb::MergeArgs fm{};
@@ -527,15 +523,26 @@ struct tq_bucketed {
         fm.out_id = sc.fl_i.as<uint64_t>();
         fm.entry_count = ba.append_count;
         fm.pad_id = ~0ull;
-        eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
-          cudaError_t e = vcb::launch_merge(fm, s);
-          if (e != cudaSuccess) return e;
-          return vcb::launch_probe_floor(fm.out_score, fm.out_id, static_cast<long long>(m),
-                                         static_cast<int>(kscan), ~0ull, sc.floor.as<float>(), s);
-        });
+        // Probe 0 alone, then probes 1..first-1 above probe 0's floor (the
+        // first probes cost most without a floor), then the floor of all
+        // first probes for the rest. Each floor is the k-th best of the
+        // candidates appended so far, a lower bound of the final k-th best.
+        const int steps[3] = {0, 1, first};
+        for (int st = 0; st < 2; ++st) {
+          pa.probe_begin = steps[st];
+          pa.probe_end = steps[st + 1];
+          eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
+          eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
+          eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
+            cudaError_t e = vcb::launch_merge(fm, s);
+            if (e != cudaSuccess) return e;
+            return vcb::launch_probe_floor(fm.out_score, fm.out_id, static_cast<long long>(m),
+                                           static_cast<int>(kscan), ~0ull, sc.floor.as<float>(), s);
+          });
+          ba.floor = sc.floor.as<float>();
+        }
         pa.probe_begin = first;
         pa.probe_end = max_probe;
-        ba.floor = sc.floor.as<float>();
       }
       eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
