@@ -41,11 +41,11 @@ cudaError_t launch_assign(const float* A, long long m, const float* B, long long
 // Largest number of buckets one query may probe.
 constexpr int kMaxProbe = 2048;
 // Probes scanned before the rest to bound the candidates kept from the rest:
-// 8, or 16 from 256 probes on (measured at 1.2M x 100, 4-bit, k = 100 kept
-// candidates: 16 first probes scan 512 probes 3.6 % faster than 8, 2 and 4
-// are slower; with per-query probe counts averaging 178, 8 and 16 tie).
+// 8, or 32 from 256 probes on (measured at 1.2M x 100, 4-bit, k = 100 kept
+// candidates, probe 0 scanned alone first: 32 first probes scan 512 probes
+// 3.3 % and 256 probes 3.8 % faster than 16; 64 is no faster than 32).
 constexpr int kFloorProbes = 8;
-constexpr int kFloorProbesWide = 16;
+constexpr int kFloorProbesWide = 32;
 constexpr int kFloorWideFrom = 256;
 
 // Per row of S (row stride ld, ncols valid columns): the top p entries, score
