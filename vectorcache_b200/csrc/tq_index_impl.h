@@ -88,12 +88,14 @@ struct FlatScratch {
   DeviceBuffer* cand_s;
   DeviceBuffer* cand_i;
   DeviceBuffer* partial = nullptr;  // nullptr: the scan does not split
+  long long range_cap = 0;          // > 0: at most this many vectors per scan CTA
 };
 
 // Owning variant for callers that run searches concurrently (one per stream).
 struct FlatScratchStore {
   DeviceBuffer luts, qf, cand_s, cand_i, partial;
-  FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i, &partial}; }
+  long long range_cap = 0;  // see FlatScratch::range_cap
+  FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i, &partial, range_cap}; }
 };
 
 }  // namespace vcb
@@ -303,7 +305,7 @@ struct tq_index {
       prep_queries(d_q + q0 * dim, m, s, nullptr, sc);
       vcb::ScanPlan plan;
       if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
-                          static_cast<int>(k_eff), sms, &plan)) {
+                          static_cast<int>(k_eff), sms, &plan, sc.range_cap)) {
         vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
       }
       const size_t lists = static_cast<size_t>(plan.n_ranges) * plan.lists_per_range;

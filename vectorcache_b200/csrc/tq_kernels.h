@@ -155,7 +155,9 @@ struct ScanPlan {
   // of CTAs part-full); it needs ScanArgs::partial.
   int split_batches = 0;
 };
-bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan);
+// max_range_vectors > 0 bounds the vectors one CTA scans (shorter CTAs let
+// higher-priority work on other streams start sooner).
+bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors = 0);
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 

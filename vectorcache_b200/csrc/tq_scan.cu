@@ -736,7 +736,7 @@ size_t scan_warp_bytes(int q, int kmax) {
 
 }  // namespace
 
-bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan) {
+bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors) {
   if (k < 1 || k > kMaxK || n <= 0 || nq <= 0) return false;
   const int kmax = k <= kRegTopK ? kRegTopK : (k <= 64 ? 64 : 256);
   const bool reg = kmax <= kRegTopK;
@@ -780,6 +780,10 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
       ranges = rr;
     }
     if (rr == blocks) break;
+  }
+  if (max_range_vectors > 0) {
+    const long long cap_blocks = std::max(1LL, max_range_vectors / kScanBlockVectors);
+    ranges = std::max(ranges, (blocks + cap_blocks - 1) / cap_blocks);
   }
   if (ranges > 65535) ranges = 65535;
   const long long blocks_per_range = (blocks + ranges - 1) / ranges;

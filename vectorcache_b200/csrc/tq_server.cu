@@ -42,6 +42,11 @@
 
 namespace {
 
+// Vectors per scan CTA of a served flat search: a 10M x 768 3-bit scan of 128
+// queries then runs in CTAs of a few ms, so bucketed batches on the
+// high-priority stream wait at most that long for an SM.
+constexpr long long kServingRangeVectors = 65536;
+
 int64_t now_ns() {
   return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
       .count();
@@ -70,7 +75,8 @@ struct Request {
 };
 
 struct Slot {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;     // flat batches (normal priority)
+  cudaStream_t stream_hi = nullptr;  // bucketed batches (highest priority)
   cudaEvent_t done = nullptr;
   float* h_q = nullptr;
   float* h_s = nullptr;
@@ -84,11 +90,13 @@ struct Slot {
   std::atomic<int64_t> done_ns{0};
   ~Slot() {
     if (stream) cudaStreamSynchronize(stream);
+    if (stream_hi) cudaStreamSynchronize(stream_hi);
     if (h_q) cudaFreeHost(h_q);
     if (h_s) cudaFreeHost(h_s);
     if (h_i) cudaFreeHost(h_i);
     if (done) cudaEventDestroy(done);
     if (stream) cudaStreamDestroy(stream);
+    if (stream_hi) cudaStreamDestroy(stream_hi);
     if (bkt) vcb::bucket_scratch_delete(bkt);
   }
 };
@@ -138,22 +146,27 @@ struct tq_server {
       row += r->nq;
     }
     sl.nq = row;
-    vcb::check(cudaMemcpyAsync(sl.d_q.get(), sl.h_q, row * t.dim_in * 4, cudaMemcpyHostToDevice, sl.stream), "H2D");
+    // Flat scans are long (every vector for every query) and run on the slot's
+    // normal-priority stream, in CTAs of bounded work; bucketed batches go to
+    // its highest-priority stream, so the block scheduler starts their CTAs as
+    // soon as running flat CTAs retire instead of after the whole flat scan.
+    cudaStream_t s = t.flat ? sl.stream : sl.stream_hi;
+    vcb::check(cudaMemcpyAsync(sl.d_q.get(), sl.h_q, row * t.dim_in * 4, cudaMemcpyHostToDevice, s), "H2D");
     size_t ke;
     if (t.flat) {
       ke = std::min(r0->k, t.flat->n);
-      t.flat->search_device(sl.d_q.as<float>(), row, r0->k, sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), ke,
-                            sl.stream, sl.flat.ref());
+      t.flat->search_device(sl.d_q.as<float>(), row, r0->k, sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), ke, s,
+                            sl.flat.ref());
     } else {
       const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
       ke = vcb::bucketed_search_with(t.bkt, sl.d_q.as<float>(), row, r0->k, r0->n_probe, t.mlp ? &lp : nullptr,
-                                     sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), sl.stream, *sl.bkt);
+                                     sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), s, *sl.bkt);
     }
     sl.k_eff = ke;
-    vcb::check(cudaMemcpyAsync(sl.h_s, sl.d_s.get(), row * ke * 4, cudaMemcpyDeviceToHost, sl.stream), "D2H");
-    vcb::check(cudaMemcpyAsync(sl.h_i, sl.d_i.get(), row * ke * 8, cudaMemcpyDeviceToHost, sl.stream), "D2H");
-    vcb::check(cudaLaunchHostFunc(sl.stream, mark_done, &sl), "cudaLaunchHostFunc");
-    vcb::check(cudaEventRecord(sl.done, sl.stream), "cudaEventRecord");
+    vcb::check(cudaMemcpyAsync(sl.h_s, sl.d_s.get(), row * ke * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    vcb::check(cudaMemcpyAsync(sl.h_i, sl.d_i.get(), row * ke * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    vcb::check(cudaLaunchHostFunc(s, mark_done, &sl), "cudaLaunchHostFunc");
+    vcb::check(cudaEventRecord(sl.done, s), "cudaEventRecord");
     sl.busy = true;
     ++batches;
     queries += row;
@@ -298,6 +311,11 @@ struct tq_server {
     for (size_t s = 0; s < max_slots; ++s) {
       auto sl = std::make_unique<Slot>();
       vcb::check(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      int least = 0, greatest = 0;
+      vcb::check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+      vcb::check(cudaStreamCreateWithPriority(&sl->stream_hi, cudaStreamNonBlocking, greatest),
+                 "cudaStreamCreateWithPriority");
+      sl->flat.range_cap = kServingRangeVectors;
       vcb::check(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming), "cudaEventCreate");
       vcb::check(cudaMallocHost(&sl->h_q, max_batch * max_dim * 4), "cudaMallocHost");
       vcb::check(cudaMallocHost(&sl->h_s, max_batch * max_k * 4), "cudaMallocHost");
