@@ -798,7 +798,6 @@ __global__ void pair_count_kernel(PairArgs a) {
   if (t >= a.nq * a.max_probe) return;
   const long long q = t / a.max_probe;
   const int j = static_cast<int>(t % a.max_probe);
-  if (j == 0) a.list_count[q] = 2u * static_cast<uint32_t>(probes_of(a, q));
   if (!pair_in_range(a, q, j)) return;
   const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
   if (b < static_cast<uint32_t>(a.nb)) atomicAdd(&a.counts[b], 1u);
@@ -816,22 +815,8 @@ __global__ void pair_scatter_kernel(PairArgs a) {
   a.pairs[pos] = static_cast<uint32_t>(t);
 }
 
-// One warp per (query, probe): offset <q_hat, enc[b]>.
-__global__ void pair_offset_kernel(PairArgs a) {
-  const long long t = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp;
-  const int lane = threadIdx.x & 31;
-  if (t >= a.nq * a.max_probe) return;
-  const long long q = t / a.max_probe;
-  const int j = static_cast<int>(t % a.max_probe);
-  if (!pair_in_range(a, q, j)) return;
-  const uint32_t b = a.probes[q * (a.probe_stride ? a.probe_stride : a.max_probe) + j];
-  if (b >= static_cast<uint32_t>(a.nb)) return;
-  const float d = warp_dot(a.q_hat + q * a.dim, a.enc + static_cast<long long>(b) * a.dim, a.dim, lane);
-  if (lane == 0) a.offsets[t] = d;
-}
-
-// One thread per (query, probe): the offset read from the precomputed
-// q_hat . enc^T matrix.
+// One thread per (query, probe): the offset <q_hat, enc[b]> read from the
+// q_hat . enc^T product computed before the pairs.
 __global__ void pair_offset_gather_kernel(PairArgs a) {
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= a.nq * a.max_probe) return;
@@ -1536,11 +1521,7 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
   if (total > 0) {
     pair_scatter_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (a.enc_scores) {
-      pair_offset_gather_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
-    } else {
-      pair_offset_kernel<<<static_cast<unsigned>((total * kWarp + 255) / 256), 256, 0, stream>>>(a);
-    }
+    pair_offset_gather_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, stream>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   item_build_kernel<<<static_cast<unsigned>((a.nb + 255) / 256), 256, 0, stream>>>(a);

@@ -114,9 +114,10 @@ struct PairArgs {
   int max_probe;
   long long nq;
   int nb;
-  const float* q_hat;        // nq x dim
-  const float* enc;          // nb x dim encode centroids
-  int dim;
+  // q_hat . enc^T (nq rows, row stride enc_ld: <q_hat, encode centroid> of
+  // every bucket), computed before the pairs; offsets are gathered from it.
+  const float* enc_scores;
+  long long enc_ld;
   // outputs / scratch (device)
   uint32_t* counts;          // nb
   unsigned long long* pair_start;  // nb + 1
@@ -126,15 +127,10 @@ struct PairArgs {
   float* offsets;            // nq * max_probe: <q_hat, enc[probe]>
   uint4* items;              // (bucket, first pair, pair count, 0)
   unsigned long long* n_items;
-  uint32_t* list_count;      // nq: 2 * n_probe (candidate lists per query)
   // Probe positions [probe_begin, probe_end) of each query get pairs (the
-  // search scans probe 0 first to bound the rest; list_count always counts all).
+  // search scans its first probes before the rest).
   int probe_begin = 0;
   int probe_end = 1 << 30;
-  // Optional: q_hat . enc^T (nq rows, row stride enc_ld) computed beforehand;
-  // offsets are then read from it instead of one dot product per pair.
-  const float* enc_scores = nullptr;
-  long long enc_ld = 0;
 };
 // Groups the (query, probe) pairs by bucket and builds the scan work items.
 cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);

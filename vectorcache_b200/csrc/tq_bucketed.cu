@@ -44,7 +44,7 @@ namespace vcb {
 // Device scratch of one bucketed search (routing, probe pairs, candidate
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
-  DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, lcount, cand_s,
+  DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, cand_s,
       cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount, encs;
   FlatScratchStore flat;
   ProbeScratch probe;
@@ -441,7 +441,6 @@ struct tq_bucketed {
       sc.off.reserve(m * max_probe * 4);
       sc.items.reserve(static_cast<size_t>(items) * 16);
       sc.nitems.reserve(8);
-      sc.lcount.reserve(m * 4);
       vcb::PairArgs pa{};
       pa.probes = sc.top_i.as<uint32_t>();
       pa.probe_stride = ptop;
@@ -450,9 +449,6 @@ struct tq_bucketed {
       pa.max_probe = max_probe;
       pa.nq = static_cast<long long>(m);
       pa.nb = nb;
-      pa.q_hat = qh;
-      pa.enc = d_enc.as<float>();
-      pa.dim = static_cast<int>(dim);
       pa.counts = sc.counts.as<uint32_t>();
       pa.pair_start = sc.pstart.as<unsigned long long>();
       pa.item_start = sc.istart.as<unsigned long long>();
@@ -461,7 +457,6 @@ struct tq_bucketed {
       pa.offsets = sc.off.as<float>();
       pa.items = sc.items.as<uint4>();
       pa.n_items = sc.nitems.as<unsigned long long>();
-      pa.list_count = sc.lcount.as<uint32_t>();
       // Offsets <q_hat, encode_c> of every probed bucket: one q_hat . enc^T
       // product per pass, gathered per pair.
       sc.encs.reserve(m * nb * 4);

@@ -106,19 +106,16 @@ struct MergeArgs {
   const uint32_t* cand_id;
   long long nq;
   int n_lists;   // candidate lists per query
-  int k;         // entries per list (sorted, padded with -inf / 0xffffffff)
+  int k;         // entries per list (padded with -inf / 0xffffffff)
   int k_out;     // k_eff = min(k, n)
   float* out_score;     // nq x k_out
   uint64_t* out_id;
-  // Optional: lists actually filled per query (the first list_count[q] of its
-  // n_lists); nullptr means all n_lists.
-  const uint32_t* list_count = nullptr;
   // Id written into result slots no candidate filled (their score is 0).
   uint64_t pad_id = 0;
-  // Lists per query in memory when only the first n_lists are merged (0: n_lists).
+  // Lists per query in memory (0: n_lists).
   int list_stride = 0;
   // Optional per query: its candidates are the first entry_count[q] entries of
-  // its region (list_stride * k entries), unpadded; list_count is then unused.
+  // its region (list_stride * k entries), unpadded, instead of n_lists lists.
   const uint32_t* entry_count = nullptr;
 };
 

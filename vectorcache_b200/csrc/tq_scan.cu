@@ -519,10 +519,8 @@ __global__ void __launch_bounds__(kMergeThreads) merge_kernel(MergeArgs a) {
   __shared__ int n_new;
   const long long qi = blockIdx.x;
   const long long stride = static_cast<long long>(a.list_stride ? a.list_stride : a.n_lists) * a.k;
-  const long long total =
-      a.entry_count ? static_cast<long long>(a.entry_count[qi])
-                    : (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
-                                    : static_cast<long long>(a.n_lists)) * a.k;
+  const long long total = a.entry_count ? static_cast<long long>(a.entry_count[qi])
+                                        : static_cast<long long>(a.n_lists) * a.k;
   const float* cs = a.cand_score + qi * stride;
   const uint32_t* ci = a.cand_id + qi * stride;
   const int kout = a.k_out;
@@ -602,10 +600,8 @@ __global__ void __launch_bounds__(kMergeThreads) merge_reg_kernel(MergeArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long qi = blockIdx.x;
   const long long stride = static_cast<long long>(a.list_stride ? a.list_stride : a.n_lists) * a.k;
-  const long long total =
-      a.entry_count ? static_cast<long long>(a.entry_count[qi])
-                    : (a.list_count ? static_cast<long long>(min(a.list_count[qi], static_cast<uint32_t>(a.n_lists)))
-                                    : static_cast<long long>(a.n_lists)) * a.k;
+  const long long total = a.entry_count ? static_cast<long long>(a.entry_count[qi])
+                                        : static_cast<long long>(a.n_lists) * a.k;
   const float* cs = a.cand_score + qi * stride;
   const uint32_t* ci = a.cand_id + qi * stride;
   const int kout = a.k_out;
