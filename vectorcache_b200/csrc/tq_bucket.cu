@@ -845,6 +845,7 @@ __global__ void item_build_kernel(PairArgs a) {
 // Bucket scan
 // ---------------------------------------------------------------------------
 constexpr int kBsWarps = 4;
+constexpr int kBsQueriesPerWarp = 2;  // bucket scan; the multi-index scan keeps 4
 constexpr int kBsPrefetch = 4;
 constexpr int kBsBuf = 512;  // per-warp sort buffer: up to 256 new + 256 kept
 
@@ -906,10 +907,15 @@ struct ItemQueries {
   float floor[kItemQueries];     // scores below it are not kept (-inf: keep all)
 };
 
-// Scans one item with the CTA's 4 warps (2 query quads x 2 tile sets) and
-// writes one sorted candidate list of k per (query, tile set).
-template <bool NIBBLE8>
+// Scans one item with the CTA's 4 warps and writes one candidate list of k per
+// (query, tile set). QW = 4: 2 groups of 4 queries x 2 tile sets (a warp scans
+// every other 256-slot tile set); QW = 2: 4 groups of 2 queries x 1 tile set
+// (a warp scans every tile set: half the registers for accumulators, so more
+// CTAs fit on an SM; the bucket scan takes this form).
+template <bool NIBBLE8, int QW = 4>
 __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& iq, unsigned char* smem) {
+  constexpr int kGroups = kItemQueries / QW;  // query groups per item
+  constexpr int kTsets = kBsWarps / kGroups;  // tile sets scanned side by side
   const int nbg = v.nbg, k = v.k, pc = v.pc;
   const int chunk = nbg < kFlushGroups ? nbg : kFlushGroups;
   const bool resident = chunk >= nbg;
@@ -919,10 +925,10 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   const int kmax = kmax_of(k);
   // Per-warp top-k lists and sort buffer after the LUT area.
   unsigned char* warp_area = smem + static_cast<size_t>(kItemQueries) * chunk * 32 +
-                             warp * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
+                             warp * (static_cast<size_t>(QW) * kmax * 8 + kBsBuf * 8);
   float* list_s = reinterpret_cast<float*>(warp_area);
-  uint32_t* list_i = reinterpret_cast<uint32_t*>(list_s + 4 * kmax);
-  float* buf_s = reinterpret_cast<float*>(list_i + 4 * kmax);
+  uint32_t* list_i = reinterpret_cast<uint32_t*>(list_s + QW * kmax);
+  float* buf_s = reinterpret_cast<float*>(list_i + QW * kmax);
   uint32_t* buf_i = reinterpret_cast<uint32_t*>(buf_s + kBsBuf);
 
   auto load_lut_chunk = [&](int g_first, int g_count) {
@@ -942,17 +948,17 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
     __syncthreads();
   }
 
-  const int quad = warp & 1, tset = warp >> 1;
-  const bool quad_ok = quad * 4 < pc;
+  const int quad = warp % kGroups, tset = warp / kGroups;
+  const bool quad_ok = quad * QW < pc;
   const unsigned long long slot0 = static_cast<unsigned long long>(v.slot0);
   const int size = v.size;
   const int n_sub = (size + kBucketSlotAlign - 1) / kBucketSlotAlign;
   // per-query constants stay in shared memory (iq): fewer live registers
-  float thr_s[4];
-  uint32_t thr_i[4];
-  int cnt[4];
+  float thr_s[QW];
+  uint32_t thr_i[QW];
+  int cnt[QW];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < QW; ++q) {
     thr_s[q] = -FLT_MAX;
     thr_i[q] = 0xffffffffu;
     cnt[q] = 0;
@@ -961,22 +967,22 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   const int k_rank = (k + j_rank - 1) / j_rank;  // rank among the 32 lane values
   constexpr long long kGroupStride = kTileWords / 2;  // uint2 per group row
 
-  const int rounds = (n_sub + 1) / 2;
+  const int rounds = (n_sub + kTsets - 1) / kTsets;
   for (int r = 0; r < rounds; ++r) {
-    const int st = tset + 2 * r;
+    const int st = tset + kTsets * r;
     const bool active = quad_ok && st < n_sub;
     const long long sub = static_cast<long long>(slot0 / kBucketSlotAlign) + st;
     const long long tile = sub >> 1;
     const int half = static_cast<int>(sub & 1);
     const uint2* wp = reinterpret_cast<const uint2*>(v.codes + tile * nbg * kTileWords + half * 64) + lane;
     const long long vbase = sub * kBucketSlotAlign + 8 * lane;
-    float fa[4][8];
-    uint32_t acc[4][8];
+    float fa[QW][8];
+    uint32_t acc[QW][8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < QW; ++q)
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        fa[q][j] = iq.init[quad * 4 + q];
+        fa[q][j] = iq.init[quad * QW + q];
         acc[q][j] = 0u;
       }
     for (int gb = 0; gb < nbg; gb += kFlushGroups) {
@@ -1018,9 +1024,9 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
             tb0h = tb0 >> 16;
             tb1h = tb1 >> 16;
           }
-          const LutHalf* lg = s_lut + (quad * 4) * chunk * 2 + (g + u - chunk_base) * 2;
+          const LutHalf* lg = s_lut + (quad * QW) * chunk * 2 + (g + u - chunk_base) * 2;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
+          for (int q = 0; q < QW; ++q) {
             const LutHalf Fa = lg[q * chunk * 2];
             const LutHalf Sa = lg[q * chunk * 2 + 1];
             const LutHalf Fb = lg[q * chunk * 2 + 2];
@@ -1056,10 +1062,10 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       }
       // f32 flush of this batch (search_avx2.cpp:24-48).
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < QW; ++q)
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          fa[q][j] = __fmaf_rn(iq.scale[quad * 4 + q], __uint2float_rn(acc[q][j]), fa[q][j]);
+          fa[q][j] = __fmaf_rn(iq.scale[quad * QW + q], __uint2float_rn(acc[q][j]), fa[q][j]);
           acc[q][j] = 0u;
         }
     }
@@ -1088,14 +1094,14 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       if (vbase + j - static_cast<long long>(slot0) < size) valid |= 1u << j;
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (quad * 4 + q >= pc) break;  // warp-uniform
+    for (int q = 0; q < QW; ++q) {
+      if (quad * QW + q >= pc) break;  // warp-uniform
       float sc[8];
       unsigned ok = 0;
-      const float fl = iq.floor[quad * 4 + q];
+      const float fl = iq.floor[quad * QW + q];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), iq.off[quad * 4 + q]);
+        sc[j] = __fadd_rn(__fmul_rn(fa[q][j], al[j]), iq.off[quad * QW + q]);
         if ((valid >> j & 1u) && sc[j] > -INFINITY && !(sc[j] < fl)) ok |= 1u << j;
       }
       if (!__any_sync(full_mask(), ok != 0u)) continue;  // nothing at or above the floor
@@ -1209,14 +1215,14 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   if (!quad_ok) return;
   if (v.append_count) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (quad * 4 + q >= pc) break;
+    for (int q = 0; q < QW; ++q) {
+      if (quad * QW + q >= pc) break;
       const int c = cnt[q];
       if (c == 0) continue;  // warp-uniform
       unsigned at = 0;
-      if (lane == 0) at = atomicAdd(v.append_count + iq.q[quad * 4 + q], static_cast<unsigned>(c));
+      if (lane == 0) at = atomicAdd(v.append_count + iq.q[quad * QW + q], static_cast<unsigned>(c));
       at = __shfl_sync(full_mask(), at, 0);
-      const long long base = iq.list[quad * 4 + q] * k + at;
+      const long long base = iq.list[quad * QW + q] * k + at;
       for (int t = lane; t < c; t += kWarp) {
         v.cand_s[base + t] = list_s[q * kmax + t];
         v.cand_i[base + t] = list_i[q * kmax + t];
@@ -1225,9 +1231,9 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
     return;
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    if (quad * 4 + q >= pc) break;
-    const long long list = iq.list[quad * 4 + q] + tset;
+  for (int q = 0; q < QW; ++q) {
+    if (quad * QW + q >= pc) break;
+    const long long list = iq.list[quad * QW + q] + tset;
     float* os = v.cand_s + list * k;
     uint32_t* oi = v.cand_i + list * k;
     for (int t = lane; t < k; t += kWarp) {
@@ -1238,8 +1244,10 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   }
 }
 
+// kBsQueriesPerWarp = 2: 96 registers, 5 CTAs per SM (20 warps; 4 queries per
+// warp held 4 CTAs); measured 8 % faster at 1.2M x 100, n_probe 512.
 template <bool NIBBLE8>
-__global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketScanArgs a) {
+__global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketScanArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ ItemQueries iq;
   if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
@@ -1271,7 +1279,7 @@ __global__ void __launch_bounds__(kBsWarps * 32, 4) bucket_scan_kernel(BucketSca
   const ItemView v{a.codes, a.alpha, a.slot_ids, static_cast<long long>(a.slot_start[b]),
                    static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id,
                    a.append_count};
-  scan_item<NIBBLE8>(v, iq, smem);
+  scan_item<NIBBLE8, kBsQueriesPerWarp>(v, iq, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1579,8 +1587,9 @@ cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStre
   if (a.k < 1 || a.k > kMaxK) return cudaErrorInvalidValue;
   const int chunk = a.nbg < kFlushGroups ? a.nbg : kFlushGroups;
   const int kmax = kmax_of(a.k);
-  const size_t smem = static_cast<size_t>(kItemQueries) * chunk * 32 +
-                      static_cast<size_t>(kBsWarps) * (static_cast<size_t>(4) * kmax * 8 + kBsBuf * 8);
+  const size_t smem =
+      static_cast<size_t>(kItemQueries) * chunk * 32 +
+      static_cast<size_t>(kBsWarps) * (static_cast<size_t>(kBsQueriesPerWarp) * kmax * 8 + kBsBuf * 8);
   cudaError_t e;
   if (a.bits == 3) {
     e = cudaFuncSetAttribute(bucket_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
