@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
     p.add_argument("--rerank", type=int, default=100, help="bucketed: candidates re-ranked exactly (0 = off)")
     p.add_argument("--epochs", type=int, default=30)
+    p.add_argument("--probe-objective", choices=("recall", "classes"), default="recall",
+                   help="learned n_probe: fit each class's recall (trade-off rule) or one label class per query "
+                        "(cumulative-probability rule)")
     p.add_argument("--bucketed-fixed-only", type=int, default=0,
                    help="bucketed: time the plain path at this n_probe only (no sweep, no learned probe)")
     return p.parse_args()
@@ -488,6 +491,42 @@ BUCKETED_METRIC = "QPS at Recall@10 >= 0.95 (bucketed 1.2Mx100 4-bit cosine, lea
 PROBE_CLASSES = (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048)
 FIXED_PROBES = (64, 128, 256, 384, 512, 768, 1024, 1536, 2048)
 RECALL_TARGET = 0.95
+# Prediction-rule sweeps of the learned n_probe, fewest buckets first:
+# trade-offs (recall objective) and coverages (classes objective).
+PROBE_RULES = {"recall": (0.3, 0.2, 0.15, 0.12, 0.1, 0.08, 0.06, 0.04, 0.02),
+               "classes": (0.5, 0.7, 0.8, 0.9, 0.95, 0.98)}
+
+
+def train_probe_mlp(idx, train_q, labels, rec, classes, objective, epochs, device, local, stream=None):
+    """Routes the training queries, standardizes their features and trains the
+    probe MLP on the GPU (batches of 512, Adam lr 2e-3) against label classes
+    or per-class recall targets. Returns (model, mean loss of the last 50 steps)."""
+    import torch
+
+    from vectorcache_b200.probe import ProbeMLP
+
+    mlp = ProbeMLP(classes=classes, hidden=128, layers=2, seed=17, device=local, objective=objective)
+    d_train = torch.from_numpy(train_q).to(device)
+    tr_s = torch.empty((train_q.shape[0], 256), dtype=torch.float32, device=device)
+    tr_i = torch.empty((train_q.shape[0], 256), dtype=torch.int32, device=device)
+    idx.route_device(d_train, 256, tr_s, tr_i, stream=stream)
+    torch.cuda.synchronize()
+    raw = mlp.features(tr_s.cpu().numpy())
+    mlp.set_normalization(raw.mean(axis=0), raw.std(axis=0) + 1e-6)
+    if objective == "recall":
+        d_tgt = torch.from_numpy(np.ascontiguousarray(rec, np.float32)).to(device)
+    else:
+        d_tgt = torch.from_numpy(labels.astype(np.int32)).to(device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(5)
+    losses = []
+    for epoch in range(epochs):
+        perm = torch.randperm(train_q.shape[0], device=device, generator=gen)
+        for s in range(0, train_q.shape[0], 512):
+            sel = perm[s:s + 512]
+            losses.append(mlp.train_step_device(tr_s[sel].contiguous(), d_tgt[sel].contiguous(), sel.numel(), 256,
+                                                2e-3, stream=stream))
+    return mlp, float(np.mean(losses[-50:]))
 
 
 def run_bucketed(args, world, rank, local):
@@ -496,13 +535,15 @@ def run_bucketed(args, world, rank, local):
     max_bucket_size 800, energy_soft 400, expected_n = corpus size. One step =
     one search of 10,000 queries (k = 10). The plain path scans the fixed
     n_probe = 64 best-routed buckets; the learned path routes, runs the probe
-    MLP (trained here on the GPU on labels the plain index generates against
-    exact top-10 for 50,000 training queries) and scans each query's predicted
-    number of buckets. Both re-rank their top `--rerank` candidates exactly."""
+    MLP (trained here on the GPU on the recall at every candidate n_probe that
+    the plain index reaches against exact top-10 for 50,000 training queries,
+    or on label classes with --probe-objective classes) and scans each query's
+    predicted number of buckets. Both re-rank their top `--rerank` candidates
+    exactly."""
     import torch
 
     import vectorcache_b200 as vcb
-    from vectorcache_b200.probe import ProbeMLP, probe_labels, recall_rows
+    from vectorcache_b200.probe import probe_labels, recall_rows
     from vectorcache_b200.synthetic import vmf_mixture
 
     if world > 1:
@@ -580,25 +621,10 @@ def run_bucketed(args, world, rank, local):
     t0 = time.perf_counter()
     labels, rec = probe_labels(lambda q, p: idx.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
     label_s = time.perf_counter() - t0
-    mlp = ProbeMLP(classes=classes, hidden=128, layers=2, seed=17, device=local)
-    d_train = torch.from_numpy(train_q).to(device)
-    tr_s = torch.empty((train_q.shape[0], 256), dtype=torch.float32, device=device)
-    tr_i = torch.empty((train_q.shape[0], 256), dtype=torch.int32, device=device)
-    idx.route_device(d_train, 256, tr_s, tr_i, stream=stream)
-    torch.cuda.synchronize()
-    raw = mlp.features(tr_s.cpu().numpy())
-    mlp.set_normalization(raw.mean(axis=0), raw.std(axis=0) + 1e-6)
-    d_lab = torch.from_numpy(labels.astype(np.int32)).to(device)
-    gen = torch.Generator(device=device)
-    gen.manual_seed(5)
     t0 = time.perf_counter()
-    losses = []
-    for epoch in range(args.epochs):
-        perm = torch.randperm(train_q.shape[0], device=device, generator=gen)
-        for s in range(0, train_q.shape[0], 512):
-            sel = perm[s:s + 512]
-            losses.append(mlp.train_step_device(tr_s[sel].contiguous(), d_lab[sel].contiguous(), sel.numel(), 256,
-                                                2e-3))
+    objective = args.probe_objective
+    mlp, final_loss = train_probe_mlp(idx, train_q, labels, rec, classes, objective, args.epochs, device, local,
+                                      stream)
     train_s = time.perf_counter() - t0
 
     te_s = torch.empty((nq, 256), dtype=torch.float32, device=device)
@@ -606,19 +632,19 @@ def run_bucketed(args, world, rank, local):
     npq = torch.empty(nq, dtype=torch.int32, device=device)
     best = None
     learned_sweep = []
-    for cov in (0.5, 0.7, 0.8, 0.9, 0.95, 0.98):
-        def learned_step(cov=cov):
+    for rule in PROBE_RULES[objective]:
+        def learned_step(rule=rule):
             # one routing pass feeds the network and the probes
-            idx.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=cov, min_confidence=0.0,
+            idx.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, min_confidence=0.0,
                                       fallback_n_probe=p_op, stream=stream)
 
         ms = timed(learned_step)
         r = float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())
         # the per-query probe counts of that search (recomputed outside the timed region)
         idx.route_device(d_q, 256, te_s, te_i, stream=stream)
-        mlp.predict_device(te_s, nq, 256, npq, coverage=cov, min_confidence=0.0, fallback=p_op, stream=stream)
+        mlp.predict_device(te_s, nq, 256, npq, coverage=rule, min_confidence=0.0, fallback=p_op, stream=stream)
         mean_probe = float(npq.float().mean().item())
-        cand = {"coverage": cov, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
+        cand = {"rule": rule, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
                 "mean_n_probe": mean_probe}
         learned_sweep.append(cand)
         if r >= min(RECALL_TARGET, recall_fixed) and (best is None or cand["qps"] > best["qps"]):
@@ -642,7 +668,7 @@ def run_bucketed(args, world, rank, local):
     fixed["kernel_ms"] = kernel_ms(lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, stream=stream))
     if best:
         best["kernel_ms"] = kernel_ms(lambda: idx.search_learned_device(
-            d_q, k, mlp, d_s, d_i, coverage=best["coverage"], min_confidence=0.0, fallback_n_probe=p_op,
+            d_q, k, mlp, d_s, d_i, coverage=best["rule"], min_confidence=0.0, fallback_n_probe=p_op,
             stream=stream))
     line = {
         "metric": BUCKETED_METRIC, "value": best["qps"] if best else None, "unit": "queries/s", "n_gpus": 1,
@@ -653,7 +679,7 @@ def run_bucketed(args, world, rank, local):
                    "n_buckets": info["n_buckets"], "n_slots": info["n_slots"], "build_s": build_s, "gen_s": gen_s,
                    "label_s": label_s, "train_s": train_s, "train_queries": train_q.shape[0],
                    "label_histogram": np.bincount(labels, minlength=len(classes)).tolist(),
-                   "classes": list(classes), "final_loss": float(np.mean(losses[-50:])),
+                   "classes": list(classes), "final_loss": final_loss, "probe_objective": objective,
                    "recall_target": RECALL_TARGET},
         "fixed": fixed, "learned": best, "speedup_vs_fixed": (best["qps"] / qps_fixed) if best else None,
         "fixed_sweep": list(sweep.values()), "learned_sweep": learned_sweep,
@@ -678,7 +704,7 @@ def run_serving(args, world, rank, local):
     import torch
 
     import vectorcache_b200 as vcb
-    from vectorcache_b200.probe import ProbeMLP, probe_labels, recall_rows
+    from vectorcache_b200.probe import probe_labels, recall_rows
     from vectorcache_b200.synthetic import power_law_torch, vmf_mixture
 
     if world > 1:
@@ -727,33 +753,19 @@ def run_serving(args, world, rank, local):
             p_op = p
             break
     classes = tuple(c for c in PROBE_CLASSES if c <= p_op)
-    labels, _ = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
-    mlp = ProbeMLP(classes=classes, hidden=128, layers=2, seed=17, device=local)
-    d_train = torch.from_numpy(train_q).to(device)
-    tr_s = torch.empty((train_q.shape[0], 256), dtype=torch.float32, device=device)
-    tr_i = torch.empty((train_q.shape[0], 256), dtype=torch.int32, device=device)
-    bkt.route_device(d_train, 256, tr_s, tr_i)
-    torch.cuda.synchronize()
-    raw = mlp.features(tr_s.cpu().numpy())
-    mlp.set_normalization(raw.mean(axis=0), raw.std(axis=0) + 1e-6)
-    d_lab = torch.from_numpy(labels.astype(np.int32)).to(device)
-    gen = torch.Generator(device=device)
-    gen.manual_seed(5)
-    for epoch in range(args.epochs):
-        perm = torch.randperm(train_q.shape[0], device=device, generator=gen)
-        for s in range(0, train_q.shape[0], 512):
-            sel = perm[s:s + 512]
-            mlp.train_step_device(tr_s[sel].contiguous(), d_lab[sel].contiguous(), sel.numel(), 256, 2e-3)
-    # learned operating point: the lowest coverage whose Recall@10 reaches the target
-    cov_op = 0.98
+    labels, rec = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
+    objective = args.probe_objective
+    mlp, _ = train_probe_mlp(bkt, train_q, labels, rec, classes, objective, args.epochs, device, local)
+    # learned operating point: the rule with the fewest buckets whose Recall@10 reaches the target
+    cov_op = PROBE_RULES[objective][-1]
     d_q = torch.from_numpy(test_q).to(device)
     d_s = torch.empty((nq, k), dtype=torch.float32, device=device)
     d_i = torch.empty((nq, k), dtype=torch.int64, device=device)
-    for cov in (0.7, 0.8, 0.9, 0.95, 0.98):
-        bkt.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=cov, fallback_n_probe=p_op)
+    for rule in PROBE_RULES[objective]:
+        bkt.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, fallback_n_probe=p_op)
         torch.cuda.synchronize()
         if recall_rows(d_i.cpu().numpy(), ex_test, k).mean() >= RECALL_TARGET:
-            cov_op = cov
+            cov_op = rule
             break
 
     srv = vcb.Server(device=local, hbm_budget_bytes=120 << 30, max_slots=4, max_batch=1024)
@@ -806,7 +818,8 @@ def run_serving(args, world, rank, local):
         "config": {"workload": f"serving: flat {flat_n}x{flat_dim} 3-bit + bucketed {n}x{dim} 4-bit, HBM budget "
                                f"120 GB, rates {list(SERVING_RATES)} q/s", "slots": info["slots"],
                    "slot_bytes": info["slot_bytes"], "resident_bytes": info["resident_bytes"],
-                   "fixed_n_probe": p_op, "learned_coverage": cov_op, "flat_build_s": flat_build_s},
+                   "fixed_n_probe": p_op, "learned_rule": cov_op, "probe_objective": objective,
+                   "flat_build_s": flat_build_s},
         "per_rate": per_rate, "server_stats": srv.stats(),
     }
     print(json.dumps(line), flush=True)

@@ -293,16 +293,31 @@ int tq_bucketed_engine(tq_bucketed* h, tq_index** engine);
  * standardized by tq_probe_mlp_set_normalization), n_layers hidden layers of
  * `hidden` units (ReLU) and one logit per class; class c stands for the
  * n_probe value classes[c] (increasing, <= 2048). Matrix products use bf16
- * weights and activations with fp32 accumulation; training (softmax
- * cross-entropy, Adam) keeps fp32 master weights. Everything runs on the GPU.
- * Prediction: the smallest class whose cumulative probability reaches
- * `coverage`, or `fallback` when the largest class probability is below
- * `min_confidence`. Parameters are flattened as, per layer, W (fan_in x
- * fan_out, row-major) then b (fan_out). */
+ * weights and activations with fp32 accumulation; training (Adam) keeps fp32
+ * master weights. Everything runs on the GPU. Two training objectives:
+ *   TQ_PROBE_OBJECTIVE_CLASSES (default): softmax cross-entropy against one
+ *     label class per query (its smallest sufficient n_probe). Prediction:
+ *     the smallest class whose cumulative probability reaches `coverage`, or
+ *     `fallback` when the largest class probability is below
+ *     `min_confidence`.
+ *   TQ_PROBE_OBJECTIVE_RECALL: one sigmoid per class, binary cross-entropy
+ *     (mean over queries and classes) against the query's measured recall at
+ *     each class (targets in [0, 1]); output r_c estimates the recall at
+ *     classes[c]. Prediction: the class maximizing
+ *     r_c - coverage * classes[c] / classes[last] (the lowest such class on
+ *     ties), i.e. `coverage` carries the trade-off: recall given up to save
+ *     the largest class's whole probe budget; `fallback` when the largest
+ *     r_c is below `min_confidence`. Confidence = the largest r_c.
+ * Parameters are flattened as, per layer, W (fan_in x fan_out, row-major)
+ * then b (fan_out). */
 typedef struct tq_probe_mlp tq_probe_mlp;
+
+enum { TQ_PROBE_OBJECTIVE_CLASSES = 0, TQ_PROBE_OBJECTIVE_RECALL = 1 };
 
 int tq_probe_mlp_create(size_t hidden, size_t n_layers, const uint32_t* classes, size_t n_classes,
                         uint64_t seed, int device, tq_probe_mlp** out);
+/* Chooses the training objective and the prediction rule (before training). */
+int tq_probe_mlp_set_objective(tq_probe_mlp* h, int objective);
 int tq_probe_mlp_destroy(tq_probe_mlp* h);
 int tq_probe_mlp_info(const tq_probe_mlp* h, size_t* n_inputs, size_t* n_params, size_t* n_classes);
 /* Raw (unstandardized) 512 features of m rows of top routing scores (row
@@ -314,13 +329,19 @@ int tq_probe_mlp_set_params(tq_probe_mlp* h, const float* params);
 /* Logits (m x n_classes) of host rows. */
 int tq_probe_mlp_forward(tq_probe_mlp* h, const float* top_scores, size_t m, size_t p, float* logits);
 /* Mean cross-entropy and its gradients (n_params floats) for a host batch,
- * without updating the parameters. */
+ * without updating the parameters (classes objective). */
 int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint32_t* labels, size_t m,
                            size_t p, float* loss, float* grads);
+/* The same for the recall objective: recall is m x n_classes, row-major. */
+int tq_probe_mlp_recall_gradients(tq_probe_mlp* h, const float* top_scores, const float* recall, size_t m,
+                                  size_t p, float* loss, float* grads);
 /* One Adam step (lr; beta1 0.9, beta2 0.999, eps 1e-8) on a device batch,
  * queued on `stream` (NULL: the model's own stream); returns when done. */
 int tq_probe_mlp_train_step_device(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels,
                                    size_t m, size_t p, float lr, float* loss, void* stream);
+/* The same for the recall objective (d_recall: m x n_classes targets in [0, 1]). */
+int tq_probe_mlp_train_step_recall_device(tq_probe_mlp* h, const float* d_top_scores, const float* d_recall,
+                                          size_t m, size_t p, float lr, float* loss, void* stream);
 /* Per-query n_probe (device, m entries) and optionally the confidence. */
 int tq_probe_mlp_predict_device(tq_probe_mlp* h, const float* d_top_scores, size_t m, size_t p,
                                 float coverage, float min_confidence, uint32_t fallback,

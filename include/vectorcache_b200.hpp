@@ -212,8 +212,14 @@ class BucketedTurboQuantIndex {
 class ProbeMLP {
  public:
   ProbeMLP(std::span<const std::uint32_t> classes, std::size_t hidden = 128, std::size_t layers = 2,
-           std::uint64_t seed = 1, int device = 0) {
+           std::uint64_t seed = 1, int device = 0, int objective = TQ_PROBE_OBJECTIVE_CLASSES) {
     throw_on_error(tq_probe_mlp_create(hidden, layers, classes.data(), classes.size(), seed, device, &h_));
+    const int rc = tq_probe_mlp_set_objective(h_, objective);
+    if (rc != TQ_OK) {
+      tq_probe_mlp_destroy(h_);
+      h_ = nullptr;
+      throw_on_error(rc);
+    }
   }
   ~ProbeMLP() {
     if (h_) tq_probe_mlp_destroy(h_);

@@ -4,8 +4,10 @@ The MLP has no counterpart in the reference, so this checker is not pinned to
 reference code: it restates the network's definition (vectorcache_b200
 tq_probe.cu) in float64 numpy with the same bf16 rounding points — inputs,
 weights and hidden activations are rounded to bf16 exactly where the GPU
-rounds them — and computes the mean softmax cross-entropy and its gradients
-by explicit backpropagation. Only tests/ import it.
+rounds them — and computes the mean loss of either training objective
+(softmax cross-entropy on labels, or per-class sigmoid cross-entropy on
+recall targets) and its gradients by explicit backpropagation. Also the
+prediction rules. Only tests/ import it.
 """
 from __future__ import annotations
 
@@ -39,9 +41,12 @@ def inputs(raw: np.ndarray, mean: np.ndarray, std: np.ndarray) -> np.ndarray:
 
 
 def forward_backward(x: np.ndarray, params: np.ndarray, shapes, labels: np.ndarray, rounding: bool = True):
-    """x: bf16-valued inputs (m x 512). Returns (loss, grads float64, logits).
-    rounding=False drops the bf16 rounding (float64 throughout) for
-    finite-difference checks of the backpropagation itself."""
+    """x: bf16-valued inputs (m x 512). labels: m label classes (softmax
+    cross-entropy) or an m x n_classes matrix of recall targets in [0, 1]
+    (per-class sigmoid binary cross-entropy, mean over all entries). Returns
+    (loss, grads float64, logits). rounding=False drops the bf16 rounding
+    (float64 throughout) for finite-difference checks of the
+    backpropagation itself."""
     rnd = bf16 if rounding else (lambda a: np.asarray(a, np.float64))
     layers = unpack(params if not rounding else params.astype(np.float32), shapes)
     m = x.shape[0]
@@ -55,13 +60,22 @@ def forward_backward(x: np.ndarray, params: np.ndarray, shapes, labels: np.ndarr
             h = rnd(np.maximum(z, 0.0).astype(np.float32) if rounding else np.maximum(z, 0.0)).astype(np.float64)
             acts.append(h)
     logits = zs[-1]
-    mx = logits.max(axis=1, keepdims=True)
-    e = np.exp(logits - mx)
-    p = e / e.sum(axis=1, keepdims=True)
-    loss = float(np.mean(np.log(e.sum(axis=1)) - (logits[np.arange(m), labels] - mx[:, 0])))
-    dz = p.copy()
-    dz[np.arange(m), labels] -= 1.0
-    dz /= m
+    labels = np.asarray(labels)
+    if labels.ndim == 2:
+        # recall objective: per-class sigmoid, binary cross-entropy against
+        # soft targets, mean over queries and classes
+        t = labels.astype(np.float64)
+        n_cls = logits.shape[1]
+        loss = float(np.mean(np.maximum(logits, 0.0) - t * logits + np.log1p(np.exp(-np.abs(logits)))))
+        dz = (1.0 / (1.0 + np.exp(-logits)) - t) / (m * n_cls)
+    else:
+        mx = logits.max(axis=1, keepdims=True)
+        e = np.exp(logits - mx)
+        p = e / e.sum(axis=1, keepdims=True)
+        loss = float(np.mean(np.log(e.sum(axis=1)) - (logits[np.arange(m), labels] - mx[:, 0])))
+        dz = p.copy()
+        dz[np.arange(m), labels] -= 1.0
+        dz /= m
     grads = []
     for li in range(len(layers) - 1, -1, -1):
         w, _ = layers[li]
@@ -74,3 +88,28 @@ def forward_backward(x: np.ndarray, params: np.ndarray, shapes, labels: np.ndarr
     grads.reverse()
     flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads])
     return loss, flat, logits
+
+
+def predict(logits: np.ndarray, classes, objective: str, coverage: float, min_confidence: float, fallback: int):
+    """The prediction rules on logits (float64). Returns (n_probe per row, the
+    margin of the chosen class over the runner-up: rows with a tiny margin may
+    legitimately pick differently in fp32)."""
+    z = np.asarray(logits, np.float64)
+    cls = np.asarray(classes, np.float64)
+    if objective == "recall":
+        r = 1.0 / (1.0 + np.exp(-z))
+        v = r - coverage * cls[None, :] / cls[-1]
+        pick = np.argmax(v, axis=1)
+        srt = np.sort(v, axis=1)
+        margin = srt[:, -1] - srt[:, -2]
+        conf = r.max(axis=1)
+    else:
+        e = np.exp(z - z.max(axis=1, keepdims=True))
+        p = e / e.sum(axis=1, keepdims=True)
+        c = np.cumsum(p, axis=1)
+        reach = c >= coverage
+        pick = np.where(reach.any(axis=1), reach.argmax(axis=1), z.shape[1] - 1)
+        margin = np.min(np.abs(c - coverage), axis=1)
+        conf = p.max(axis=1)
+    out = np.where(conf < min_confidence, fallback, cls[pick].astype(np.int64))
+    return out, margin

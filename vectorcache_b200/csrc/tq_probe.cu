@@ -10,10 +10,17 @@
 // accumulation; the optimizer (Adam) keeps fp32 master weights and rewrites the
 // bf16 copies after each step. Biases, pre-activations and gradients are fp32.
 //
-// Prediction: softmax over the classes (ascending n_probe); the query gets the
-// smallest n_probe whose cumulative probability reaches `coverage`, or the
-// fixed fallback n_probe when the largest class probability is below
-// `min_confidence`.
+// Classes objective (softmax cross-entropy on one label class per query):
+// the query gets the smallest n_probe whose cumulative probability reaches
+// `coverage`, or the fixed fallback n_probe when the largest class
+// probability is below `min_confidence`.
+//
+// Recall objective (one sigmoid per class, binary cross-entropy against the
+// query's measured recall at every class): r_c estimates the recall at
+// classes[c], and the query gets the class maximizing
+// r_c - lambda * classes[c] / classes[last] with lambda passed as `coverage`.
+// One lambda for all queries spends probes where the predicted recall gain
+// per probe is largest, instead of asking every query for the same recall.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -162,6 +169,26 @@ __global__ void softmax_xent_kernel(const float* __restrict__ Z, long long M, in
   loss_rows[q] = __fsub_rn(logf(sum), __fsub_rn(z[y], mx));
 }
 
+// Row-wise sigmoid binary cross-entropy against soft targets t in [0, 1]:
+// loss_rows[q] = mean_j (max(z, 0) - t z + log(1 + exp(-|z|))),
+// dZ = (sigmoid(z) - t) / (M N).
+__global__ void sigmoid_bce_kernel(const float* __restrict__ Z, long long M, int N, const float* __restrict__ T,
+                                   float* __restrict__ dZ, float* __restrict__ loss_rows) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  const float inv = 1.f / (static_cast<float>(M) * static_cast<float>(N));
+  float row = 0.f;
+  for (int j = 0; j < N; ++j) {
+    const float z = Z[q * N + j], t = T[q * N + j];
+    const float e = expf(-fabsf(z));
+    row = __fadd_rn(row, __fadd_rn(__fsub_rn(fmaxf(z, 0.f), __fmul_rn(t, z)), log1pf(e)));
+    // sigmoid(z) from e = exp(-|z|) without overflow
+    const float sg = z >= 0.f ? __fdiv_rn(1.f, __fadd_rn(1.f, e)) : __fdiv_rn(e, __fadd_rn(1.f, e));
+    dZ[q * N + j] = __fmul_rn(__fsub_rn(sg, t), inv);
+  }
+  loss_rows[q] = __fdiv_rn(row, static_cast<float>(N));
+}
+
 // dZ *= (Zprev > 0)
 __global__ void relu_grad_kernel(float* __restrict__ dA, const float* __restrict__ Z, long long total) {
   const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -200,11 +227,28 @@ __global__ void to_bf16_kernel(const float* __restrict__ src, bf16* __restrict__
 
 // Logits -> n_probe per query (see the file comment).
 __global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, const uint32_t* __restrict__ classes,
-                               float coverage, float min_conf, uint32_t fallback, uint32_t* __restrict__ out,
-                               float* __restrict__ conf_out) {
+                               int objective, float coverage, float min_conf, uint32_t fallback,
+                               uint32_t* __restrict__ out, float* __restrict__ conf_out) {
   const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (q >= M) return;
   const float* z = Z + q * N;
+  if (objective == TQ_PROBE_OBJECTIVE_RECALL) {
+    const float per_probe = coverage / static_cast<float>(classes[N - 1]);
+    float best = -INFINITY, top_r = 0.f;
+    int pick = N - 1;
+    for (int j = 0; j < N; ++j) {
+      const float r = 1.f / (1.f + expf(-z[j]));
+      const float v = r - per_probe * static_cast<float>(classes[j]);
+      if (v > best) {
+        best = v;
+        pick = j;
+      }
+      top_r = fmaxf(top_r, r);
+    }
+    out[q] = top_r < min_conf ? fallback : classes[pick];
+    if (conf_out) conf_out[q] = top_r;
+    return;
+  }
   float mx = -INFINITY;
   for (int j = 0; j < N; ++j) mx = fmaxf(mx, z[j]);
   float sum = 0.f;
@@ -251,6 +295,7 @@ struct tq_probe_mlp {
   int device = 0;
   cudaStream_t stream = nullptr;
   int hidden = 128, n_layers = 2, n_classes = 0;
+  int objective = TQ_PROBE_OBJECTIVE_CLASSES;
   std::vector<uint32_t> classes;
   std::vector<int> fan_in, fan_out;  // per linear layer
   std::vector<size_t> w_off, b_off;  // offsets into the flat fp32 parameter vector
@@ -260,7 +305,7 @@ struct tq_probe_mlp {
   size_t n_wbf = 0;
   int64_t step = 0;
   // scratch
-  vcb::DeviceBuffer d_x, d_raw, d_top, d_labels, d_loss, d_out;
+  vcb::DeviceBuffer d_x, d_raw, d_top, d_labels, d_targets, d_loss, d_out;
   vcb::DeviceBuffer z[5], a[5], dz[5];  // per linear layer (n_layers <= 4)
 
   ~tq_probe_mlp() {
@@ -306,13 +351,19 @@ struct tq_probe_mlp {
     }
   }
 
-  // Gradients of the mean cross-entropy into d_grad; returns the loss.
-  float backward(const uint32_t* d_lab, size_t m, cudaStream_t s) {
+  // Gradients of the mean loss into d_grad; returns the loss. Labels (classes
+  // objective) or recall targets (recall objective), by the model's objective.
+  float backward(const uint32_t* d_lab, const float* d_tgt, size_t m, cudaStream_t s) {
     const long long M = static_cast<long long>(m);
     const int L = n_lin();
-    vcb::softmax_xent_kernel<<<vcb::blocks(M), 256, 0, s>>>(z[L - 1].as<float>(), M, n_classes, d_lab,
-                                                             dz[L - 1].as<float>(), d_loss.as<float>());
-    vcb::check(cudaGetLastError(), "softmax kernel");
+    if (objective == TQ_PROBE_OBJECTIVE_RECALL) {
+      vcb::sigmoid_bce_kernel<<<vcb::blocks(M), 256, 0, s>>>(z[L - 1].as<float>(), M, n_classes, d_tgt,
+                                                              dz[L - 1].as<float>(), d_loss.as<float>());
+    } else {
+      vcb::softmax_xent_kernel<<<vcb::blocks(M), 256, 0, s>>>(z[L - 1].as<float>(), M, n_classes, d_lab,
+                                                               dz[L - 1].as<float>(), d_loss.as<float>());
+    }
+    vcb::check(cudaGetLastError(), "loss kernel");
     float* g = d_grad.as<float>();
     for (int l = L - 1; l >= 0; --l) {
       const int K = fan_in[l], N = fan_out[l];
@@ -396,8 +447,8 @@ void probe_predict(tq_probe_mlp* h, const float* d_top, size_t m, int p, float c
     check(cudaGetLastError(), "bias kernel");
     in = out;
   }
-  predict_kernel<<<blocks(M), 256, 0, s>>>(sc.z.as<float>(), M, h->n_classes, h->d_classes.as<uint32_t>(), coverage,
-                                           min_conf, fallback, d_out, nullptr);
+  predict_kernel<<<blocks(M), 256, 0, s>>>(sc.z.as<float>(), M, h->n_classes, h->d_classes.as<uint32_t>(),
+                                           h->objective, coverage, min_conf, fallback, d_out, nullptr);
   check(cudaGetLastError(), "predict kernel");
 }
 
@@ -482,6 +533,15 @@ int tq_probe_mlp_create(size_t hidden, size_t n_layers, const uint32_t* classes,
     h->refresh_bf16(h->stream);
     h->sync();
     *out = h.release();
+  });
+}
+
+int tq_probe_mlp_set_objective(tq_probe_mlp* h, int objective) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(objective == TQ_PROBE_OBJECTIVE_CLASSES || objective == TQ_PROBE_OBJECTIVE_RECALL,
+            TQ_ERR_INVALID_ARGUMENT, "unknown objective");
+    h->objective = objective;
   });
 }
 
@@ -582,6 +642,7 @@ int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint3
     require(top_scores && labels && grads, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
     require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
+    require(h->objective == TQ_PROBE_OBJECTIVE_CLASSES, TQ_ERR_STATE, "model has the recall objective");
     for (size_t i = 0; i < m; ++i) {
       require(labels[i] < static_cast<uint32_t>(h->n_classes), TQ_ERR_INVALID_ARGUMENT, "label out of range");
     }
@@ -591,30 +652,77 @@ int tq_probe_mlp_gradients(tq_probe_mlp* h, const float* top_scores, const uint3
     vcb::check(cudaMemcpyAsync(h->d_top.get(), top_scores, m * p * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
     vcb::check(cudaMemcpyAsync(h->d_labels.get(), labels, m * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
     h->forward(h->d_top.as<float>(), m, static_cast<int>(p), h->stream);
-    const float l = h->backward(h->d_labels.as<uint32_t>(), m, h->stream);
+    const float l = h->backward(h->d_labels.as<uint32_t>(), nullptr, m, h->stream);
     if (loss) *loss = l;
     vcb::check(cudaMemcpyAsync(grads, h->d_grad.get(), h->n_params * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
     h->sync();
   });
 }
 
+int tq_probe_mlp_recall_gradients(tq_probe_mlp* h, const float* top_scores, const float* recall, size_t m, size_t p,
+                                  float* loss, float* grads) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(top_scores && recall && grads, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+    require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
+    require(h->objective == TQ_PROBE_OBJECTIVE_RECALL, TQ_ERR_STATE, "model has the classes objective");
+    const size_t nt = m * static_cast<size_t>(h->n_classes);
+    for (size_t i = 0; i < nt; ++i) {
+      require(recall[i] >= 0.f && recall[i] <= 1.f, TQ_ERR_INVALID_ARGUMENT, "recall targets must be in [0, 1]");
+    }
+    vcb::DeviceGuard g(h->device);
+    h->d_top.reserve(m * p * 4);
+    h->d_targets.reserve(nt * 4);
+    vcb::check(cudaMemcpyAsync(h->d_top.get(), top_scores, m * p * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    vcb::check(cudaMemcpyAsync(h->d_targets.get(), recall, nt * 4, cudaMemcpyHostToDevice, h->stream), "H2D");
+    h->forward(h->d_top.as<float>(), m, static_cast<int>(p), h->stream);
+    const float l = h->backward(nullptr, h->d_targets.as<float>(), m, h->stream);
+    if (loss) *loss = l;
+    vcb::check(cudaMemcpyAsync(grads, h->d_grad.get(), h->n_params * 4, cudaMemcpyDeviceToHost, h->stream), "D2H");
+    h->sync();
+  });
+}
+
+namespace {
+
+// One Adam step on a device batch: labels or recall targets, by objective.
+void train_step(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels, const float* d_recall, size_t m,
+                size_t p, float lr, float* loss, void* stream) {
+  require(d_top_scores && (d_labels || d_recall), TQ_ERR_INVALID_ARGUMENT, "null buffer");
+  require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
+  require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
+  vcb::DeviceGuard g(h->device);
+  // On the caller's stream (where the batch was produced); the step ends
+  // with the loss read back, so it returns with its work complete.
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  if (s != h->stream) h->sync();
+  h->forward(d_top_scores, m, static_cast<int>(p), s);
+  const float l = h->backward(d_labels, d_recall, m, s);
+  h->adam(lr, s);
+  vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  if (loss) *loss = l;
+}
+
+}  // namespace
+
 int tq_probe_mlp_train_step_device(tq_probe_mlp* h, const float* d_top_scores, const uint32_t* d_labels, size_t m,
                                    size_t p, float lr, float* loss, void* stream) {
   return vcb::guarded([&] {
     checked(h);
-    require(d_top_scores && d_labels, TQ_ERR_INVALID_ARGUMENT, "null buffer");
-    require(p >= 1 && p <= 256, TQ_ERR_INVALID_ARGUMENT, "p must be in [1, 256]");
-    require(m >= 1, TQ_ERR_INVALID_ARGUMENT, "empty batch");
-    vcb::DeviceGuard g(h->device);
-    // On the caller's stream (where the batch was produced); the step ends
-    // with the loss read back, so it returns with its work complete.
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-    if (s != h->stream) h->sync();
-    h->forward(d_top_scores, m, static_cast<int>(p), s);
-    const float l = h->backward(d_labels, m, s);
-    h->adam(lr, s);
-    vcb::check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-    if (loss) *loss = l;
+    require(h->objective == TQ_PROBE_OBJECTIVE_CLASSES, TQ_ERR_STATE, "model has the recall objective");
+    require(d_labels != nullptr, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    train_step(h, d_top_scores, d_labels, nullptr, m, p, lr, loss, stream);
+  });
+}
+
+int tq_probe_mlp_train_step_recall_device(tq_probe_mlp* h, const float* d_top_scores, const float* d_recall, size_t m,
+                                          size_t p, float lr, float* loss, void* stream) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(h->objective == TQ_PROBE_OBJECTIVE_RECALL, TQ_ERR_STATE, "model has the classes objective");
+    require(d_recall != nullptr, TQ_ERR_INVALID_ARGUMENT, "null buffer");
+    train_step(h, d_top_scores, nullptr, d_recall, m, p, lr, loss, stream);
   });
 }
 
@@ -633,7 +741,7 @@ int tq_probe_mlp_predict_device(tq_probe_mlp* h, const float* d_top_scores, size
     h->forward(d_top_scores, m, static_cast<int>(p), s);
     vcb::predict_kernel<<<vcb::blocks(static_cast<long long>(m)), 256, 0, s>>>(
         h->z[h->n_lin() - 1].as<float>(), static_cast<long long>(m), h->n_classes, h->d_classes.as<uint32_t>(),
-        coverage, min_confidence, fallback, d_n_probe, d_confidence);
+        h->objective, coverage, min_confidence, fallback, d_n_probe, d_confidence);
     vcb::check(cudaGetLastError(), "predict kernel");
   });
 }

@@ -4,15 +4,23 @@ reference).
 A query's top-256 routing scores and their gaps go through a small MLP
 (2 hidden layers of 128, BF16 weights, FP32 accumulation) trained and run on
 the GPU by libvectorcache_b200.so (tq_probe_mlp_* in include/vectorcache_b200.h).
-The classes are candidate n_probe values; a query is searched with the
-smallest n_probe whose predicted cumulative probability reaches `coverage`,
-or with the fixed fallback n_probe when the model's confidence is low.
+The classes are candidate n_probe values. Two training objectives:
 
-Labels come from the plain index itself: for every training query, the
-smallest candidate n_probe whose (optionally re-ranked) top-k reaches the
-query's target recall against the exact brute-force top-k — the recall the
-index reaches at the largest candidate n_probe, capped at `target` — see
-`probe_labels`.
+* "classes": softmax cross-entropy on one label per query; a query is
+  searched with the smallest n_probe whose predicted cumulative probability
+  reaches `coverage`, or with the fixed fallback n_probe when the model's
+  confidence is low.
+* "recall": one sigmoid per class fitted to the query's measured recall at
+  that class; a query is searched with the class maximizing
+  predicted recall - coverage * n_probe / largest class, so `coverage` is a
+  trade-off (recall given up to save the largest class's probe budget) and
+  one value for all queries spends probes where the predicted gain per probe
+  is largest.
+
+Labels and recall targets come from the plain index itself (`probe_labels`):
+for every training query its recall against the exact brute-force top-k at
+each candidate n_probe, and the smallest candidate n_probe whose (optionally
+re-ranked) top-k reaches the recall the index gets at the reference n_probe.
 """
 from __future__ import annotations
 
@@ -28,6 +36,7 @@ _P = C.c_void_p
 DEFAULT_CLASSES = (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256)
 N_INPUTS = 512
 ROUTE_P = 256
+OBJECTIVES = {"classes": 0, "recall": 1}  # TQ_PROBE_OBJECTIVE_CLASSES / _RECALL
 
 
 def _declare_probe(lib):
@@ -44,6 +53,10 @@ def _declare_probe(lib):
         "tq_probe_mlp_forward": (C.c_int, [_P, _P, _SZ, _SZ, _P]),
         "tq_probe_mlp_gradients": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.POINTER(C.c_float), _P]),
         "tq_probe_mlp_train_step_device": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.c_float, C.POINTER(C.c_float), _P]),
+        "tq_probe_mlp_set_objective": (C.c_int, [_P, C.c_int]),
+        "tq_probe_mlp_recall_gradients": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.POINTER(C.c_float), _P]),
+        "tq_probe_mlp_train_step_recall_device": (C.c_int, [_P, _P, _P, _SZ, _SZ, C.c_float,
+                                                            C.POINTER(C.c_float), _P]),
         "tq_probe_mlp_predict_device": (C.c_int, [_P, _P, _SZ, _SZ, C.c_float, C.c_float, C.c_uint32, _P, _P, _P]),
         "tq_probe_mlp_synchronize": (C.c_int, [_P]),
     }
@@ -58,14 +71,19 @@ def _declare_probe(lib):
 class ProbeMLP:
     """The MLP itself: parameters live on the device (fp32 master + bf16 copy)."""
 
-    def __init__(self, classes=DEFAULT_CLASSES, hidden: int = 128, layers: int = 2, seed: int = 1, device: int = 0):
+    def __init__(self, classes=DEFAULT_CLASSES, hidden: int = 128, layers: int = 2, seed: int = 1, device: int = 0,
+                 objective: str = "classes"):
+        if objective not in OBJECTIVES:
+            raise ValueError(f"objective must be one of {sorted(OBJECTIVES)}")
         self._lib = _declare_probe(load_library())
         self.classes = np.ascontiguousarray(classes, np.uint32)
         self.hidden, self.layers, self.device = int(hidden), int(layers), int(device)
+        self.objective = objective
         h = _P()
         _check(self._lib.tq_probe_mlp_create(hidden, layers, _ptr(self.classes), len(self.classes), seed, device,
                                              C.byref(h)))
         self._h = h
+        _check(self._lib.tq_probe_mlp_set_objective(h, OBJECTIVES[objective]))
         ni, npar, nc = _SZ(), _SZ(), _SZ()
         _check(self._lib.tq_probe_mlp_info(h, C.byref(ni), C.byref(npar), C.byref(nc)))
         self.n_inputs, self.n_params, self.n_classes = ni.value, npar.value, nc.value
@@ -115,23 +133,39 @@ class ProbeMLP:
         _check(self._lib.tq_probe_mlp_forward(self._h, _ptr(t), t.shape[0], t.shape[1], _ptr(out)))
         return out
 
-    def gradients(self, top_scores, labels) -> tuple[float, np.ndarray]:
+    def gradients(self, top_scores, targets) -> tuple[float, np.ndarray]:
+        """Mean loss and gradients for a host batch: targets are label
+        classes (classes objective) or an m x n_classes recall matrix (recall
+        objective)."""
         t = np.ascontiguousarray(top_scores, np.float32)
-        lab = np.ascontiguousarray(labels, np.uint32)
         g = np.empty(self.n_params, np.float32)
         loss = C.c_float()
-        _check(self._lib.tq_probe_mlp_gradients(self._h, _ptr(t), _ptr(lab), t.shape[0], t.shape[1],
-                                                C.byref(loss), _ptr(g)))
+        if self.objective == "recall":
+            r = np.ascontiguousarray(targets, np.float32)
+            if r.shape != (t.shape[0], self.n_classes):
+                raise ValueError("recall targets must be m x n_classes")
+            _check(self._lib.tq_probe_mlp_recall_gradients(self._h, _ptr(t), _ptr(r), t.shape[0], t.shape[1],
+                                                           C.byref(loss), _ptr(g)))
+        else:
+            lab = np.ascontiguousarray(targets, np.uint32)
+            _check(self._lib.tq_probe_mlp_gradients(self._h, _ptr(t), _ptr(lab), t.shape[0], t.shape[1],
+                                                    C.byref(loss), _ptr(g)))
         return loss.value, g
 
-    def train_step_device(self, d_top, d_labels, m: int, p: int, lr: float, stream=None) -> float:
+    def train_step_device(self, d_top, d_targets, m: int, p: int, lr: float, stream=None) -> float:
+        """One Adam step on device rows: d_targets are int32 labels (classes
+        objective) or an m x n_classes float32 recall matrix (recall objective)."""
         loss = C.c_float()
-        _check(self._lib.tq_probe_mlp_train_step_device(self._h, _dev(d_top)[0], _dev(d_labels)[0], m, p, lr,
-                                                        C.byref(loss), _stream_ptr(stream)))
+        fn = (self._lib.tq_probe_mlp_train_step_recall_device if self.objective == "recall"
+              else self._lib.tq_probe_mlp_train_step_device)
+        _check(fn(self._h, _dev(d_top)[0], _dev(d_targets)[0], m, p, lr, C.byref(loss), _stream_ptr(stream)))
         return loss.value
 
     def predict_device(self, d_top, m: int, p: int, d_out, coverage: float = 0.9, min_confidence: float = 0.0,
                        fallback: int = 64, d_confidence=None, stream=None) -> None:
+        """Per-query n_probe into d_out (m int32). `coverage` is the cumulative
+        probability (classes objective) or the recall trade-off (recall
+        objective)."""
         conf = None if d_confidence is None else _dev(d_confidence)[0]
         _check(self._lib.tq_probe_mlp_predict_device(self._h, _dev(d_top)[0], m, p, coverage, min_confidence,
                                                      fallback, _dev(d_out)[0], conf, _stream_ptr(stream)))
