@@ -790,7 +790,18 @@ __device__ __forceinline__ int probes_of(const PairArgs& a, long long q) {
 
 // Probe position j of query q gets a pair in this build.
 __device__ __forceinline__ bool pair_in_range(const PairArgs& a, long long q, int j) {
-  return j >= a.probe_begin && j < a.probe_end && j < probes_of(a, q);
+  const int np = probes_of(a, q);
+  int lo = a.probe_begin, hi = a.probe_end;
+  if (a.first_split) {
+    int f = np >= kFloorWideFrom ? kFloorProbesWide : kFloorProbes;
+    f = f < np ? f : np;
+    if (a.first_split == 1) {
+      hi = hi < f ? hi : f;
+    } else {
+      lo = lo > f ? lo : f;
+    }
+  }
+  return j >= lo && j < hi && j < np;
 }
 
 __global__ void pair_count_kernel(PairArgs a) {
@@ -846,6 +857,8 @@ __global__ void item_build_kernel(PairArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kBsWarps = 4;
 constexpr int kBsQueriesPerWarp = 2;  // bucket scan; the multi-index scan keeps 4
+static_assert(kBsWarps / (kItemQueries / kBsQueriesPerWarp) == kBsListsPerProbe,
+              "bucket-scan tile sets per item must match the candidate lists per probe");
 constexpr int kBsPrefetch = 4;
 constexpr int kBsBuf = 512;  // per-warp sort buffer: up to 256 new + 256 kept
 
@@ -1244,14 +1257,10 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
   }
 }
 
-// kBsQueriesPerWarp = 2: 96 registers, 5 CTAs per SM (20 warps; 4 queries per
-// warp held 4 CTAs); measured 8 % faster at 1.2M x 100, n_probe 512.
+// One work item (a bucket and up to kItemQueries of its probing queries).
 template <bool NIBBLE8>
-__global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketScanArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ ItemQueries iq;
-  if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
-  const uint4 it = a.items[blockIdx.x];
+__device__ __forceinline__ void bucket_scan_item(const BucketScanArgs& a, const uint4 it, ItemQueries& iq,
+                                                 unsigned char* smem) {
   const int b = static_cast<int>(it.x);
   const int pc = static_cast<int>(it.z);
   if (threadIdx.x < kItemQueries) {
@@ -1261,7 +1270,8 @@ __global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketSca
       const int q = static_cast<int>(pr / static_cast<uint32_t>(a.max_probe));
       iq.q[t] = q;
       // (query, probe) lists, or the query's region when appending
-      iq.list[t] = a.append_count ? static_cast<long long>(q) * a.max_probe * 2 : static_cast<long long>(pr) * 2;
+      iq.list[t] = (a.append_count ? static_cast<long long>(q) * a.max_probe : static_cast<long long>(pr)) *
+                   kBsListsPerProbe;
       iq.scale[t] = a.lut_scale[q];
       iq.init[t] = a.fa_init[q];
       iq.off[t] = a.offsets[pr];
@@ -1280,6 +1290,19 @@ __global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketSca
                    static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id,
                    a.append_count};
   scan_item<NIBBLE8, kBsQueriesPerWarp>(v, iq, smem);
+}
+
+// kBsQueriesPerWarp = 2: 96 registers, 5 CTAs per SM (20 warps; 4 queries per
+// warp held 4 CTAs); measured 8 % faster at 1.2M x 100, n_probe 512. One item
+// per CTA over the host's item bound (CTAs past the real count exit at once):
+// a grid of 4 resident waves looping over the items measured 9 % slower, the
+// block scheduler balances uneven items better than a fixed stride.
+template <bool NIBBLE8>
+__global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketScanArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ ItemQueries iq;
+  if (static_cast<unsigned long long>(blockIdx.x) >= *a.n_items) return;
+  bucket_scan_item<NIBBLE8>(a, a.items[blockIdx.x], iq, smem);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,6 +20,9 @@ namespace vcb {
 constexpr int kBucketSlotAlign = 256;
 // Queries per bucket-scan work item (two groups of four, one per warp pair).
 constexpr int kItemQueries = 8;
+// Candidate lists per (query, probe) of the bucket scan: one per tile set
+// scanned side by side within an item (one with 2 queries per warp).
+constexpr int kBsListsPerProbe = 1;
 // Fixed-point scale of the deterministic centroid sums (|x| <= 1 per coordinate).
 constexpr double kFixedScale = 4294967296.0;  // 2^32
 
@@ -131,6 +134,10 @@ struct PairArgs {
   // search scans its first probes before the rest).
   int probe_begin = 0;
   int probe_end = 1 << 30;
+  // 1: also end at the query's own first-probe count, 2: begin there. That
+  // count follows the query's n_probe: kFloorProbesWide from kFloorWideFrom
+  // probes, else kFloorProbes (at most its n_probe).
+  int first_split = 0;
 };
 // Groups the (query, probe) pairs by bucket and builds the scan work items.
 cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);
@@ -150,15 +157,15 @@ struct BucketScanArgs {
   const uint4* items;
   const unsigned long long* n_items;
   int nbg, bits, k, max_probe;
-  float* cand_score;         // (nq * max_probe * 2) lists of k
+  float* cand_score;         // (nq * max_probe * kBsListsPerProbe) lists of k
   uint32_t* cand_id;
   // Optional per query: scores below floor[q] cannot reach the query's top k
   // and are not kept (nullptr: no floor).
   const float* floor = nullptr;
   // Optional per query (zeroed by the caller): the kept candidates of query q
-  // are appended, unpadded, to its region of 2 * max_probe * k entries at
-  // cand_score/cand_id + q * 2 * max_probe * k, and append_count[q] counts
-  // them. nullptr: one -inf padded list of k per (query, probe, tile set).
+  // are appended, unpadded, to its region of L = max_probe * kBsListsPerProbe
+  // lists of k entries at cand_score/cand_id + q * L * k, and append_count[q]
+  // counts them. nullptr: one -inf padded list of k per (query, probe, tile set).
   uint32_t* append_count = nullptr;
 };
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);

@@ -384,11 +384,15 @@ struct tq_bucketed {
   }
 
   // Queries per pass: routing scores (nb floats per query) within 256 MiB and
-  // candidate lists (2 * max_probe lists of kscan (score, id) per query)
-  // within 1 GiB.
+  // candidate lists (max_probe lists of kscan (score, id) per query) within
+  // 4 GiB — 10,485 queries at 512 probes and a re-rank of 100. Every pass
+  // repeats the routing, pair and floor launches on a smaller grid: at 1 GiB
+  // with two lists per probe the same search ran in 8 passes and took 1.7x
+  // as long for 64 probes per query under a 512-probe cap.
   size_t pass_queries(size_t max_probe = 1, size_t kscan = 1) const {
     const size_t by_route = std::max<size_t>(1, (size_t{256} << 20) / (static_cast<size_t>(nb) * 4));
-    const size_t by_cand = std::max<size_t>(1, (size_t{1} << 30) / (max_probe * 2 * kscan * 8));
+    const size_t by_cand =
+        std::max<size_t>(1, (size_t{4} << 30) / (max_probe * vcb::kBsListsPerProbe * kscan * 8));
     return std::min<size_t>({16384, by_route, by_cand});
   }
 
@@ -466,7 +470,7 @@ struct tq_bucketed {
       });
       pa.enc_scores = sc.encs.as<float>();
       pa.enc_ld = nb;
-      const size_t lists = m * max_probe * 2;
+      const size_t lists = m * max_probe * vcb::kBsListsPerProbe;
       sc.cand_s.reserve(lists * kscan * 4);
       sc.cand_i.reserve(lists * kscan * 4);
       sc.floor.reserve(m * 4);
@@ -499,10 +503,12 @@ struct tq_bucketed {
       // first 8 (32 from 256 probes) probes is a lower bound of its k-th best over all
       // probes, so the scan of the remaining probes keeps only scores at or
       // above it (few insertions, few candidates for the merge). The kept top
-      // k is the same.
+      // k is the same. The first-probe count follows each query's own n_probe
+      // (per-query counts: a query with 64 probes spends 8 of them without
+      // the full floor, as a fixed n_probe of 64 does, not 32).
       const int first =
           std::min(max_probe >= vcb::kFloorWideFrom ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
-      const bool two_phase = max_probe > first;
+      const bool two_phase = max_probe > vcb::kFloorProbes;
       if (two_phase) {
         sc.fl_s.reserve(m * kscan * 4);
         sc.fl_i.reserve(m * kscan * 8);
@@ -510,8 +516,8 @@ struct tq_bucketed {
         fm.cand_score = ba.cand_score;
         fm.cand_id = ba.cand_id;
         fm.nq = static_cast<long long>(m);
-        fm.n_lists = 2 * first;
-        fm.list_stride = 2 * max_probe;
+        fm.n_lists = first * vcb::kBsListsPerProbe;
+        fm.list_stride = max_probe * vcb::kBsListsPerProbe;
         fm.k = static_cast<int>(kscan);
         fm.k_out = static_cast<int>(kscan);
         fm.out_score = sc.fl_s.as<float>();
@@ -525,7 +531,8 @@ struct tq_bucketed {
         const int steps[3] = {0, 1, first};
         for (int st = 0; st < 2; ++st) {
           pa.probe_begin = steps[st];
-          pa.probe_end = steps[st + 1];
+          pa.probe_end = st == 0 ? 1 : max_probe;
+          pa.first_split = st == 0 ? 0 : 1;  // probes 1 .. the query's first count
           eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
           eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
           eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
@@ -536,8 +543,9 @@ struct tq_bucketed {
           });
           ba.floor = sc.floor.as<float>();
         }
-        pa.probe_begin = first;
+        pa.probe_begin = 0;
         pa.probe_end = max_probe;
+        pa.first_split = 2;  // from the query's first count on
       }
       eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
       eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
@@ -545,7 +553,7 @@ struct tq_bucketed {
       mg.cand_score = ba.cand_score;
       mg.cand_id = ba.cand_id;
       mg.nq = static_cast<long long>(m);
-      mg.n_lists = max_probe * 2;
+      mg.n_lists = max_probe * vcb::kBsListsPerProbe;
       mg.k = static_cast<int>(kscan);
       mg.k_out = static_cast<int>(kscan);
       mg.out_score = d_scores + q0 * ke;
