@@ -528,13 +528,18 @@ struct tq_bucketed {
         // first probes cost most without a floor), then the floor of all
         // first probes for the rest. Each floor is the k-th best of the
         // candidates appended so far, a lower bound of the final k-th best.
+        // The scan grid of a step is its own item bound (pairs / 8 + buckets):
+        // one probe per query, then at most first - 1 (a query's first count
+        // never exceeds the one of max_probe), then at most max_probe - 1.
         const int steps[3] = {0, 1, first};
         for (int st = 0; st < 2; ++st) {
           pa.probe_begin = steps[st];
           pa.probe_end = st == 0 ? 1 : max_probe;
           pa.first_split = st == 0 ? 0 : 1;  // probes 1 .. the query's first count
+          const long long step_items = vcb::max_items(static_cast<long long>(m), st == 0 ? 1 : first - 1, nb);
           eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
-          eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
+          eng->launch(tq_index::kScan, s, "bucket scan kernel",
+                      [&] { return vcb::launch_bucket_scan(ba, std::min(items, step_items), s); });
           eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
             cudaError_t e = vcb::launch_merge(fm, s);
             if (e != cudaSuccess) return e;
@@ -547,8 +552,11 @@ struct tq_bucketed {
         pa.probe_end = max_probe;
         pa.first_split = 2;  // from the query's first count on
       }
+      const long long last_items =
+          two_phase ? std::min(items, vcb::max_items(static_cast<long long>(m), max_probe - 1, nb)) : items;
       eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
-      eng->launch(tq_index::kScan, s, "bucket scan kernel", [&] { return vcb::launch_bucket_scan(ba, items, s); });
+      eng->launch(tq_index::kScan, s, "bucket scan kernel",
+                  [&] { return vcb::launch_bucket_scan(ba, last_items, s); });
       vcb::MergeArgs mg{};
       mg.cand_score = ba.cand_score;
       mg.cand_id = ba.cand_id;
