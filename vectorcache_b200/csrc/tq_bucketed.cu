@@ -531,12 +531,22 @@ struct tq_bucketed {
         // The scan grid of a step is its own item bound (pairs / 8 + buckets):
         // one probe per query, then at most first - 1 (a query's first count
         // never exceeds the one of max_probe), then at most max_probe - 1.
-        const int steps[3] = {0, 1, first};
-        for (int st = 0; st < 2; ++st) {
+        // With 32 first probes, a floor after the first 8 as well: probes 8..31
+        // then scan above the k-th best of 8 probes instead of probe 0's.
+        int steps[4] = {0, 1, first, 0};
+        int n_steps = 2;
+        if (first > vcb::kFloorProbes) {
+          steps[2] = vcb::kFloorProbes;
+          steps[3] = first;
+          n_steps = 3;
+        }
+        for (int st = 0; st < n_steps; ++st) {
           pa.probe_begin = steps[st];
-          pa.probe_end = st == 0 ? 1 : max_probe;
-          pa.first_split = st == 0 ? 0 : 1;  // probes 1 .. the query's first count
-          const long long step_items = vcb::max_items(static_cast<long long>(m), st == 0 ? 1 : first - 1, nb);
+          // the last first-probe step ends at the query's own first count
+          pa.probe_end = st == 0 ? 1 : (st + 1 == n_steps ? max_probe : steps[st + 1]);
+          pa.first_split = st == 0 ? 0 : 1;
+          const long long step_items =
+              vcb::max_items(static_cast<long long>(m), steps[st + 1] - steps[st], nb);
           eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
           eng->launch(tq_index::kScan, s, "bucket scan kernel",
                       [&] { return vcb::launch_bucket_scan(ba, std::min(items, step_items), s); });
