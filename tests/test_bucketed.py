@@ -182,6 +182,24 @@ def test_per_query_probe_counts(small):
 
 
 @pytest.mark.gpu
+def test_query_passes_match_small_batches(small):
+    # 20,000 queries exceed one pass (at most 16,384 queries); with per-query
+    # probe counts and re-ranking the passes must give exactly what the same
+    # queries give in batches that fit one pass.
+    db, _, params = small
+    p = vcb.BucketParams(**{**params.__dict__, "rerank_k": 20})
+    idx = _build(db, 4, p)
+    q = vmf_mixture(20_000, db.shape[1], seed=19, clusters=60)
+    counts = (np.arange(q.shape[0]) % 13 + 1).astype(np.uint32)
+    whole = idx.search(q, 10, n_probe=13, n_probe_per_query=counts)
+    for s in range(0, q.shape[0], 5000):
+        part = idx.search(q[s:s + 5000], 10, n_probe=13, n_probe_per_query=counts[s:s + 5000])
+        assert np.array_equal(whole.ids[s:s + 5000], part.ids)
+        assert bits_equal(whole.scores[s:s + 5000], part.scores)
+    idx.close()
+
+
+@pytest.mark.gpu
 def test_recall_grows_with_n_probe(small):
     db, q, params = small
     idx = _build(db, 4, params)
