@@ -44,12 +44,15 @@ cudaError_t launch_assign(const float* A, long long m, const float* B, long long
 // Largest number of buckets one query may probe.
 constexpr int kMaxProbe = 2048;
 // Probes scanned before the rest to bound the candidates kept from the rest:
-// 8, or 32 from 256 probes on (measured at 1.2M x 100, 4-bit, k = 100 kept
-// candidates, probe 0 scanned alone first: 32 first probes scan 512 probes
-// 3.3 % and 256 probes 3.8 % faster than 16; 64 is no faster than 32).
+// 8, or 32 from 128 probes on (with a floor after 8 of the 32). Measured at
+// 1.2M x 100, 4-bit, k = 100 kept candidates, probe 0 scanned alone first: 32
+// first probes scan 512 probes 3.3 % and 256 probes 3.8 % faster than 16, 64 is
+// no faster than 32; from 128 instead of 256 probes on, a learned per-query
+// assignment runs 0.8 % faster and fixed n_probe 128 is unchanged, from 64 on
+// fixed n_probe 64 is 5 % slower.
 constexpr int kFloorProbes = 8;
 constexpr int kFloorProbesWide = 32;
-constexpr int kFloorWideFrom = 256;
+constexpr int kFloorWideFrom = 128;
 
 // Per row of S (row stride ld, ncols valid columns): the top p entries, score
 // descending, equal scores by lower column; p <= kMaxProbe. Rows with fewer

@@ -500,7 +500,7 @@ struct tq_bucketed {
       vcb::check(cudaMemsetAsync(sc.acount.get(), 0, m * 4, s), "cudaMemsetAsync");
       ba.append_count = sc.acount.as<uint32_t>();
       // The best-routed buckets first: the k-th best score over a query's
-      // first 8 (32 from 256 probes) probes is a lower bound of its k-th best over all
+      // first 8 (32 from 128 probes) probes is a lower bound of its k-th best over all
       // probes, so the scan of the remaining probes keeps only scores at or
       // above it (few insertions, few candidates for the merge). The kept top
       // k is the same. The first-probe count follows each query's own n_probe
