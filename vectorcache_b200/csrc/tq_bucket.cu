@@ -793,7 +793,7 @@ __device__ __forceinline__ bool pair_in_range(const PairArgs& a, long long q, in
   const int np = probes_of(a, q);
   int lo = a.probe_begin, hi = a.probe_end;
   if (a.first_split) {
-    int f = np >= kFloorWideFrom ? kFloorProbesWide : kFloorProbes;
+    int f = np >= a.wide_from ? kFloorProbesWide : kFloorProbes;
     f = f < np ? f : np;
     if (a.first_split == 1) {
       hi = hi < f ? hi : f;

@@ -53,6 +53,12 @@ constexpr int kMaxProbe = 2048;
 constexpr int kFloorProbes = 8;
 constexpr int kFloorProbesWide = 32;
 constexpr int kFloorWideFrom = 128;
+// Passes of fewer queries skip the floor after 8 probes and keep 8 first
+// probes up to 256 probes: there the extra step's launches (pairs, scan,
+// merge) cost more than they save (measured at 1.2M x 100: 16 queries at 128
+// probes 0.568 -> 0.475 ms, 64 at 512 probes 0.814 -> 0.754 ms without them).
+constexpr int kFloorWideFromSmall = 256;
+constexpr long long kMidFloorMinQueries = 4096;
 
 // Per row of S (row stride ld, ncols valid columns): the top p entries, score
 // descending, equal scores by lower column; p <= kMaxProbe. Rows with fewer
@@ -138,9 +144,10 @@ struct PairArgs {
   int probe_begin = 0;
   int probe_end = 1 << 30;
   // 1: also end at the query's own first-probe count, 2: begin there. That
-  // count follows the query's n_probe: kFloorProbesWide from kFloorWideFrom
+  // count follows the query's n_probe: kFloorProbesWide from wide_from
   // probes, else kFloorProbes (at most its n_probe).
   int first_split = 0;
+  int wide_from = kFloorWideFrom;
 };
 // Groups the (query, probe) pairs by bucket and builds the scan work items.
 cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream);

@@ -506,8 +506,10 @@ struct tq_bucketed {
       // k is the same. The first-probe count follows each query's own n_probe
       // (per-query counts: a query with 64 probes spends 8 of them without
       // the full floor, as a fixed n_probe of 64 does, not 32).
+      const bool mid_floor = static_cast<long long>(m) >= vcb::kMidFloorMinQueries;
+      pa.wide_from = mid_floor ? vcb::kFloorWideFrom : vcb::kFloorWideFromSmall;
       const int first =
-          std::min(max_probe >= vcb::kFloorWideFrom ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
+          std::min(max_probe >= pa.wide_from ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
       const bool two_phase = max_probe > vcb::kFloorProbes;
       if (two_phase) {
         sc.fl_s.reserve(m * kscan * 4);
@@ -535,7 +537,7 @@ struct tq_bucketed {
         // then scan above the k-th best of 8 probes instead of probe 0's.
         int steps[4] = {0, 1, first, 0};
         int n_steps = 2;
-        if (first > vcb::kFloorProbes) {
+        if (mid_floor && first > vcb::kFloorProbes) {
           steps[2] = vcb::kFloorProbes;
           steps[3] = first;
           n_steps = 3;
