@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--recall-queries", type=int, default=1000)
     p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-variants", action="store_true", help="skip the (bits, k) variants of the flat workload")
     p.add_argument("--workload", choices=["flat", "bucketed", "serving", "multi"], default="flat",
                    help="flat: the 1M x 1536 flat search (default); bucketed: the 1.2M x 100 bucketed index, "
                         "learned n_probe against fixed n_probe; serving: the continuous-batching server over a "
@@ -217,16 +218,19 @@ def recall_at(approx_ids, exact_ids, t):
     return hits / (t * a.shape[0])
 
 
-def cpu_reference_run(db_host, q_host, calib_host, bits, k, sample_queries, steps, warmup):
-    """Times the reference's own CPU search_flat (all host cores) on the same
-    index; returns (qps_list, threads, build_seconds)."""
+def reference_index(db_host, calib_host, bits):
+    """The reference's own CPU index (fit_calibration + encode + repack on all
+    host cores); returns (index, threads, build_seconds)."""
     from oracle.oracle import Reference, ReferenceIndex
 
     ref = Reference()
-    threads = ref.max_threads()
     t0 = time.perf_counter()
     idx = ReferenceIndex(ref, db_host, bits, calib_rows=calib_host)
-    build_s = time.perf_counter() - t0
+    return idx, ref.max_threads(), time.perf_counter() - t0
+
+
+def time_reference(idx, q_host, k, sample_queries, steps, warmup):
+    """QPS of the reference's search_flat per step of `sample_queries` queries."""
     qps = []
     nq = q_host.shape[0]
     for step in range(warmup + steps):
@@ -237,8 +241,49 @@ def cpu_reference_run(db_host, q_host, calib_host, bits, k, sample_queries, step
         dt = time.perf_counter() - t
         if step >= warmup:
             qps.append(qs.shape[0] / dt)
+    return qps
+
+
+def cpu_reference_run(db_host, q_host, calib_host, bits, k, sample_queries, steps, warmup):
+    """Times the reference's own CPU search_flat (all host cores) on the same
+    index; returns (qps_list, threads, build_seconds)."""
+    idx, threads, build_s = reference_index(db_host, calib_host, bits)
+    qps = time_reference(idx, q_host, k, sample_queries, steps, warmup)
     idx.close()
     return qps, threads, build_s
+
+
+def search_parity(ref_idx, q_host, k, got_scores, got_ids):
+    """Top-k of our search against the reference's search_flat on the same
+    queries: ids identical and scores bit-equal (score desc, ties by lower id)."""
+    ws, wi = ref_idx.search(q_host, k)
+    got_ids = np.asarray(got_ids).astype(np.uint64)
+    got_scores = np.ascontiguousarray(got_scores, np.float32)
+    rows_ids = int(np.count_nonzero(np.any(got_ids != wi, axis=1)))
+    rows_sc = int(np.count_nonzero(np.any(got_scores.view(np.uint32) != ws.view(np.uint32), axis=1)))
+    return {"queries": int(q_host.shape[0]), "k": int(k), "ids_equal": rows_ids == 0,
+            "scores_bitequal": rows_sc == 0, "rows_with_id_mismatch": rows_ids,
+            "rows_with_score_mismatch": rows_sc}
+
+
+def code_parity(ref_idx, index):
+    """Codes, alpha and TQ+ calibration of our index against the reference's
+    encode of the same rows. A code row that differs would be a rounding
+    difference at a codebook boundary (allowed within 1e-6 relative); it is
+    counted, not hidden."""
+    rp, ra = ref_idx.packed()
+    gp, ga = index.packed(), index.alpha()
+    out = {"rows": int(rp.shape[0]),
+           "code_rows_differing": int(np.count_nonzero(np.any(gp != rp, axis=1))),
+           "alpha_bitequal": bool(np.array_equal(ga.view(np.uint32), ra.view(np.uint32)))}
+    try:
+        rsh, rsc = ref_idx.calibration()
+        gsh, gsc = index.calibration()
+        out["calibration_bitequal"] = bool(np.array_equal(gsh.view(np.uint32), rsh.view(np.uint32)) and
+                                           np.array_equal(gsc.view(np.uint32), rsc.view(np.uint32)))
+    except RuntimeError:
+        out["calibration_bitequal"] = None
+    return out
 
 
 def make_data(args, rank, device):
@@ -278,7 +323,9 @@ def run_reference(args, world, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": f"flat TurboQuant search {args.n}x{args.dim} {args.bits}-bit TQ+, k={args.k}",
                    "n": args.n, "dim": args.dim, "bits": args.bits, "k": args.k, "nq": args.nq,
-                   "queries_per_step": args.cpu_queries},
+                   "queries_per_step": args.cpu_queries,
+                   "batch_note": f"steps of {args.cpu_queries} queries (our arm: {args.nq} per step) so that "
+                                 "the run ends within minutes; QPS is per query"},
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -286,18 +333,45 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# Other (bits, k) points of the 1M x 1536 configuration, timed and checked
+# against the reference beside the headline (4-bit, k = 10).
+VARIANTS = ((4, 64), (2, 10), (2, 64))
+
+
+def device_timed(fn, stream, steps, warmup):
+    """Mean ms per call of fn on `stream`, CUDA events, after `warmup` calls."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
 def run_ours(args, world, rank, local):
     import torch
 
     import vectorcache_b200 as vcb
+    from vectorcache_b200.sharded import ShardedIndex
 
     device = torch.device("cuda", local)
     db, q = make_data(args, rank, device)
-    index = vcb.TurboQuantIndex(args.dim, args.bits, device=local)
+    # Shard r holds global ids [r * n, (r + 1) * n). One TQ+ calibration for
+    # every shard: rank 0's first rows, broadcast to the other ranks.
+    shard = ShardedIndex(args.dim, args.bits, device=local, shard_base=rank * args.n)
+    index = shard.index
     idx_stream = torch.cuda.ExternalStream(index.stream(), device=device)
 
-    # Build: calibrate on the first rows, stage, encode (timed as encode vectors/s).
-    index.calibrate_device(db[: args.calib])
+    # Build: calibrate, stage, encode (timed as encode vectors/s).
+    sample = db[: args.calib].clone() if rank == 0 else torch.empty((args.calib, args.dim), device=device)
+    shard.calibrate_shared(sample)
+    del sample
     index.add_device(db)
     index.set_profiling(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -308,6 +382,7 @@ def run_ours(args, world, rank, local):
     prof_build = index.read_profile()
     prepare_ms = ev0.elapsed_time(ev1)  # includes growing the layout buffers
     encode_vps = args.n / (prof_build["encode_ms"] / 1e3)  # encode + relayout kernels
+    encode_kernels_ms = prof_build["encode_ms"]
 
     k = args.k
     # An explicit stream: NULL would mean the index's own (non-blocking) stream.
@@ -317,10 +392,9 @@ def run_ours(args, world, rank, local):
     d_ids = torch.empty((args.nq, k), dtype=torch.int64, device=device)
 
     def step():
-        index.search_device(q, k, d_scores, d_ids, stream=stream)
         if world > 1:
-            off = torch.as_tensor(rank * args.n, device=device)
-            return merge_shards(world, d_scores, d_ids + off, k)
+            return shard.search_device(q, k, d_scores, d_ids, stream=stream)
+        index.search_device(q, k, d_scores, d_ids, stream=stream)
         return d_scores, d_ids
 
     # Recall@10 of the returned top-k against exact fp32 inner-product top-k.
@@ -329,7 +403,6 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     exact = exact_topk(db, q[:nr], 10)
     recall10 = recall_at(d_ids[:nr].cpu().numpy(), exact.cpu().numpy(), min(10, k))
-    del exact
 
     for _ in range(args.warmup):
         step()
@@ -348,9 +421,13 @@ def run_ours(args, world, rank, local):
     elapsed_ms = max_over_ranks(world, t0.elapsed_time(t1))
     prof = index.read_profile()
     clocks = clk.summary()
+    plan = index.scan_plan(args.nq, k)
 
     queries_scanned = args.nq * args.steps * world  # one query against one 1M-vector shard = one unit
     value = queries_scanned / (elapsed_ms / 1e3)
+    # this shard's own top-k of the first queries, for the reference comparison
+    n_par = min(args.cpu_queries, args.nq)
+    dev_top = (d_scores[:n_par].cpu().numpy(), d_ids[:n_par].cpu().numpy()) if world == 1 else None
 
     # Latency of small batches (device-resident queries): p50 / p99 over repeats.
     latency = {}
@@ -407,14 +484,16 @@ def run_ours(args, world, rank, local):
         host_step()
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(idx_stream)
-    for _ in range(args.steps):
-        host_step()
-    e1.record(idx_stream)
-    e1.synchronize()
+    with ClockSampler(local) as clk_e2e:
+        e0.record(idx_stream)
+        for _ in range(args.steps):
+            host_step()
+        e1.record(idx_stream)
+        e1.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(world, e0.elapsed_time(e1))
     e2e_value = args.nq * args.steps * world / (e2e_ms / 1e3)
+    e2e_top = (out_s.reshape(args.nq, k)[:n_par].copy(), out_i.reshape(args.nq, k)[:n_par].copy())
 
     # Roofline of the dominant kernel (scan): algorithmic bytes per launch over
     # its mean event-timed duration.
@@ -431,23 +510,76 @@ def run_ours(args, world, rank, local):
     nbg = args.dim // (8 // args.bits)
     lookups = 2.0 * args.nq * args.n * nbg
     total_kernel_ms = prof["prep_ms"] + prof["scan_ms"] + prof["merge_ms"]
+    encode_bytes = args.n * (args.dim * 4 + nbg + 4)  # rows read, codes + alpha written
+
+    # The other (bits, k) points of the same data: device-timed QPS, Recall@10,
+    # and their top-k for the reference comparison below.
+    variants = []
+    if world == 1 and not args.no_variants:
+        second = {}
+        with ClockSampler(local) as clk_var:
+            for bits, kv in VARIANTS:
+                if (bits, kv) == (args.bits, k):
+                    continue
+                if bits == args.bits:
+                    vidx = index
+                else:
+                    if bits not in second:
+                        second[bits] = vcb.TurboQuantIndex(args.dim, bits, device=local)
+                        second[bits].calibrate_device(db[: args.calib])
+                        second[bits].add_device(db)
+                        second[bits].prepare()
+                    vidx = second[bits]
+                vs = torch.empty((args.nq, kv), dtype=torch.float32, device=device)
+                vi = torch.empty((args.nq, kv), dtype=torch.int64, device=device)
+                steps_v = max(2, min(args.steps, 3))
+                ms = device_timed(lambda: vidx.search_device(q, kv, vs, vi, stream=stream), stream, steps_v, 3)
+                variants.append({"bits": bits, "k": kv, "qps": args.nq / (ms / 1e3), "ms_per_step": ms,
+                                 "steps": steps_v, "warmup": 3,
+                                 "recall_at_10": recall_at(vi[:nr].cpu().numpy(), exact.cpu().numpy(), 10),
+                                 "_top": (vs[:n_par].cpu().numpy(), vi[:n_par].cpu().numpy())})
+        var_clocks = clk_var.summary()
+        for v in variants:
+            v["clocks"] = var_clocks
+    del exact
 
     cpu_base = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             db_h = db.cpu().numpy()
             q_h = q.cpu().numpy()
             del db
             torch.cuda.empty_cache()
-            qps, threads, build_s = cpu_reference_run(db_h, q_h, db_h[: args.calib], args.bits, k,
-                                                      args.cpu_queries, 2, 1)
+            ref_idx, threads, build_s = reference_index(db_h, db_h[: args.calib], args.bits)
+            qps = time_reference(ref_idx, q_h, k, args.cpu_queries, 2, 1)
             cpu_base = {"value": statistics.mean(qps), "unit": "queries/s", "cores": threads, "kind": "reference",
                         "sample": f"{args.cpu_queries} queries x 2 timed steps against the same "
                                   f"{args.n}x{args.dim} {args.bits}-bit TQ+ data, index built by the "
                                   f"reference's own encode/repack on the host ({build_s:.1f}s), avx2_perm0"}
+            # Parity at the headline size: our codes and top-k against the
+            # reference's own encode and search_flat of the same rows.
+            qp = q_h[:n_par]
+            parity = {"reference": "search_flat, avx2_perm0 backend (oracle/_ref)",
+                      "codes": code_parity(ref_idx, index),
+                      "device_search": search_parity(ref_idx, qp, k, *dev_top),
+                      "host_abi_search": search_parity(ref_idx, qp, k, *e2e_top)}
+            for v in variants:
+                if v["bits"] == args.bits:
+                    v["parity"] = search_parity(ref_idx, qp, v["k"], *v["_top"])
+            ref_idx.close()
+            for bits in sorted({v["bits"] for v in variants} - {args.bits}):
+                ref2, _, _ = reference_index(db_h, db_h[: args.calib], bits)
+                codes2 = code_parity(ref2, second[bits])
+                for v in variants:
+                    if v["bits"] == bits:
+                        v["parity"] = dict(search_parity(ref2, qp, v["k"], *v["_top"]), codes=codes2)
+                ref2.close()
         except Exception as exc:  # the baseline is reported, never required
             cpu_base = {"value": None, "unit": "queries/s", "cores": os.cpu_count(), "kind": "reference",
                         "sample": f"unavailable: {exc}"}
+    for v in variants:
+        v.pop("_top", None)
 
     if rank == 0:
         line = {
@@ -462,11 +594,14 @@ def run_ours(args, world, rank, local):
                 "recall_queries": nr, "l2": "inputs larger than L2 (codes %.0f MB per shard)"
                                            % (args.n * (nbg + 4) / 1e6),
                 "parallelism": f"shard{world}" if world > 1 else "single",
+                "scan_plan": plan,
                 "encode_vectors_per_s": encode_vps, "prepare_ms": prepare_ms,
                 "kernel_ms_per_step": {"prep": prof["prep_ms"] / args.steps, "scan": prof["scan_ms"] / args.steps,
                                        "merge": prof["merge_ms"] / args.steps},
                 "nibble_lookups_per_s": lookups * args.steps / (prof["scan_ms"] / 1e3) if prof["scan_ms"] else None,
-                "encode_kernel_ms": prof_build["encode_ms"],
+                "encode_kernel_ms": encode_kernels_ms,
+                "encode_roofline": {"bytes": encode_bytes, "achieved_gbs": encode_bytes / (encode_kernels_ms / 1e3) / 1e9,
+                                    "peak": peak, "frac": encode_bytes / (encode_kernels_ms / 1e3) / 1e9 / peak},
                 "latency_ms": latency,
             },
             "roofline": {"kernel": "scan_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -478,18 +613,23 @@ def run_ours(args, world, rank, local):
                          "one_query_pass": (dict(one_query, peak=peak, frac=one_query["achieved"] / peak)
                                             if one_query else None)},
             "cpu_baseline": cpu_base,
+            "parity": parity,
+            "variants": variants,
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * args.dim * 4,
-                    "d2h_bytes_per_step": args.nq * k * 12},
+                    "d2h_bytes_per_step": args.nq * k * 12, "clocks": clk_e2e.summary()},
             "gpu_launches": prof["prep_launches"] + prof["scan_launches"] + prof["merge_launches"],
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
+    for extra in (second.values() if world == 1 and not args.no_variants else ()):
+        extra.close()
     index.close()
 
 
 BUCKETED_METRIC = "QPS at Recall@10 >= 0.95 (bucketed 1.2Mx100 4-bit cosine, learned n_probe vs fixed n_probe)"
 PROBE_CLASSES = (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048)
 FIXED_PROBES = (64, 128, 256, 384, 512, 768, 1024, 1536, 2048)
+FINE_STEP = 16  # fixed n_probe grid step below the first coarse point reaching the target
 RECALL_TARGET = 0.95
 # Prediction-rule sweeps of the learned n_probe, fewest buckets first:
 # trade-offs (recall objective) and coverages (classes objective).
@@ -599,19 +739,34 @@ def run_bucketed(args, world, rank, local):
         return e0.elapsed_time(e1) / args.steps
 
     # The plain path at fixed n_probe: QPS and Recall@10 per n_probe; the
-    # operating point is the smallest n_probe reaching the recall target.
+    # operating point is the smallest n_probe reaching the recall target,
+    # found on a coarse grid and then in steps of 16 below the first coarse
+    # point that reaches it.
+    clk = ClockSampler(local).__enter__()
     sweep = {}
-    for p in ([args.bucketed_fixed_only] if args.bucketed_fixed_only else FIXED_PROBES):
-        ms = timed(lambda p=p: idx.search_device(d_q, k, d_s, d_i, n_probe=p, stream=stream))
+
+    def fixed_point(p):
+        ms = timed(lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=p, stream=stream))
         sweep[p] = {"n_probe": p, "ms_per_step": ms, "qps": nq / (ms / 1e3),
                     "recall_at_10": float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())}
+
+    for p in ([args.bucketed_fixed_only] if args.bucketed_fixed_only else FIXED_PROBES):
+        fixed_point(p)
     if args.bucketed_fixed_only:
         # the plain path at one n_probe only (profiling runs)
-        print(json.dumps({"metric": BUCKETED_METRIC, "fixed_only": sweep[args.bucketed_fixed_only]}), flush=True)
+        clk.__exit__()
+        print(json.dumps({"metric": BUCKETED_METRIC, "fixed_only": sweep[args.bucketed_fixed_only],
+                          "clocks": clk.summary()}), flush=True)
         idx.close()
         return
     reach = [p for p in FIXED_PROBES if sweep[p]["recall_at_10"] >= RECALL_TARGET]
-    p_op = reach[0] if reach else FIXED_PROBES[-1]
+    p_coarse = reach[0] if reach else FIXED_PROBES[-1]
+    below = [p for p in FIXED_PROBES if p < p_coarse]
+    for p in range((below[-1] if below else 0) + FINE_STEP, p_coarse, FINE_STEP):
+        fixed_point(p)
+    grid = sorted(sweep)
+    reach = [p for p in grid if sweep[p]["recall_at_10"] >= RECALL_TARGET]
+    p_op = reach[0] if reach else p_coarse
     fixed = sweep[p_op]
     recall_fixed = fixed["recall_at_10"]
     fixed_ms = fixed["ms_per_step"]
@@ -670,6 +825,7 @@ def run_bucketed(args, world, rank, local):
         best["kernel_ms"] = kernel_ms(lambda: idx.search_learned_device(
             d_q, k, mlp, d_s, d_i, coverage=best["rule"], min_confidence=0.0, fallback_n_probe=p_op,
             stream=stream))
+    clk.__exit__()
     line = {
         "metric": BUCKETED_METRIC, "value": best["qps"] if best else None, "unit": "queries/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -682,7 +838,8 @@ def run_bucketed(args, world, rank, local):
                    "classes": list(classes), "final_loss": final_loss, "probe_objective": objective,
                    "recall_target": RECALL_TARGET},
         "fixed": fixed, "learned": best, "speedup_vs_fixed": (best["qps"] / qps_fixed) if best else None,
-        "fixed_sweep": list(sweep.values()), "learned_sweep": learned_sweep,
+        "fixed_sweep": [sweep[p] for p in sorted(sweep)], "learned_sweep": learned_sweep,
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     mlp.close()
@@ -776,6 +933,7 @@ def run_serving(args, world, rank, local):
     info = srv.info()
     rng = np.random.default_rng(11)
     per_rate = []
+    clk = ClockSampler(local).__enter__()
     for rate in SERVING_RATES:
         budget_q = min(40_000, int(rate * 2.0))
         t, base = 0.0, []
@@ -810,6 +968,7 @@ def run_serving(args, world, rank, local):
                          "flat_p99_ms": float(np.percentile(lat_ms[~is_b], 99)) if (~is_b).any() else None,
                          "bucketed_recall_at_10": hits / max(tot, 1)}
         per_rate.append(row)
+    clk.__exit__()
     best = max(per_rate, key=lambda r: r["learned"]["qps"])
     line = {
         "metric": "serving QPS and p50/p99 latency (10Mx768 3-bit flat + 1.2Mx100 bucketed, Poisson bursts 1-256)",
@@ -820,7 +979,7 @@ def run_serving(args, world, rank, local):
                    "slot_bytes": info["slot_bytes"], "resident_bytes": info["resident_bytes"],
                    "fixed_n_probe": p_op, "learned_rule": cov_op, "probe_objective": objective,
                    "flat_build_s": flat_build_s},
-        "per_rate": per_rate, "server_stats": srv.stats(),
+        "per_rate": per_rate, "server_stats": srv.stats(), "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     srv.close()
@@ -890,6 +1049,7 @@ def run_multi(args, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / args.steps
 
+    clk = ClockSampler(local).__enter__()
     seq_ms = timed(seq_step)
     multi = MultiIndex(idxs)
     t0 = time.perf_counter()
@@ -898,6 +1058,7 @@ def run_multi(args, world, rank, local):
     for j, q in enumerate(queries):
         multi.set_queries(j, q.cpu().numpy())
     multi_ms = timed(lambda: multi.launch(stream=stream))
+    clk.__exit__()
     # exactness: every index's result equals its own search
     seq_step()
     torch.cuda.synchronize()
@@ -919,6 +1080,7 @@ def run_multi(args, world, rank, local):
                    "plan_and_autotune_s": plan_s, "autotuned": cfg},
         "per_index_sequential": {"ms_per_step": seq_ms, "qps": total_q / (seq_ms / 1e3)},
         "speedup_vs_sequential": seq_ms / multi_ms, "identical_to_per_index_search": exact,
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     multi.close()

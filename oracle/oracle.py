@@ -22,7 +22,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libtqoracle.so"
 REF_SO = HERE / "_ref" / "libtqref.so"
-REF_TREE = Path(os.environ.get("VCB_REFERENCE_TREE", "/root/reference"))
+# The reference source tree, when the caller names one (no default location).
+REF_TREE_ENV = "VCB_REFERENCE_TREE"
 
 _SZ = C.c_size_t
 _P = C.c_void_p
@@ -32,11 +33,13 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(_P)
 
 
-def build(reference: bool = True) -> None:
-    """Compile the C oracle, and the reference in place when its tree exists."""
+def build(reference_tree: str | os.PathLike | None = None) -> None:
+    """Compile the C oracle; with `reference_tree` (or $VCB_REFERENCE_TREE) set
+    and present, also compile the reference's own CPU code in place from it."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if reference and REF_TREE.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_TREE}", f"-j{os.cpu_count() or 4}"],
+    tree = reference_tree or os.environ.get(REF_TREE_ENV)
+    if tree and (Path(tree) / "src").is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={tree}", f"-j{os.cpu_count() or 4}"],
                        check=True)
 
 
@@ -249,6 +252,25 @@ class ReferenceIndex:
             raise RuntimeError(self.ref.lib.tqref_last_error().decode())
         kk = ke.value
         return s[: nq * kk].reshape(nq, kk), i[: nq * kk].reshape(nq, kk)
+
+    def packed(self):
+        """The reference's encode output for the index rows: bit-plane codes
+        (n x bits*dim/8) and alpha (n)."""
+        packed = np.zeros((self.n, self.bits * self.dim // 8), np.uint8)
+        alpha = np.zeros(self.n, np.float32)
+        rc = self.ref.lib.tqref_index_packed(self.h, _p(packed), _p(alpha))
+        if rc != 0:
+            raise RuntimeError(self.ref.lib.tqref_last_error().decode())
+        return packed, alpha
+
+    def calibration(self):
+        """The reference's TQ+ shift / scale (raises if not calibrated)."""
+        sh = np.zeros(self.dim, np.float32)
+        sc = np.zeros(self.dim, np.float32)
+        rc = self.ref.lib.tqref_index_calibration(self.h, _p(sh), _p(sc))
+        if rc != 0:
+            raise RuntimeError(self.ref.lib.tqref_last_error().decode())
+        return sh, sc
 
     def close(self):
         if self.h:

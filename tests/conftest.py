@@ -28,7 +28,7 @@ def oracle():
     from oracle import oracle as o
 
     if not o.ORACLE_SO.exists():
-        o.build(reference=False)
+        o.build()
     return o.Oracle()
 
 

@@ -234,3 +234,40 @@ def test_add_after_prepare_keeps_invariants(small):
     res = idx.search(q, 10)
     assert res.ids.shape == (q.shape[0], 10)
     idx.close()
+
+
+@pytest.mark.gpu
+def test_floor_schedules_at_many_buckets(oracle):
+    # Passes of >= 4096 queries take 32 first probes from n_probe 128 on, with
+    # an extra floor after 8 probes; smaller passes take 8 first probes below
+    # n_probe 256 and no middle floor. Both must return the exhaustive top-k
+    # of the probed buckets: the same queries in one pass and in passes below
+    # 4096 agree bit for bit, and both equal the oracle's scan of every probed
+    # bucket (no floor) on the routing's probes and offsets.
+    db = vmf_mixture(120_000, 100, seed=41, clusters=300)
+    params = vcb.BucketParams(n_probe=128, max_bucket_size=300, energy_soft=150, kmeans_iters=3, seed=5)
+    idx = _build(db, 4, params)
+    nb = idx.info()["n_buckets"]
+    assert nb >= 512
+    q = vmf_mixture(4608, 100, seed=42, clusters=300)
+    eng = idx.engine()
+    lay = idx.layout()
+    ns = idx.info()["n_slots"]
+    flat, alpha = eng.codes_flat()[:ns], eng.alpha()[:ns]
+    slot_ids = lay["slot_ids"].astype(np.uint64)
+    starts, sizes = lay["slot_start"].astype(np.int64), lay["bucket_size"].astype(np.int64)
+    for n_probe in (128, 512):
+        whole = idx.search(q, 10, n_probe=n_probe)
+        for s in range(0, q.shape[0], 1536):
+            part = idx.search(q[s:s + 1536], 10, n_probe=n_probe)
+            assert np.array_equal(whole.ids[s:s + 1536], part.ids), (n_probe, s)
+            assert bits_equal(whole.scores[s:s + 1536], part.scores), (n_probe, s)
+        sub = slice(0, 512)
+        tr = idx.search_trace(q[sub], 10, n_probe=n_probe)
+        prep = oracle.prepare_queries(tr["q_hat"], 4)
+        counts = np.full(tr["probes"].shape[0], n_probe, np.uint32)
+        ws, wi = oracle.ivf_search(prep, flat, alpha, slot_ids, starts, sizes, tr["probes"], counts,
+                                   tr["offsets"], 10)
+        assert np.array_equal(whole.ids[sub], wi), n_probe
+        assert bits_equal(whole.scores[sub], ws), n_probe
+    idx.close()

@@ -65,6 +65,86 @@ def test_two_rank_shards_equal_one_index(oracle):
     assert np.array_equal(out["scores"].view(np.uint32), want_s.view(np.uint32))
 
 
+class OracleShardIndex:
+    """The CPU oracle behind the TurboQuantIndex methods ShardedIndex calls
+    (calibrate / add / prepare / search_device), standing in for a device
+    shard on CPU."""
+
+    def __init__(self, bits):
+        from oracle.oracle import Oracle
+
+        self.orc = Oracle()
+        self.bits = bits
+        self.shift = self.scale = None
+        self.rows = []
+
+    def calibrate(self, sample):
+        self.shift, self.scale = self.orc.fit_calibration(np.asarray(sample, np.float32), self.bits)
+
+    def add(self, vectors):
+        self.rows.append(np.asarray(vectors, np.float32))
+
+    def prepare(self):
+        x = np.concatenate(self.rows)
+        self.packed, self.alpha = self.orc.encode(x, self.bits, self.shift, self.scale)
+
+    def search_device(self, q, k, out_s, out_i, stream=None):
+        s, i = self.orc.search_flat(q.numpy(), self.bits, self.packed, self.alpha, k, self.shift, self.scale)
+        ke = s.shape[1]
+        out_s.view(-1)[: s.size] = torch.from_numpy(s.reshape(-1))
+        out_i.view(-1)[: i.size] = torch.from_numpy(i.reshape(-1).astype(np.int64))
+        return ke
+
+
+def _bench_path_rank(rank, world, port, shards, q, n_calib, bits, k, out):
+    """The benchmark's multi-GPU path: rank 0's first rows broadcast as the one
+    calibration sample, each rank's own shard, ids offset by rank * shard
+    size, one all-gather merge."""
+    import torch.distributed as dist
+
+    from vectorcache_b200.sharded import ShardedIndex
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        db = shards[rank]
+        shard = ShardedIndex(db.shape[1], bits, device=0, shard_base=rank * shards[0].shape[0],
+                             index=OracleShardIndex(bits))
+        sample = torch.from_numpy(db[:n_calib].copy()) if rank == 0 else torch.zeros((n_calib, db.shape[1]))
+        shard.calibrate_shared(sample)
+        shard.add(db)
+        shard.prepare()
+        ms, mi = shard.search_device(torch.from_numpy(q), k)
+        out[f"scores{rank}"] = ms.numpy()
+        out[f"ids{rank}"] = mi.numpy()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_sharded_path_equals_one_index(oracle):
+    """Two ranks with different shards (different seeds, as the benchmark
+    generates them) and one broadcast calibration: both ranks return the top-k
+    of one index over the union, calibrated on rank 0's first rows."""
+    from vectorcache_b200.synthetic import power_law
+
+    dim, bits, n, nq, k, n_calib = 128, 4, 2000, 7, 10, 400
+    shards = [power_law(n, dim, seed=1000 + r) for r in range(2)]
+    shards[1][5] = shards[0][11]  # equal scores across the shards: the lower id wins
+    q = power_law(nq, dim, seed=7)
+    manager = mp.get_context("spawn").Manager()
+    out = manager.dict()
+    mp.start_processes(_bench_path_rank, args=(2, _free_port(), shards, q, n_calib, bits, k, out), nprocs=2,
+                       join=True, start_method="spawn")
+    union = np.concatenate(shards)
+    shift, scale = oracle.fit_calibration(shards[0][:n_calib], bits)
+    packed, alpha = oracle.encode(union, bits, shift, scale)
+    want_s, want_i = oracle.search_flat(q, bits, packed, alpha, k, shift, scale)
+    for r in range(2):
+        assert np.array_equal(out[f"ids{r}"], want_i.astype(np.int64))
+        assert np.array_equal(out[f"scores{r}"].view(np.uint32), want_s.view(np.uint32))
+
+
 def test_merge_topk_order():
     s = torch.tensor([[1.0, 3.0, 3.0, 2.0, 3.0]])
     i = torch.tensor([[9, 7, 2, 5, 4]])

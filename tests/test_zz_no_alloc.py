@@ -7,7 +7,9 @@ fixed 16 MiB array inside the library.
 The test calls it through the C ABI twice in a row, with different query
 batches, and checks each result bit for bit against the regular
 tq_index_search_device on the same index; an over-size request must fail
-cleanly. This file is collected last (name order) so that a run which stops at
+cleanly. Further cases cover 3-bit and 2-bit indexes, k above 32 (eight
+candidate lists per vector range) and a request whose candidate lists would
+overflow the array unless the search uses fewer vector ranges. This file is collected last (name order) so that a run which stops at
 the first failure has already run every other test.
 """
 import ctypes as C
@@ -36,8 +38,7 @@ def _search(lib, fn, h, q, k, torch):
     return scores[:, :kk].cpu().numpy(), ids[:, :kk].cpu().numpy()
 
 
-def test_noalloc_search_matches_regular_search():
-    torch = pytest.importorskip("torch")
+def _noalloc_fn(torch):
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
     lib = vcb.load_library()
@@ -45,6 +46,12 @@ def test_noalloc_search_matches_regular_search():
     fn.restype = C.c_int
     fn.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p,
                    C.POINTER(C.c_size_t), C.c_void_p]
+    return lib, fn
+
+
+def test_noalloc_search_matches_regular_search():
+    torch = pytest.importorskip("torch")
+    lib, fn = _noalloc_fn(torch)
 
     dim, bits, n = 768, 4, 20000
     db = power_law(n, dim, seed=31)
@@ -75,4 +82,37 @@ def test_noalloc_search_matches_regular_search():
             C.c_void_p(out_s.data_ptr()), C.c_void_p(out_i.data_ptr()), C.byref(ke), None)
     assert rc == vcb.TQ_ERR_INVALID_ARGUMENT
     assert "no-alloc scratch" in lib.tq_last_error().decode()
+    idx.close()
+
+
+# (dim, bits, n, TQ+, [(queries, k), ...]). The last case needs 392 candidate
+# lists of 64 x 200 entries (40 MB) under the regular plan, so the no-alloc
+# search must cut the vector ranges to fit its 16 MiB array.
+MORE_CASES = [
+    (768, 3, 20000, True, [(40, 10), (9, 64)]),
+    (1536, 2, 9000, True, [(33, 10), (5, 100)]),
+    (256, 4, 30000, False, [(50, 100), (3, 256)]),
+    (256, 4, 100000, False, [(64, 200), (64, 200)]),
+]
+
+
+@pytest.mark.parametrize("case", MORE_CASES, ids=lambda c: f"d{c[0]}_b{c[1]}_n{c[2]}")
+def test_noalloc_bits_and_list_plans(case):
+    torch = pytest.importorskip("torch")
+    lib, fn = _noalloc_fn(torch)
+    dim, bits, n, tq, batches = case
+    db = power_law(n, dim, seed=dim + n)
+    idx = vcb.TurboQuantIndex(dim, bits)
+    if tq:
+        idx.calibrate(db[:2000])
+    idx.add(db)
+    idx.prepare()
+    dev = torch.device("cuda", 0)
+    for j, (nq, k) in enumerate(batches):
+        q = torch.from_numpy(power_law(nq, dim, seed=100 + j)).to(dev)
+        want_s, want_i = _search(lib, lib.tq_index_search_device, idx._h, q, k, torch)
+        got_s, got_i = _search(lib, fn, idx._h, q, k, torch)
+        assert got_i.shape == want_i.shape == (nq, min(k, n))
+        assert np.array_equal(got_i, want_i), (nq, k)
+        assert np.array_equal(got_s.view(np.uint32), want_s.view(np.uint32)), (nq, k)
     idx.close()

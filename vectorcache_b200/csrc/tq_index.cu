@@ -437,6 +437,27 @@ int tq_index_replay_count(const tq_index* h, uint64_t* count) {
   });
 }
 
+int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, int* n_ranges,
+                       uint64_t* range_vectors, int* split_batches) {
+  return vcb::guarded([&] {
+    require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
+    require(h->prepared, TQ_ERR_STATE, "scan plan before prepare");
+    require(k >= 1 && k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be in [1, 256]");
+    require(nq >= 1, TQ_ERR_INVALID_ARGUMENT, "nq must be >= 1");
+    // search_device plans each pass of at most 65,536 queries.
+    const size_t m = std::min<size_t>(nq, size_t{1} << 16);
+    vcb::ScanPlan plan;
+    if (!vcb::plan_scan(static_cast<long long>(h->n), static_cast<long long>(m), static_cast<int>(h->nbg),
+                        static_cast<int>(std::min(k, h->n)), h->sms, &plan)) {
+      vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
+    }
+    if (q_per_cta) *q_per_cta = plan.q_per_cta;
+    if (n_ranges) *n_ranges = plan.n_ranges;
+    if (range_vectors) *range_vectors = static_cast<uint64_t>(plan.range_vectors);
+    if (split_batches) *split_batches = std::max(1, plan.split_batches);
+  });
+}
+
 }  // extern "C"
 
 extern "C" {
@@ -536,7 +557,14 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     require(d_queries && d_scores && d_ids, TQ_ERR_INVALID_ARGUMENT, "null buffer");
     check_aligned(d_queries, "queries");
 
-    // Carve the fixed array: LUTs, per-query constants, candidate lists.
+    // Carve the fixed array: LUTs, per-query constants, candidate lists. The
+    // query count is bounded first so that the byte counts below cannot wrap.
+    if (nq > kNoAllocScratchBytes / (h->nbg * 32)) {
+      vcb::fail(TQ_ERR_INVALID_ARGUMENT,
+                "request of " + std::to_string(nq) + " queries does not fit the no-alloc scratch (" +
+                    std::to_string(kNoAllocScratchBytes) + " bytes; at most " +
+                    std::to_string(kNoAllocScratchBytes / (h->nbg * 32)) + " queries of LUTs at this dim)");
+    }
     const size_t lut_bytes = align256(nq * h->nbg * 32);
     const size_t qf_bytes = align256(nq * 4 * sizeof(float));
     const size_t per_list = nq * ke * (sizeof(float) + sizeof(uint32_t));
@@ -592,7 +620,7 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     p.fa_init = qf + 3 * nq;
     p.q_rot = nullptr;
     p.replay_count = h->d_counter.as<unsigned long long>();
-    vcb::check(vcb::launch_query_prep(p, h->sms, s), "query prep kernel");
+    h->launch(tq_index::kPrep, s, "query prep kernel", [&] { return vcb::launch_query_prep(p, h->sms, s); });
 
     vcb::ScanArgs a{};
     a.codes = h->d_codes.as<uint32_t>();
@@ -608,9 +636,12 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     a.range_vectors = plan.range_vectors;
     a.n_ranges = plan.n_ranges;
     a.lut_chunk_groups = plan.lut_chunk_groups;
+    a.bits = static_cast<int>(h->bits);
     a.cand_score = cand_s;
     a.cand_id = cand_i;
-    vcb::check(vcb::launch_scan(a, plan, s), "scan kernel");
+    h->launch(tq_index::kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
+    h->scan_stream_bytes += static_cast<uint64_t>((nq + plan.q_per_cta - 1) / plan.q_per_cta) * h->n * (h->nbg + 4);
+    h->scan_queries += nq;
 
     vcb::MergeArgs m{};
     m.cand_score = cand_s;
@@ -621,7 +652,7 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     m.k_out = static_cast<int>(ke);
     m.out_score = d_scores;
     m.out_id = d_ids;
-    vcb::check(vcb::launch_merge(m, s), "merge kernel");
+    h->launch(tq_index::kMerge, s, "merge kernel", [&] { return vcb::launch_merge(m, s); });
   });
 }
 

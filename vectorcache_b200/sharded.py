@@ -49,34 +49,75 @@ def shard_bounds(n_total: int, world: int, rank: int) -> tuple[int, int]:
     return b, min(n_total, b + per)
 
 
+def _world(group) -> int:
+    return dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+
+
 class ShardedIndex:
     """One shard of a flat index spread over the ranks of a process group.
 
-    Every rank calls the same methods in the same order (collective calls).
+    Every rank calls the same methods in the same order (collective calls):
+    `calibrate_shared` (one broadcast), `add*`, `prepare`, then any number of
+    `search_device` calls (one all-gather each). `index` defaults to a
+    TurboQuantIndex on `device`; any object with the same calibrate / add /
+    prepare / search_device methods serves (the CPU tests pass one backed by
+    the oracle).
     """
 
-    def __init__(self, dim: int, bits: int, device: int, shard_base: int, group=None):
-        from . import TurboQuantIndex
+    def __init__(self, dim: int, bits: int, device: int, shard_base: int, group=None, index=None):
+        if index is None:
+            from . import TurboQuantIndex
 
-        self.index = TurboQuantIndex(dim, bits, device=device)
+            index = TurboQuantIndex(dim, bits, device=device)
+        self.index = index
+        self.dim = int(dim)
         self.base = int(shard_base)
         self.group = group
-        self.device = torch.device("cuda", device)
 
     def calibrate(self, sample) -> None:
-        """The same sample on every rank, so all shards share one calibration."""
+        """Calibrate on host rows; the caller passes the same sample on every
+        rank, so all shards share one TQ+ calibration."""
         self.index.calibrate(sample)
+
+    def calibrate_shared(self, sample: torch.Tensor, src: int = 0) -> None:
+        """Broadcast rank `src`'s sample rows (every rank passes a tensor of the
+        same shape, dtype and device) and calibrate on them: one TQ+ shift /
+        scale for every shard, so the shards score exactly like one index
+        over their union."""
+        if _world(self.group) > 1:
+            dist.broadcast(sample, src, group=self.group)
+        if sample.is_cuda:
+            self.index.calibrate_device(sample)
+        else:
+            self.index.calibrate(sample.numpy())
 
     def add(self, vectors) -> None:
         self.index.add(vectors)
 
+    def add_device(self, d_vectors) -> None:
+        self.index.add_device(d_vectors)
+
     def prepare(self) -> None:
         self.index.prepare()
 
-    def search_device(self, d_queries: torch.Tensor, k: int, stream=None):
+    def search_device(self, d_queries: torch.Tensor, k: int, out_scores=None, out_ids=None, stream=None):
+        """This shard's top-k (ids offset by the shard base), all-gathered and
+        merged: every rank returns the top-k of the union. With one rank the
+        rows hold k_eff = min(k, n) entries; with several, k entries, ending
+        in (-inf, 2^63 - 1) when the union holds fewer than k vectors."""
         nq = d_queries.shape[0]
-        s = torch.empty((nq, k), dtype=torch.float32, device=self.device)
-        i = torch.empty((nq, k), dtype=torch.int64, device=self.device)
+        dev = d_queries.device
+        s = out_scores if out_scores is not None else torch.empty((nq, k), dtype=torch.float32, device=dev)
+        i = out_ids if out_ids is not None else torch.empty((nq, k), dtype=torch.int64, device=dev)
         ke = self.index.search_device(d_queries, k, s, i, stream=stream)
-        s, i = s[:, :ke], i[:, :ke] + self.base
+        if ke < k:  # rows were written with stride k_eff = min(k, shard size)
+            s = s.reshape(-1)[: nq * ke].view(nq, ke)
+            i = i.reshape(-1)[: nq * ke].view(nq, ke)
+        i = i + self.base
+        if _world(self.group) == 1:
+            return s, i
+        if ke < k:  # equal shapes on every rank for the all-gather
+            pad_s = torch.full((nq, k - ke), float("-inf"), dtype=torch.float32, device=dev)
+            pad_i = torch.full((nq, k - ke), torch.iinfo(torch.int64).max, dtype=torch.int64, device=dev)
+            s, i = torch.cat([s, pad_s], 1), torch.cat([i, pad_i], 1)
         return allgather_merge(s, i, k, self.group)
