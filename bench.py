@@ -54,11 +54,13 @@ def parse():
     p.add_argument("--cpu-queries", type=int, default=64, help="queries per CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true", help="skip the (bits, k) variants of the flat workload")
-    p.add_argument("--workload", choices=["flat", "bucketed", "serving", "multi"], default="flat",
+    p.add_argument("--ref-gpu-queries", type=int, default=2368,
+                   help="queries the reference's own GPU index searches beside ours (0: skip)")
+    p.add_argument("--workload", choices=["flat", "bucketed", "serving", "multi", "encode"], default="flat",
                    help="flat: the 1M x 1536 flat search (default); bucketed: the 1.2M x 100 bucketed index, "
                         "learned n_probe against fixed n_probe; serving: the continuous-batching server over a "
                         "10M x 768 flat index and the bucketed index; multi: 32 flat indexes in one persistent "
-                        "graph-captured launch")
+                        "graph-captured launch; encode: the encode kernels alone")
     p.add_argument("--serving-flat-n", type=int, default=10_000_000)
     p.add_argument("--bucketed-n", type=int, default=1_200_000)
     p.add_argument("--bucketed-train", type=int, default=50_000, help="training queries of the learned probe")
@@ -253,6 +255,38 @@ def cpu_reference_run(db_host, q_host, calib_host, bits, k, sample_queries, step
     return qps, threads, build_s
 
 
+def reference_gpu_run(db_h, q_h, exact_np, dim, bits, k, nq_time):
+    """The reference's own GPU flat index (gpu::FlatIndex from src/gpu, built
+    by `make -C oracle refgpu` with the one cast kernels.cu needs) on the same
+    B200, data and queries: its host-buffer search of nq_time queries (query
+    upload and result download included, as in our e2e number), timed with
+    the host clock around the synchronous call; Recall@10 against the same
+    exact top-10. It has no TQ+ and keeps an approximate top-k."""
+    from oracle.oracle import REF_GPU_SO, ReferenceGpuIndex
+
+    if not REF_GPU_SO.exists():
+        return {"unavailable": "oracle/_ref/libtqrefgpu.so was not built"}
+    idx = ReferenceGpuIndex(dim, bits)
+    try:
+        t0 = time.perf_counter()
+        idx.add(db_h)
+        idx.prepare()
+        build_s = time.perf_counter() - t0
+        idx.search(q_h[:4], k)  # first launch (module load, buffers)
+        qs = q_h[:nq_time]
+        t0 = time.perf_counter()
+        _, ids = idx.search(qs, k)
+        dt = time.perf_counter() - t0
+        nr = min(exact_np.shape[0], nq_time)
+        return {"impl": "reference gpu::FlatIndex (src/gpu/kernels.cu scan_mq_topk, float ADC, no TQ+)",
+                "qps": nq_time / dt, "seconds": dt, "queries": nq_time, "k": k,
+                "recall_at_10": recall_at(ids[:nr], exact_np[:nr], min(10, k)), "recall_queries": nr,
+                "prepare_s": build_s, "timing": "host clock around the synchronous search (H2D/D2H included)",
+                "top_k": "approximate: a few candidates per thread and query (kernels.cu:393-516)"}
+    finally:
+        idx.close()
+
+
 def search_parity(ref_idx, q_host, k, got_scores, got_ids):
     """Top-k of our search against the reference's search_flat on the same
     queries: ids identical and scores bit-equal (score desc, ties by lower id)."""
@@ -402,7 +436,8 @@ def run_ours(args, world, rank, local):
     step()
     torch.cuda.synchronize()
     exact = exact_topk(db, q[:nr], 10)
-    recall10 = recall_at(d_ids[:nr].cpu().numpy(), exact.cpu().numpy(), min(10, k))
+    exact_np = exact.cpu().numpy()
+    recall10 = recall_at(d_ids[:nr].cpu().numpy(), exact_np, min(10, k))
 
     for _ in range(args.warmup):
         step()
@@ -545,12 +580,18 @@ def run_ours(args, world, rank, local):
 
     cpu_base = None
     parity = None
+    ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             db_h = db.cpu().numpy()
             q_h = q.cpu().numpy()
             del db
             torch.cuda.empty_cache()
+            if args.ref_gpu_queries > 0:
+                try:
+                    ref_gpu = reference_gpu_run(db_h, q_h, exact_np, args.dim, args.bits, k, args.ref_gpu_queries)
+                except Exception as exc:  # reported, never required
+                    ref_gpu = {"unavailable": f"{type(exc).__name__}: {exc}"}
             ref_idx, threads, build_s = reference_index(db_h, db_h[: args.calib], args.bits)
             qps = time_reference(ref_idx, q_h, k, args.cpu_queries, 2, 1)
             cpu_base = {"value": statistics.mean(qps), "unit": "queries/s", "cores": threads, "kind": "reference",
@@ -615,6 +656,7 @@ def run_ours(args, world, rank, local):
             "cpu_baseline": cpu_base,
             "parity": parity,
             "variants": variants,
+            "reference_gpu": ref_gpu,
             "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * args.dim * 4,
                     "d2h_bytes_per_step": args.nq * k * 12, "clocks": clk_e2e.summary()},
             "gpu_launches": prof["prep_launches"] + prof["scan_launches"] + prof["merge_launches"],
@@ -1088,8 +1130,59 @@ def run_multi(args, world, rank, local):
         idx.close()
 
 
+def run_encode(args, world, rank, local):
+    """Encode workload: n x dim power-law rows (TQ+ calibrated on the first
+    `--calib` rows) encoded into a fresh index per step (calibrate excluded):
+    the encode kernel and the relayout into the scan layout. Reports encode
+    vectors/s and the encode kernel's HBM roofline (rows read, codes and alpha
+    written)."""
+    import torch
+
+    import vectorcache_b200 as vcb
+    from vectorcache_b200.synthetic import power_law_torch
+
+    if world > 1:
+        raise SystemExit("--workload encode runs on one GPU")
+    device = torch.device("cuda", local)
+    db = power_law_torch(args.n, args.dim, seed=1000, device=device)
+    torch.cuda.synchronize()
+    nbg = args.dim // (8 // args.bits)
+    peak, peak_kind = load_peaks()
+    times = {"encode": [], "relayout": []}
+    with ClockSampler(local) as clk:
+        for step in range(args.warmup + args.steps):
+            idx = vcb.TurboQuantIndex(args.dim, args.bits, device=local)
+            idx.calibrate_device(db[: args.calib])
+            idx.add_device(db)
+            idx.set_profiling(True)
+            idx.read_profile()
+            idx.prepare()
+            prof = idx.read_profile()
+            if step >= args.warmup:
+                times["encode"].append(prof["encode_ms"])
+            idx.close()
+    ms = statistics.mean(times["encode"])
+    bytes_alg = args.n * (args.dim * 4 + nbg + 4)
+    line = {
+        "metric": "encode vectors/s", "value": args.n / (ms / 1e3), "unit": "vectors/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"encode {args.n}x{args.dim} {args.bits}-bit TQ+ (calibration on "
+                               f"{args.calib} rows, excluded)", "n": args.n, "dim": args.dim, "bits": args.bits},
+        "roofline": {"kernel": "encode + relayout", "bound": "hbm", "achieved": bytes_alg / (ms / 1e3) / 1e9,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": bytes_alg / (ms / 1e3) / 1e9 / peak, "bytes_per_launch": bytes_alg},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "encode":
+        world, rank, local = dist_setup(args)
+        run_encode(args, world, rank, local)
+        return
     if args.workload == "multi":
         world, rank, local = dist_setup(args)
         run_multi(args, world, rank, local)

@@ -1,10 +1,14 @@
-"""Test infrastructure only — ctypes loaders for the two CPU checkers.
+"""Test infrastructure only — ctypes loaders for the CPU checkers and the
+reference's own GPU index.
 
 * `Oracle`   — oracle/_build/libtqoracle.so, the plain-C restatement of the
                reference's flat TurboQuant arithmetic (tq_oracle.c).
 * `Reference` — oracle/_ref/libtqref.so, the reference's own CPU code compiled
                in place by oracle/Makefile (only where the reference tree was
                available at build time).
+* `ReferenceGpuIndex` — oracle/_ref/libtqrefgpu.so, the reference's own GPU
+               flat index (make -C oracle refgpu), timed by bench.py as the GPU
+               bar to beat.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
 arms use this module, and only as the checker or the timed CPU baseline; the
@@ -22,6 +26,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libtqoracle.so"
 REF_SO = HERE / "_ref" / "libtqref.so"
+REF_GPU_SO = HERE / "_ref" / "libtqrefgpu.so"
 # The reference source tree, when the caller names one (no default location).
 REF_TREE_ENV = "VCB_REFERENCE_TREE"
 
@@ -39,7 +44,7 @@ def build(reference_tree: str | os.PathLike | None = None) -> None:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     tree = reference_tree or os.environ.get(REF_TREE_ENV)
     if tree and (Path(tree) / "src").is_dir():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={tree}", f"-j{os.cpu_count() or 4}"],
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "refgpu", f"REF={tree}", f"-j{os.cpu_count() or 4}"],
                        check=True)
 
 
@@ -300,3 +305,50 @@ def oracle_float_rescore(orc: "Oracle", queries, corpus, ids):
 def reference_float_rescore(ref: "Reference", queries, corpus, ids):
     """The reference's own float_rescore_topk on the same candidate ids."""
     return _float_rescore(ref.lib, "tqref_float_rescore", queries, corpus, ids)
+
+
+class ReferenceGpuIndex:
+    """The reference's own GPU flat index (gpu::FlatIndex: add, prepare,
+    search with host buffers; oracle/_ref/libtqrefgpu.so). Timed as the GPU
+    bar to beat; its top-k is approximate (a few candidates per thread), so
+    it is judged by recall, not compared bit for bit."""
+
+    def __init__(self, dim: int, bits: int, path: Path = REF_GPU_SO):
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle refgpu REF=<reference tree>)")
+        self.h = None
+        self.lib = C.CDLL(str(path))
+        self.lib.tqrefgpu_last_error.restype = C.c_char_p
+        self.dim = dim
+        h = _P()
+        self._check(self.lib.tqrefgpu_create(_SZ(dim), _SZ(bits), C.byref(h)))
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.tqrefgpu_last_error().decode())
+
+    def add(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        self._check(self.lib.tqrefgpu_add(self.h, _p(x), _SZ(x.shape[0])))
+
+    def prepare(self):
+        self._check(self.lib.tqrefgpu_prepare(self.h))
+
+    def search(self, q, k):
+        q = np.ascontiguousarray(q, np.float32)
+        nq = q.shape[0]
+        s = np.zeros(max(nq * k, 1), np.float32)
+        i = np.zeros(max(nq * k, 1), np.uint64)
+        ke = _SZ(0)
+        self._check(self.lib.tqrefgpu_search(self.h, _p(q), _SZ(nq), _SZ(k), _p(s), _p(i), C.byref(ke)))
+        kk = ke.value
+        return s[: nq * kk].reshape(nq, kk), i[: nq * kk].reshape(nq, kk)
+
+    def close(self):
+        if self.h:
+            self.lib.tqrefgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -59,6 +59,12 @@ CASES = [
     ("pl", 2048, 300, 5, 4, True),
     ("mix", 8, 100, 4, 4, False),
     ("mix", 96, 64, 3, 3, True),
+    # the remaining register layouts of the pipelined encode (512, 1024, 520)
+    # and a dim that takes the per-warp row kernel (1000)
+    ("pl", 512, 1000, 5, 4, True),
+    ("mix", 1024, 700, 4, 2, False),
+    ("mix", 520, 900, 5, 4, True),
+    ("pl", 1000, 600, 3, 3, True),
     # wider than 2048: the shared-memory row kernels
     ("mix", 3072, 300, 4, 3, True),
     ("mix", 4096, 257, 3, 4, False),

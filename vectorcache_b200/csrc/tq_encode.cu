@@ -4,6 +4,8 @@
 // Follows the reference's encode (src/encode/encode.cpp:112-231, :294-307) and
 // pack (src/pack/pack.cpp:70-131) arithmetic bit for bit; see tq_device.cuh for
 // the rounding contract.
+#include <type_traits>
+
 #include "tq_kernels.h"
 #include "tq_device.cuh"
 
@@ -307,6 +309,373 @@ __global__ void __launch_bounds__(256) order_stats_kernel(const float* __restric
   }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined encode (dims whose register layout below applies; others use
+// encode_rows_kernel). Persistent CTAs, one per SM; each warp encodes ROWS
+// rows per iteration:
+//   * the rows arrive in shared memory by cp.async (16-byte copies), issued for
+//     the warp's next rows as soon as each row's gather has read its slot, so
+//     the loads of the next rows overlap the arithmetic of the current ones;
+//   * the norm: lane 8j + c runs chain c of row j (the reference's 8-chain
+//     order) out of shared memory;
+//   * the rotation: element i of the row lives in lane l, register r with
+//     i = (r / E) * 32E + l * E + r % E, so butterfly strides below E pair
+//     registers of one lane, strides E .. 16E pair lanes (one shuffle and one
+//     fused multiply-add by +-1 per element, which rounds exactly like the
+//     reference's a + b / a - b), larger strides pair register segments;
+//   * a lane's E consecutive codes pack into whole codes_flat bytes in its own
+//     registers (no cross-lane packing) and leave as one 2-8 byte store.
+// The per-element tables (source offset and sign of the permutation, TQ+
+// shift/scale, the double inv_scale/shift of the inner-product estimate) are
+// stored in the same (register, lane) order, so every table read is one
+// conflict-free shared-memory access.
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Index of the row element held by (lane, register r).
+template <int E>
+__device__ __forceinline__ int pipe_elem(int r, int lane) {
+  return (r / E) * (32 * E) + lane * E + (r % E);
+}
+
+struct PipeLayout {
+  int stride;         // floats per row slot (>= dim + 1, == 8 mod 32)
+  size_t off_bk, off_ss, off_cen, off_src, off_bnd, off_rows, total;
+};
+
+__host__ __device__ inline PipeLayout pipe_layout(int dim, int r_regs, bool tqplus, int warps, int rows) {
+  PipeLayout L;
+  int pad = (8 - dim % 32 + 32) % 32;
+  if (pad == 0) pad = 32;
+  L.stride = dim + pad;
+  const size_t slots = static_cast<size_t>(r_regs) * 32;
+  size_t o = 0;
+  L.off_bk = o;
+  o += tqplus ? slots * 16 : 0;
+  L.off_ss = o;
+  o += tqplus ? slots * 8 : 0;
+  L.off_cen = o;
+  o += 16 * 8;
+  L.off_src = o;
+  o += slots * 4;
+  L.off_bnd = o;
+  o += 16 * 4;
+  o = (o + 15) / 16 * 16;
+  L.off_rows = o;
+  o += static_cast<size_t>(warps) * rows * L.stride * 4;
+  L.total = o;
+  return L;
+}
+
+// Count of boundaries strictly below v, boundaries in shared memory, BITS levels.
+template <int BITS>
+__device__ __forceinline__ unsigned pipe_code(float v, const float* __restrict__ bnd) {
+  unsigned idx = 0;
+#pragma unroll
+  for (int step = 1 << (BITS - 1); step > 0; step >>= 1) {
+    if (v > bnd[idx + step - 1]) idx += step;
+  }
+  return idx;
+}
+
+template <int R, int E, int BITS, int ROWS, int MAXW>
+__global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a) {
+  static_assert(R % E == 0, "segments of E registers");
+  constexpr int SEG = R / E;
+  constexpr int CPB = 8 / BITS;                 // codes per codes_flat byte
+  constexpr int FIELD = BITS == 3 ? 4 : BITS;   // bits per code inside the byte
+  constexpr int RUN_BYTES = E / CPB;            // bytes of one lane's E codes
+  static_assert(RUN_BYTES == 1 || RUN_BYTES == 2 || RUN_BYTES == 4 || RUN_BYTES == 8, "run size");
+  using Run = typename std::conditional<RUN_BYTES == 8, unsigned long long,
+              typename std::conditional<RUN_BYTES == 4, uint32_t,
+              typename std::conditional<RUN_BYTES == 2, uint16_t, uint8_t>::type>::type>::type;
+
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int dim = a.dim;
+  const int warps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const PipeLayout L = pipe_layout(dim, R, a.tqplus, warps, ROWS);
+  double2* s_bk = reinterpret_cast<double2*>(smem + L.off_bk);   // {inv_scale, shift} (TQ+)
+  float2* s_ss = reinterpret_cast<float2*>(smem + L.off_ss);     // {shift, scale} (TQ+)
+  double* s_cen = reinterpret_cast<double*>(smem + L.off_cen);
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + L.off_src);
+  float* s_bnd = reinterpret_cast<float*>(smem + L.off_bnd);
+  float* rows = reinterpret_cast<float*>(smem + L.off_rows) + static_cast<size_t>(warp) * ROWS * L.stride;
+
+  // Tables in (register, lane) order. Elements past dim read the zero word at
+  // column dim of every row slot and have zero TQ+ tables, so they add nothing.
+  for (int t = threadIdx.x; t < R * 32; t += blockDim.x) {
+    const int r = t / 32, l = t % 32;
+    const int i = pipe_elem<E>(r, l);
+    uint32_t src = static_cast<uint32_t>(dim) * 4u;
+    double2 bk = make_double2(0.0, 0.0);
+    float2 ss = make_float2(0.f, 0.f);
+    if (i < dim) {
+      const uint32_t e = a.perm_sign[i];
+      src = ((e & 0x7fffffffu) * 4u) | (e & 0x80000000u);
+      if (a.tqplus) {
+        bk = make_double2(static_cast<double>(a.inv_scale[i]), static_cast<double>(a.shift[i]));
+        ss = make_float2(a.shift[i], a.scale[i]);
+      }
+    }
+    s_src[t] = src;
+    if (a.tqplus) {
+      s_bk[t] = bk;
+      s_ss[t] = ss;
+    }
+  }
+  if (threadIdx.x < 16) {
+    s_cen[threadIdx.x] = static_cast<double>(a.centroids[threadIdx.x]);
+    s_bnd[threadIdx.x] = threadIdx.x < 15 ? a.boundaries[threadIdx.x] : 0.f;
+  }
+  for (int j = lane; j < ROWS; j += 32) rows[j * L.stride + dim] = 0.f;
+
+  const long long n_groups = (a.n + ROWS - 1) / ROWS;
+  const long long g_step = static_cast<long long>(gridDim.x) * warps;
+  const int chunks = dim / 4;  // 16-byte pieces of a row
+  auto prefetch = [&](long long v, int j) {
+    const float* src = a.x + v * static_cast<long long>(dim);
+    float* dst = rows + j * L.stride;
+    for (int c = lane; c < chunks; c += 32) cp_async16(dst + 4 * c, src + 4 * c);
+  };
+  long long grp = static_cast<long long>(blockIdx.x) * warps + warp;
+  if (grp < n_groups) {
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+      if (grp * ROWS + j < a.n) prefetch(grp * ROWS + j, j);
+    }
+  }
+  cp_async_commit();
+  __syncthreads();
+
+  const bool tq = a.tqplus;
+  for (; grp < n_groups; grp += g_step) {
+    cp_async_wait_all();
+    __syncwarp();
+
+    // Norms: lane 8j + c runs chain c of row j (encode.cpp:16-26).
+    float nrm_lane;
+    {
+      const int j = min(lane >> 3, ROWS - 1), c = lane & 7;
+      const float* xr = rows + j * L.stride + c;
+      float s = 0.f;
+      const int steps = dim >> 3;
+      int t = 0;
+      for (; t + 4 <= steps; t += 4) {
+        const float v0 = xr[8 * t], v1 = xr[8 * t + 8], v2 = xr[8 * t + 16], v3 = xr[8 * t + 24];
+        s = __fmaf_rn(v0, v0, s);
+        s = __fmaf_rn(v1, v1, s);
+        s = __fmaf_rn(v2, v2, s);
+        s = __fmaf_rn(v3, v3, s);
+      }
+      for (; t < steps; ++t) {
+        const float v = xr[8 * t];
+        s = __fmaf_rn(v, v, s);
+      }
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 1));
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 2));
+      s = __fadd_rn(s, __shfl_xor_sync(full_mask(), s, 4));
+      nrm_lane = __fsqrt_rn(s);
+    }
+
+    const long long next = grp + g_step;
+#pragma unroll 1
+    for (int j = 0; j < ROWS; ++j) {
+      const long long v = grp * ROWS + j;
+      const float nrm = __shfl_sync(full_mask(), nrm_lane, 8 * j);
+      if (v >= a.n) break;
+      const float inv = (nrm > kMinInputNorm) ? __fdiv_rn(1.f, nrm) : 0.f;
+      const uint32_t inv_bits = __float_as_uint(inv);
+
+      // Gather y = (x[perm[i]] * inv) * sign[i] (rotation.cpp:185-205).
+      float y[R];
+      {
+        const unsigned char* xb = reinterpret_cast<const unsigned char*>(rows + j * L.stride);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const uint32_t e = s_src[r * 32 + lane];
+          const float xv = *reinterpret_cast<const float*>(xb + (e & 0x7fffffffu));
+          y[r] = __uint_as_float(__float_as_uint(__fmul_rn(xv, __uint_as_float(inv_bits))) ^ (e & 0x80000000u));
+        }
+      }
+      __syncwarp();
+      // The slot is free: bring in this warp's row j of its next group.
+      if (next < n_groups && next * ROWS + j < a.n) prefetch(next * ROWS + j, j);
+      cp_async_commit();
+
+      // Walsh-Hadamard butterflies, strides 1, 2, 4, ... < block (rotation.cpp:38-85).
+      const int block = a.block;
+#pragma unroll
+      for (int s = 1; s < E; s <<= 1) {
+        if (s < block) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if ((r & s) == 0) {
+              const float p = y[r], q = y[r | s];
+              y[r] = __fadd_rn(p, q);
+              y[r | s] = __fsub_rn(p, q);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int m = 1; m < 32; m <<= 1) {
+        if (m * E < block) {
+          const float sgn = (lane & m) ? -1.f : 1.f;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const float o = __shfl_xor_sync(full_mask(), y[r], m);
+            y[r] = __fmaf_rn(sgn, y[r], o);  // lower lane: y + o; upper lane: o - y
+          }
+        }
+      }
+#pragma unroll
+      for (int sg = 1; sg < SEG; sg <<= 1) {
+        if (32 * E * sg < block) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int seg = r / E;
+            if ((seg & sg) == 0 && (seg | sg) < SEG) {
+              const float p = y[r], q = y[r + sg * E];
+              y[r] = __fadd_rn(p, q);
+              y[r + sg * E] = __fsub_rn(p, q);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) y[r] = __fmul_rn(y[r], a.inv_sqrt_block);
+
+      // Codes, packed runs, inner-product estimate (encode.cpp:112-157).
+      double est = 0.0, mag = 0.0;
+      uint8_t* flat_row = a.out_flat + v * static_cast<long long>(a.flat_stride);
+#pragma unroll
+      for (int sgi = 0; sgi < SEG; ++sgi) {
+        Run run = 0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int r = sgi * E + e;
+          unsigned code;
+          double term;
+          if (tq) {
+            const float2 ss = s_ss[r * 32 + lane];
+            const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
+            code = pipe_code<BITS>(c, s_bnd);
+            const double2 bk = s_bk[r * 32 + lane];
+            const double back = __dsub_rn(__dmul_rn(s_cen[code], bk.x), bk.y);
+            term = __dmul_rn(static_cast<double>(y[r]), back);
+          } else {
+            code = pipe_code<BITS>(y[r], s_bnd);
+            term = __dmul_rn(static_cast<double>(y[r]), s_cen[code]);
+          }
+          est = __dadd_rn(est, term);
+          mag = __dadd_rn(mag, fabs(term));
+          // codes_flat: CPB codes per byte, first code in the high bits (pack.cpp:70-131)
+          const int byte = e / CPB, slot = e % CPB;
+          run |= static_cast<Run>(code) << (8 * byte + FIELD * (CPB - 1 - slot));
+        }
+        const int i0 = sgi * 32 * E + lane * E;
+        if (i0 < dim) *reinterpret_cast<Run*>(flat_row + i0 / CPB) = run;
+      }
+      est = warp_sum_d(est);
+      mag = warp_sum_d(mag);
+
+      float alpha = 0.f;
+      bool above = false;
+      float inner_f = 0.f;
+      const int nc = (dim + 3) / 4;
+      if (decide_float_of_sum(est, mag, nc + 2 + R + 6, kDegenerateInner, &above, &inner_f)) {
+        alpha = above ? __fdiv_rn(nrm, inner_f) : 0.f;
+      } else {
+        // Exact replay of the reference's four sequential double chains
+        // (chain i % 4, one fused multiply-add per term, encode.cpp:117-156).
+        // Chain c visits its elements in index order; a lane holds E
+        // consecutive elements of a segment, so each chain's running value
+        // passes from lane to lane (a shuffle per lane), segment after segment.
+        double ch[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int sgi = 0; sgi < SEG; ++sgi) {
+#pragma unroll 1
+          for (int l = 0; l < 32; ++l) {
+            if (lane == l) {
+#pragma unroll
+              for (int e = 0; e < E; ++e) {
+                const int r = sgi * E + e;
+                if (pipe_elem<E>(r, lane) < dim) {
+                  double back;
+                  if (tq) {
+                    const float2 ss = s_ss[r * 32 + lane];
+                    const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
+                    const unsigned code = pipe_code<BITS>(c, s_bnd);
+                    const double2 bk = s_bk[r * 32 + lane];
+                    back = __dsub_rn(__dmul_rn(s_cen[code], bk.x), bk.y);
+                  } else {
+                    back = s_cen[pipe_code<BITS>(y[r], s_bnd)];
+                  }
+                  ch[e & 3] = __fma_rn(static_cast<double>(y[r]), back, ch[e & 3]);
+                }
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) ch[c] = __shfl_sync(full_mask(), ch[c], l);
+          }
+        }
+        const double inner = __dadd_rn(__dadd_rn(ch[0], ch[1]), __dadd_rn(ch[2], ch[3]));
+        alpha = inner > kDegenerateInner ? __fdiv_rn(nrm, __double2float_rn(inner)) : 0.f;
+        if (lane == 0 && a.replay_count) atomicAdd(a.replay_count, 1ull);
+      }
+      if (lane == 0) a.out_alpha[v] = alpha;
+    }
+  }
+  cp_async_wait_all();
+}
+
+// (R, E) of the pipelined kernel for a dim, or false when no instantiated
+// layout fits (those dims use encode_rows_kernel).
+bool pipe_shape(int dim, int* r_out, int* e_out) {
+  static const int shapes[][2] = {{4, 4}, {8, 8}, {12, 4}, {16, 16}, {24, 8}, {32, 16}, {48, 16}, {64, 16}};
+  for (const auto& sh : shapes) {
+    const int r = sh[0], e = sh[1];
+    // every element has a slot, and no lane's run of E codes crosses dim
+    if (32 * r < dim || dim % e != 0) continue;
+    *r_out = r;
+    *e_out = e;
+    return true;
+  }
+  return false;
+}
+
+template <int R, int E, int BITS, int ROWS, int MAXW>
+cudaError_t launch_pipe_t(const EncodeArgs& a, int sms, int max_smem, cudaStream_t stream) {
+  int warps = MAXW;
+  while (warps > 1 && pipe_layout(a.dim, R, a.tqplus, warps, ROWS).total > static_cast<size_t>(max_smem)) --warps;
+  const size_t smem = pipe_layout(a.dim, R, a.tqplus, warps, ROWS).total;
+  if (smem > static_cast<size_t>(max_smem)) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(encode_pipe_kernel<R, E, BITS, ROWS, MAXW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  const long long groups = (a.n + ROWS - 1) / ROWS;
+  long long ctas = (groups + warps - 1) / warps;
+  if (ctas > sms) ctas = sms;
+  encode_pipe_kernel<R, E, BITS, ROWS, MAXW><<<static_cast<unsigned>(ctas), warps * 32, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int R, int E, int ROWS, int MAXW>
+cudaError_t launch_pipe_bits(const EncodeArgs& a, int sms, int max_smem, cudaStream_t stream) {
+  switch (a.bits) {
+    case 2: return launch_pipe_t<R, E, 2, ROWS, MAXW>(a, sms, max_smem, stream);
+    case 3: return launch_pipe_t<R, E, 3, ROWS, MAXW>(a, sms, max_smem, stream);
+    case 4: return launch_pipe_t<R, E, 4, ROWS, MAXW>(a, sms, max_smem, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 int rows_template(int dim) {
   const int need = (dim + kWarp - 1) / kWarp;
   const int options[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64};
@@ -337,6 +706,21 @@ bool encode_dim_supported(int dim) { return dim > 0 && dim <= 16384; }
 cudaError_t launch_encode(const EncodeArgs& a, int sms, cudaStream_t stream) {
   if (a.n == 0) return cudaSuccess;
   if (a.dim > kRegisterRowMaxDim) return launch_encode_big(a, sms, stream);
+  int pr = 0, pe = 0;
+  if (pipe_shape(a.dim, &pr, &pe)) {
+    int device = 0, max_smem = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) return e;
+#define VCB_PIPE(RR, EE)                                                                            \
+    if (pr == RR && pe == EE) {                                                                     \
+      return launch_pipe_bits<RR, EE, (RR <= 32 ? 4 : 2), (RR <= 24 ? 16 : (RR == 32 ? 12 : (RR == 48 ? 14 : 10)))>( \
+          a, sms, max_smem, stream);                                                                \
+    }
+    VCB_PIPE(4, 4) VCB_PIPE(8, 8) VCB_PIPE(12, 4) VCB_PIPE(16, 16) VCB_PIPE(24, 8) VCB_PIPE(32, 16)
+    VCB_PIPE(48, 16) VCB_PIPE(64, 16)
+#undef VCB_PIPE
+  }
   const int r = rows_template(a.dim);
   const size_t smem = encode_smem_bytes(a.dim, a.tqplus);
   const int grid = grid_for_quads(a.n, sms);
