@@ -48,6 +48,14 @@ struct BucketScratch {
       cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount, encs;
   FlatScratchStore flat;
   ProbeScratch probe;
+  void bind(ScratchArena* a) {
+    for (DeviceBuffer* b : {&qh, &route, &top_s, &top_i, &counts, &fill, &pstart, &istart, &pairs, &off, &items,
+                            &nitems, &cand_s, &cand_i, &rr_s, &rr_i, &np, &floor, &fl_s, &fl_i, &acount, &encs}) {
+      b->bind(a);
+    }
+    flat.bind(a);
+    probe.bind(a);
+  }
 };
 }  // namespace vcb
 
@@ -427,6 +435,7 @@ struct tq_bucketed {
       const uint32_t* np_pass = d_np ? d_np + q0 : nullptr;
       if (lp) {
         sc.np.reserve(m * 4);
+        vcb::probe_reserve(lp->mlp, m, sc.probe);
         eng->launch(tq_index::kPrep, s, "probe network", [&] {
           vcb::probe_predict(lp->mlp, sc.top_s.as<float>(), m, ptop, lp->coverage, lp->min_confidence,
                              static_cast<uint32_t>(max_probe), sc.np.as<uint32_t>(), s, sc.probe);
@@ -497,7 +506,7 @@ struct tq_bucketed {
       // Every (query, probe, tile set) appends its kept candidates to the
       // query's region; the merges read exactly those.
       sc.acount.reserve(m * 4);
-      vcb::check(cudaMemsetAsync(sc.acount.get(), 0, m * 4, s), "cudaMemsetAsync");
+      if (!vcb::dry_run_flag()) vcb::check(cudaMemsetAsync(sc.acount.get(), 0, m * 4, s), "cudaMemsetAsync");
       ba.append_count = sc.acount.as<uint32_t>();
       // The best-routed buckets first: the k-th best score over a query's
       // first 8 (32 from 128 probes) probes is a lower bound of its k-th best over all
@@ -599,7 +608,7 @@ struct tq_bucketed {
                                           d_ids + q0 * ke, s);
         });
       }
-      eng->scan_queries += m;
+      if (!vcb::dry_run_flag()) eng->scan_queries += m;
       if (trace_off) {
         vcb::check(cudaMemcpyAsync(trace_off + q0 * max_probe, sc.off.get(), m * max_probe * 4,
                                    cudaMemcpyDeviceToHost, s), "D2H");

@@ -28,6 +28,11 @@ namespace vcb {
 
 thread_local std::string g_last_error;
 
+bool& dry_run_flag() {
+  static thread_local bool flag = false;
+  return flag;
+}
+
 void calibrate_index(tq_index* h, const float* d_sample, size_t n, cudaStream_t s) {
   require(n >= 2, TQ_ERR_INVALID_ARGUMENT, "calibration needs at least 2 rows");
   require(!h->prepared && h->n == 0, TQ_ERR_STATE, "calibrate must precede prepare()");

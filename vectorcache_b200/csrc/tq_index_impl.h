@@ -24,7 +24,45 @@ inline void check(cudaError_t e, const char* what) {
   throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Grow-only device allocation.
+// Sizing pass of a search (serving admission): while set on the calling
+// thread, tq_index::launch and the other device calls of the search paths do
+// nothing, and scratch buffers bound to a measuring arena only count bytes.
+bool& dry_run_flag();
+
+// A region of device memory that scratch buffers bound to it draw from in
+// order (bump allocation; a buffer that grows abandons its old piece). In
+// measure mode it hands out placeholder addresses that nothing dereferences
+// and only counts the bytes, so a dry run of a search through the same host
+// code yields exactly the region size the real run needs.
+struct ScratchArena {
+  static constexpr size_t kAlign = 256;
+  unsigned char* base = nullptr;
+  size_t size = 0, used = 0;
+  bool measure = false;
+
+  static size_t piece(size_t bytes) { return (std::max<size_t>(bytes, 16) + kAlign - 1) / kAlign * kAlign; }
+  void* take(size_t bytes) {
+    const size_t b = piece(bytes);
+    if (!measure && used + b > size) {
+      throw Error(TQ_ERR_OUT_OF_MEMORY, "serving scratch region exhausted (" + std::to_string(used + b) +
+                                            " of " + std::to_string(size) + " bytes)");
+    }
+    void* p = measure ? reinterpret_cast<void*>(kPlaceholder + used) : static_cast<void*>(base + used);
+    used += b;
+    return p;
+  }
+  void reset(unsigned char* b, size_t n, bool m) {
+    base = b;
+    size = n;
+    used = 0;
+    measure = m;
+  }
+
+ private:
+  static constexpr uintptr_t kPlaceholder = uintptr_t{1} << 44;
+};
+
+// Grow-only device allocation: cudaMalloc, or a piece of a bound ScratchArena.
 class DeviceBuffer {
  public:
   DeviceBuffer() = default;
@@ -36,18 +74,28 @@ class DeviceBuffer {
     if (bytes <= bytes_ && ptr_) return ptr_;
     release();
     if (bytes == 0) bytes = 16;
-    check(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    if (arena_) {
+      ptr_ = arena_->take(bytes);
+    } else {
+      check(cudaMalloc(&ptr_, bytes), "cudaMalloc");
+    }
     bytes_ = bytes;
     return ptr_;
   }
   void release() {
-    if (ptr_) cudaFree(ptr_);
+    if (ptr_ && !arena_) cudaFree(ptr_);
     ptr_ = nullptr;
     bytes_ = 0;
+  }
+  // Later reserves draw from `a` (nullptr: cudaMalloc again); drops the current storage.
+  void bind(ScratchArena* a) {
+    release();
+    arena_ = a;
   }
   void swap(DeviceBuffer& o) noexcept {
     std::swap(ptr_, o.ptr_);
     std::swap(bytes_, o.bytes_);
+    std::swap(arena_, o.arena_);
   }
   void* get() const { return ptr_; }
   size_t bytes() const { return bytes_; }
@@ -59,6 +107,7 @@ class DeviceBuffer {
  private:
   void* ptr_ = nullptr;
   size_t bytes_ = 0;
+  ScratchArena* arena_ = nullptr;
 };
 
 class DeviceGuard {
@@ -96,6 +145,9 @@ struct FlatScratchStore {
   DeviceBuffer luts, qf, cand_s, cand_i, partial;
   long long range_cap = 0;  // see FlatScratch::range_cap
   FlatScratch ref() { return {&luts, &qf, &cand_s, &cand_i, &partial, range_cap}; }
+  void bind(ScratchArena* a) {
+    for (DeviceBuffer* b : {&luts, &qf, &cand_s, &cand_i, &partial}) b->bind(a);
+  }
 };
 
 }  // namespace vcb
@@ -161,9 +213,11 @@ struct tq_index {
     return e;
   }
 
-  // Runs one kernel launch, bracketed by events when profiling is on.
+  // Runs one kernel launch, bracketed by events when profiling is on; a
+  // sizing pass (vcb::dry_run_flag) launches nothing.
   template <typename F>
   void launch(int kind, cudaStream_t s, const char* what, F&& fn) {
+    if (vcb::dry_run_flag()) return;
     ++launches[kind];
     if (!profiling) {
       vcb::check(fn(), what);
@@ -336,8 +390,10 @@ struct tq_index {
         a.partial_batches = plan.split_batches;
       }
       launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
-      scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
-      scan_queries += m;
+      if (!vcb::dry_run_flag()) {
+        scan_stream_bytes += static_cast<uint64_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) * n * (nbg + 4);
+        scan_queries += m;
+      }
       vcb::MergeArgs mg{};
       mg.cand_score = a.cand_score;
       mg.cand_id = a.cand_id;

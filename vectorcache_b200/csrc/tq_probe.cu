@@ -424,16 +424,20 @@ struct tq_probe_mlp {
 
 namespace vcb {
 
-void probe_predict(tq_probe_mlp* h, const float* d_top, size_t m, int p, float coverage, float min_conf,
-                   uint32_t fallback, uint32_t* d_out, cudaStream_t s, ProbeScratch& sc) {
-  if (m == 0) return;
-  const long long M = static_cast<long long>(m);
+void probe_reserve(tq_probe_mlp* h, size_t m, ProbeScratch& sc) {
   int widest = 1;
   for (int l = 0; l < h->n_lin(); ++l) widest = std::max(widest, h->fan_out[l]);
   sc.x.reserve(m * kInputs * 2);
   sc.z.reserve(m * widest * 4);
   sc.act0.reserve(m * widest * 2);
   sc.act1.reserve(m * widest * 2);
+}
+
+void probe_predict(tq_probe_mlp* h, const float* d_top, size_t m, int p, float coverage, float min_conf,
+                   uint32_t fallback, uint32_t* d_out, cudaStream_t s, ProbeScratch& sc) {
+  if (m == 0) return;
+  const long long M = static_cast<long long>(m);
+  probe_reserve(h, m, sc);
   features_kernel<<<static_cast<unsigned>(m), 256, 0, s>>>(d_top, M, p, h->d_mu.as<float>(), h->d_isd.as<float>(),
                                                            sc.x.as<bf16>(), nullptr);
   check(cudaGetLastError(), "features kernel");

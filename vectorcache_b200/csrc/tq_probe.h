@@ -14,7 +14,13 @@ namespace vcb {
 
 struct ProbeScratch {
   DeviceBuffer x, z, act0, act1;
+  void bind(ScratchArena* a) {
+    for (DeviceBuffer* b : {&x, &z, &act0, &act1}) b->bind(a);
+  }
 };
+
+// Grows sc to what probe_predict needs for m queries (no device work).
+void probe_reserve(tq_probe_mlp* h, size_t m, ProbeScratch& sc);
 
 // n_probe for m queries from their top routing scores (row stride p; the first
 // min(p, 256) columns are used), written to d_out; queued on s. Same decision
