@@ -438,6 +438,12 @@ def run_ours(args, world, rank, local):
     exact = exact_topk(db, q[:nr], 10)
     exact_np = exact.cpu().numpy()
     recall10 = recall_at(d_ids[:nr].cpu().numpy(), exact_np, min(10, k))
+    keep_rows = world == 1 and not (args.no_variants and args.no_cpu_baseline)
+    if not keep_rows:
+        # Nothing later reads the float rows: free them, so a profiler run of
+        # this command holds only the index and the queries on the device.
+        del db
+        torch.cuda.empty_cache()
 
     for _ in range(args.warmup):
         step()
@@ -550,7 +556,7 @@ def run_ours(args, world, rank, local):
     # The other (bits, k) points of the same data: device-timed QPS, Recall@10,
     # and their top-k for the reference comparison below.
     variants = []
-    if world == 1 and not args.no_variants:
+    if keep_rows and not args.no_variants:
         second = {}
         with ClockSampler(local) as clk_var:
             for bits, kv in VARIANTS:
@@ -581,7 +587,7 @@ def run_ours(args, world, rank, local):
     cpu_base = None
     parity = None
     ref_gpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and keep_rows and not args.no_cpu_baseline:
         try:
             db_h = db.cpu().numpy()
             q_h = q.cpu().numpy()
@@ -663,7 +669,7 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    for extra in (second.values() if world == 1 and not args.no_variants else ()):
+    for extra in (second.values() if keep_rows and not args.no_variants else ()):
         extra.close()
     index.close()
 

@@ -371,16 +371,20 @@ int tq_bucketed_search_learned_device(tq_bucketed* h, const float* d_queries, si
 /* ---- serving loop -------------------------------------------------------------
  * No counterpart in the reference (its tools time single synchronous calls).
  * Continuous batching over resident indexes on one GPU: requests wait in a
- * FIFO queue; whenever one of the server's slots (own CUDA stream, pinned
- * staging, device buffers and search scratch) is free, the oldest request is
- * launched together with every later waiting request for the same index, k
- * and n_probe, up to max_batch queries. Batches in different slots overlap on
- * the device. start() creates slots only while the device memory in use
- * (resident indexes included) stays within hbm_budget_bytes, and grows each
- * slot's scratch by one full-size warm-up search per index, so serving
- * allocates no device memory. A query's result does not depend on the other
- * queries of its batch. Host buffers of a request must stay valid until
- * tq_server_wait returns for it. */
+ * FIFO queue; whenever one of the server's max_slots slots (own CUDA streams,
+ * pinned staging, device query / result buffers) is free, the oldest request
+ * forms a batch with every later waiting request for the same index, k and
+ * n_probe, up to max_batch queries. The batch's search scratch is sized
+ * exactly on the host (a dry run of the search code) and taken from one
+ * device arena: start() sizes the arena to what hbm_budget_bytes leaves after
+ * the resident indexes, kernels and slot buffers (at most max_slots full
+ * batches' worth, at least one, else TQ_ERR_OUT_OF_MEMORY). A batch whose
+ * scratch does not fit waits, with the requests behind it, until running
+ * batches return theirs: requests are admitted as slots and memory free up,
+ * and batches in different slots overlap on the device. Serving allocates no
+ * device memory. A query's result does not depend on the other queries of its
+ * batch. Host buffers of a request must stay valid until tq_server_wait
+ * returns for it. */
 typedef struct tq_server tq_server;
 
 int tq_server_create(int device, size_t hbm_budget_bytes, size_t max_slots, size_t max_batch,
@@ -393,7 +397,17 @@ int tq_server_add_flat(tq_server* h, tq_index* index, size_t max_k, int* target)
 int tq_server_add_bucketed(tq_server* h, tq_bucketed* index, size_t max_k, size_t max_probe,
                            tq_probe_mlp* mlp, float coverage, float min_confidence, int* target);
 int tq_server_start(tq_server* h);
+/* slot_bytes: one slot's fixed device buffers; resident_bytes: device memory
+ * in use at start() before the scratch arena (indexes, kernels, slots). */
 int tq_server_info(tq_server* h, size_t* n_slots, size_t* slot_bytes, size_t* resident_bytes);
+/* The scratch arena: its size, the most of it in use at once, the largest
+ * scratch of any admissible batch, and how many batches had to wait for
+ * arena memory. */
+int tq_server_memory(tq_server* h, size_t* arena_bytes, size_t* arena_peak, size_t* max_batch_bytes,
+                     uint64_t* memory_waits);
+/* Scratch bytes a batch of nq queries of `target` with this k and n_probe
+ * takes from the arena (the server's own sizing, on the host). */
+int tq_server_batch_bytes(tq_server* h, int target, size_t nq, size_t k, size_t n_probe, size_t* bytes);
 /* Queue a request (nq <= max_batch host rows); scores/ids receive nq x k_eff. */
 int tq_server_submit(tq_server* h, int target, const float* queries, size_t nq, size_t k,
                      size_t n_probe, float* scores, uint64_t* ids, uint64_t* request);

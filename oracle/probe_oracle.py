@@ -3,8 +3,8 @@
 The MLP has no counterpart in the reference, so this checker is not pinned to
 reference code: it restates the network's definition (vectorcache_b200
 tq_probe.cu) in float64 numpy with the same bf16 rounding points — inputs,
-weights and hidden activations are rounded to bf16 exactly where the GPU
-rounds them — and computes the mean loss of either training objective
+weights, hidden activations and the dZ operands of the backward products are
+rounded to bf16 exactly where the GPU rounds them — and computes the mean loss of either training objective
 (softmax cross-entropy on labels, or per-class sigmoid cross-entropy on
 recall targets) and its gradients by explicit backpropagation. Also the
 prediction rules. Only tests/ import it.
@@ -79,11 +79,13 @@ def forward_backward(x: np.ndarray, params: np.ndarray, shapes, labels: np.ndarr
     grads = []
     for li in range(len(layers) - 1, -1, -1):
         w, _ = layers[li]
-        gw = acts[li].T @ dz
+        # the products take dZ rounded to bf16 (from fp32); the bias gradient sums dZ itself
+        dzr = rnd(dz.astype(np.float32)).astype(np.float64) if rounding else dz
+        gw = acts[li].T @ dzr
         gb = dz.sum(axis=0)
         grads.append((gw, gb))
         if li > 0:
-            da = dz @ rnd(w).astype(np.float64).T
+            da = dzr @ rnd(w).astype(np.float64).T
             dz = da * (zs[li - 1] > 0)
     grads.reverse()
     flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads])

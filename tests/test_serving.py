@@ -1,7 +1,8 @@
 """Serving loop (continuous batching) on the GPU: every request's result is the
 same as the same search run alone, whatever it was batched or overlapped with;
 an open-loop Poisson replay completes with sane latencies; the learned probe
-runs inside the server; the HBM budget bounds the number of slots."""
+runs inside the server; a batch whose scratch does not fit the HBM budget's
+arena waits until running batches free theirs."""
 import numpy as np
 import pytest
 
@@ -114,23 +115,65 @@ def test_learned_probe_in_the_server(indexes):
     mlp.close()
 
 
-def test_budget_bounds_the_slots(indexes):
+def test_requests_wait_for_memory_and_run_when_it_frees(indexes):
+    # The HBM budget leaves scratch for about 1.5 full batches, with four slots
+    # free: of two full batches submitted together, the second waits for the
+    # first one's scratch, then runs. Both equal the same search alone.
     flat, bkt, db, xb = indexes
-    probe = vcb.Server(max_slots=1, max_batch=8192)
-    probe.add_flat(flat, 64)
-    probe.start()
-    inf = probe.info()
-    probe.close()
-    assert inf["slot_bytes"] > (8 << 20)  # LUTs alone: 8192 x 64 x 32 bytes
-    # room for about 2.5 slots: the server stops at 1 to 3 of the 8 allowed
-    srv = vcb.Server(hbm_budget_bytes=inf["resident_bytes"] + int(2.5 * inf["slot_bytes"]), max_slots=8,
-                     max_batch=8192)
-    srv.add_flat(flat, 64)
+    roomy = vcb.Server(max_slots=4, max_batch=4096)
+    fid = roomy.add_flat(flat, 64)
+    roomy.start()
+    resident = roomy.info()["resident_bytes"]
+    need = roomy.batch_bytes(fid, 4096, 64)
+    mem = roomy.memory()
+    roomy.close()
+    assert need > (32 << 20) and mem["max_batch_bytes"] >= need
+    srv = vcb.Server(hbm_budget_bytes=resident + need + need // 2, max_slots=4, max_batch=4096)
+    fid = srv.add_flat(flat, 64)
     srv.start()
-    assert 1 <= srv.info()["slots"] <= 3
+    arena = srv.memory()["arena_bytes"]
+    assert need <= arena < 2 * srv.batch_bytes(fid, 4096, 63)
+    rng = np.random.default_rng(9)
+    qa = db[rng.integers(0, db.shape[0], 4096)] + rng.normal(0, 0.01, (4096, 128)).astype(np.float32)
+    qb = db[rng.integers(0, db.shape[0], 4096)] + rng.normal(0, 0.01, (4096, 128)).astype(np.float32)
+    # different k: two batches, submitted back to back
+    lat, wall, results = srv.replay([(0.0, fid, qa, 64, 0), (0.0, fid, qb, 63, 0)])
+    mem = srv.memory()
+    assert mem["memory_waits"] >= 1
+    assert mem["arena_peak"] <= mem["arena_bytes"] and mem["arena_peak"] < 2 * need
+    assert lat[1] > lat[0]
+    for (q, k), (s, i) in zip(((qa, 64), (qb, 63)), results):
+        want = flat.search(q, k)
+        assert np.array_equal(i, want.ids) and bits_equal(s, want.scores)
+    assert srv.stats()["completed"] == 2
     srv.close()
     tiny = vcb.Server(hbm_budget_bytes=1 << 20, max_slots=2, max_batch=256)
     tiny.add_flat(flat, 10)
     with pytest.raises(vcb.TurboQuantError):
         tiny.start()
     tiny.close()
+
+
+def test_batch_sizing_matches_what_runs(indexes):
+    # The arena piece of a batch is its exact scratch: batches of every size,
+    # k and n_probe run inside their pieces (a piece too small fails the
+    # batch), and the sizing of a full batch bounds all smaller ones tried.
+    flat, bkt, db, xb = indexes
+    srv = vcb.Server(max_slots=2, max_batch=512)
+    fid = srv.add_flat(flat, 64)
+    bid = srv.add_bucketed(bkt, 64, 32)
+    srv.start()
+    top = srv.memory()["max_batch_bytes"]
+    rng = np.random.default_rng(4)
+    for _ in range(24):
+        target = int(rng.integers(0, 2))
+        nq = int(rng.choice([1, 2, 3, 17, 200, 512]))
+        k = int(rng.choice([1, 10, 33, 64]))
+        npb = int(rng.choice([4, 32]))
+        assert 0 < srv.batch_bytes(target, nq, k, npb) <= top
+        src = db if target == fid else xb
+        q = src[rng.integers(0, src.shape[0], nq)]
+        s, i, _ = srv.submit(target, q, k, npb if target == bid else 0).wait()
+        want = _alone(flat, bkt, target, fid, q, k, npb)
+        assert np.array_equal(i, want.ids)
+    srv.close()

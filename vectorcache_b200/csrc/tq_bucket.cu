@@ -98,25 +98,123 @@ __device__ __forceinline__ void tile_product(GemmTile& t, const float* __restric
   }
 }
 
-__global__ void __launch_bounds__(256) gemm_nt_kernel(const float* __restrict__ A, long long m,
-                                                      const float* __restrict__ B, long long nb, int dim,
-                                                      float* __restrict__ C, long long ldc) {
-  __shared__ __align__(16) GemmTile t;
-  const long long r0 = static_cast<long long>(blockIdx.y) * kTile;
-  const long long c0 = static_cast<long long>(blockIdx.x) * kTileB;
-  float acc[8][4];
-  tile_product(t, A, m, B, nb, dim, r0, c0, acc);
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+// ---------------------------------------------------------------------------
+// Routing and offset products on the tensor cores (mma.sync m16n8k8 TF32,
+// fp32 accumulation) in 3xTF32 form (Markidis et al., "NVIDIA Tensor Core
+// Programmability, Performance & Precision", IPDPSW 2018): each fp32 operand
+// splits as x = hi + lo with hi = tf32(x) and lo = tf32(x - hi), and a product
+// is accumulated as lo_a*hi_b + hi_a*lo_b + hi_a*hi_b, about 2^-21 relative
+// per product, well inside the 1e-5 the routing scores are checked to against
+// fp64. A CTA of 8 warps (4 along A's rows x 2 along B's rows) computes a
+// 128 x 64 tile of C; every warp a 32 x 32 piece: 2 x 4 m16n8 tiles.
+// ---------------------------------------------------------------------------
+constexpr int kTcM = 128, kTcN = 64, kTcK = 32, kTcPad = 4;
+
+struct TcTile {
+  float a[kTcM][kTcK + kTcPad];  // rows of A, coordinates k0 .. k0+31
+  float b[kTcN][kTcK + kTcPad];  // rows of B
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(__fsub_rn(x, __uint_as_float(hi)));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(256) gemm_nt_tc_kernel(const float* __restrict__ A, long long m,
+                                                         const float* __restrict__ B, long long nb, int dim,
+                                                         float* __restrict__ C, long long ldc) {
+  __shared__ __align__(16) TcTile t;
+  const long long r0 = static_cast<long long>(blockIdx.y) * kTcM;
+  const long long c0 = static_cast<long long>(blockIdx.x) * kTcN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp & 3, wn = warp >> 2;  // warp's 32 x 32 piece
+  const int g = lane >> 2, q = lane & 3;    // mma group and thread in group
+  float acc[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const long long row = r0 + ty * 8 + i;
-    if (row >= m) continue;
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const long long col = c0 + tx * 4 + j;
-      if (col < nb) C[row * ldc + col] = acc[i][j];
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+  const bool vec = (dim % 4) == 0;
+  for (int k0 = 0; k0 < dim; k0 += kTcK) {
+    __syncthreads();
+    // Stage A (128 x 32) and B (64 x 32), zero outside the matrices.
+    for (int e = threadIdx.x; e < (kTcM + kTcN) * (kTcK / 4); e += blockDim.x) {
+      const int row = e / (kTcK / 4), c4 = (e % (kTcK / 4)) * 4;
+      const bool is_a = row < kTcM;
+      const long long src_row = is_a ? r0 + row : c0 + (row - kTcM);
+      const long long rows = is_a ? m : nb;
+      const float* src = is_a ? A : B;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int col = k0 + c4;
+      if (src_row < rows) {
+        const float* p = src + src_row * dim + col;
+        if (vec && col + 4 <= dim) {
+          v = *reinterpret_cast<const float4*>(p);
+        } else {
+          v.x = col < dim ? p[0] : 0.f;
+          v.y = col + 1 < dim ? p[1] : 0.f;
+          v.z = col + 2 < dim ? p[2] : 0.f;
+          v.w = col + 3 < dim ? p[3] : 0.f;
+        }
+      }
+      float* dst = is_a ? &t.a[row][c4] : &t.b[row - kTcM][c4];
+      *reinterpret_cast<float4*>(dst) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kTcK; kk += 8) {
+      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm * 32 + i * 16 + g;
+        split_tf32(t.a[r][kk + q], ah[i][0], al[i][0]);
+        split_tf32(t.a[r + 8][kk + q], ah[i][1], al[i][1]);
+        split_tf32(t.a[r][kk + q + 4], ah[i][2], al[i][2]);
+        split_tf32(t.a[r + 8][kk + q + 4], ah[i][3], al[i][3]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = wn * 32 + j * 8 + g;
+        split_tf32(t.b[n][kk + q], bh[j][0], bl[j][0]);
+        split_tf32(t.b[n][kk + q + 4], bh[j][1], bl[j][1]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma_tf32(acc[i][j], al[i], bh[j]);
+          mma_tf32(acc[i][j], ah[i], bl[j]);
+          mma_tf32(acc[i][j], ah[i], bh[j]);
+        }
     }
   }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const long long row = r0 + wm * 32 + i * 16 + g + (e >> 1) * 8;
+        const long long col = c0 + wn * 32 + j * 8 + 2 * q + (e & 1);
+        if (row < m && col < nb) C[row * ldc + col] = acc[i][j][e];
+      }
 }
 
 __global__ void __launch_bounds__(256) assign_kernel(const float* __restrict__ A, long long m,
@@ -1405,9 +1503,9 @@ cudaError_t launch_normalize_rows(const float* x, long long n, int dim_in, int d
 cudaError_t launch_gemm_nt(const float* A, long long m, const float* B, long long nb, int dim, float* C,
                            long long ldc, cudaStream_t stream) {
   if (m == 0 || nb == 0) return cudaSuccess;
-  dim3 grid(static_cast<unsigned>((nb + kTileB - 1) / kTileB), static_cast<unsigned>((m + kTile - 1) / kTile));
+  dim3 grid(static_cast<unsigned>((nb + kTcN - 1) / kTcN), static_cast<unsigned>((m + kTcM - 1) / kTcM));
   if (grid.y > 65535) return cudaErrorInvalidValue;
-  gemm_nt_kernel<<<grid, 256, 0, stream>>>(A, m, B, nb, dim, C, ldc);
+  gemm_nt_tc_kernel<<<grid, 256, 0, stream>>>(A, m, B, nb, dim, C, ldc);
   return cudaGetLastError();
 }
 

@@ -31,13 +31,14 @@ constexpr double kFixedScale = 4294967296.0;  // 2^32
 cudaError_t launch_normalize_rows(const float* x, long long n, int dim_in, int dim, float* out,
                                   cudaStream_t stream);
 
-// C (m x nb, row stride ldc) = A (m x dim) . B (nb x dim)^T in fp32 with fused
-// multiply-add accumulation over the coordinates in order.
+// C (m x nb, row stride ldc) = A (m x dim) . B (nb x dim)^T of fp32 rows on the
+// tensor cores: 3xTF32 products (split hi/lo TF32 operands), fp32
+// accumulation, about 2^-21 relative per product.
 cudaError_t launch_gemm_nt(const float* A, long long m, const float* B, long long nb, int dim, float* C,
                            long long ldc, cudaStream_t stream);
 
 // Per row of A: the column of the largest A.B^T entry (ties: lower column) and
-// its value. Same arithmetic as launch_gemm_nt.
+// its value, in fp32 fused multiply-adds over the coordinates in order.
 cudaError_t launch_assign(const float* A, long long m, const float* B, long long nb, int dim,
                           uint32_t* label, float* best, cudaStream_t stream);
 

@@ -1006,6 +1006,7 @@ namespace vcb {
 
 BucketScratch* bucket_scratch_new() { return new BucketScratch(); }
 void bucket_scratch_delete(BucketScratch* sc) { delete sc; }
+void bucket_scratch_bind(BucketScratch* sc, ScratchArena* a) { sc->bind(a); }
 
 size_t bucketed_dim_in(const tq_bucketed* h) { return h->dim_in; }
 size_t bucketed_size(const tq_bucketed* h) { return h->n; }

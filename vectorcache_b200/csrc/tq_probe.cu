@@ -83,61 +83,85 @@ __global__ void features_kernel(const float* __restrict__ top, long long m, int 
   }
 }
 
-// C (M x N, fp32, row stride ldc) = A (M x K) . B (K x N), fp32 accumulation in
-// coordinate order. Element (i, k) of A at A[i * a_r + k * a_c]; (k, j) of B at
-// B[k * b_r + j * b_c]. T x T tile per CTA (T = 64, or 32 when 64-wide tiles
-// would leave most SMs idle), (T/16)^2 per thread, 32 coordinates per
-// shared-memory stage. Every element is the same FMA chain for either T.
-template <typename TA, typename TB, int T>
-__global__ void __launch_bounds__(256) gemm_kernel(const TA* __restrict__ A, long long a_r, long long a_c,
-                                                   const TB* __restrict__ B, long long b_r, long long b_c,
-                                                   float* __restrict__ C, long long ldc, long long M, int N, int K) {
-  constexpr int R = T / 16;
-  __shared__ float sa[32][T + 1];
-  __shared__ float sb[32][T + 1];
+// C (M x N, fp32, row stride ldc) = A (M x K) . B (K x N) with bf16 operands on
+// the tensor cores (mma.sync m16n8k16, fp32 accumulation). Element (i, k) of
+// A at A[i * a_r + k * a_c]; (k, j) of B at B[k * b_r + j * b_c]. A T x T tile
+// per CTA of 4 warps (T = 64, or 32 when 64-wide tiles would leave most SMs
+// idle), each warp a (T/2) x (T/2) piece; 32 coordinates per shared-memory
+// stage, staged k-contiguous so every fragment register is one 32-bit load.
+template <int T>
+__global__ void __launch_bounds__(128) gemm_bf16_tc_kernel(const bf16* __restrict__ A, long long a_r, long long a_c,
+                                                           const bf16* __restrict__ B, long long b_r, long long b_c,
+                                                           float* __restrict__ C, long long ldc, long long M, int N,
+                                                           int K) {
+  constexpr int KC = 32, PAD = 8;          // PAD: rows 20 words apart, conflict-free fragment loads
+  constexpr int WT = T / 2;                // warp piece
+  constexpr int MI = WT / 16, NJ = WT / 8;  // m16 and n8 tiles per warp
+  __shared__ __align__(16) bf16 sa[T][KC + PAD];
+  __shared__ __align__(16) bf16 sb[T][KC + PAD];
   const long long i0 = static_cast<long long>(blockIdx.y) * T;
   const int j0 = blockIdx.x * T;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  float acc[R][R];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int g = lane >> 2, q = lane & 3;
+  float acc[MI][NJ][4];
 #pragma unroll
-  for (int a = 0; a < R; ++a)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int b = 0; b < R; ++b) acc[a][b] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += 32) {
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  const bf16 zero = __float2bfloat16_rn(0.f);
+  for (int k0 = 0; k0 < K; k0 += KC) {
     __syncthreads();
-    for (int e = threadIdx.x; e < T * 32; e += blockDim.x) {
-      const int r = e / 32, c = e % 32;
-      const long long gi = i0 + r;
+    for (int e = threadIdx.x; e < T * KC; e += blockDim.x) {
+      const int r = e / KC, c = e % KC;
       const int gk = k0 + c;
-      sa[c][r] = (gi < M && gk < K) ? ld(A, gi * a_r + gk * a_c) : 0.f;
-      const int gj = j0 + (e % T);
-      const int gk2 = k0 + e / T;
-      sb[e / T][e % T] = (gj < N && gk2 < K) ? ld(B, gk2 * b_r + static_cast<long long>(gj) * b_c) : 0.f;
+      const long long gi = i0 + r;
+      sa[r][c] = (gi < M && gk < K) ? A[gi * a_r + gk * a_c] : zero;
+      const int gj = j0 + r;
+      sb[r][c] = (gj < N && gk < K) ? B[gk * b_r + static_cast<long long>(gj) * b_c] : zero;
     }
     __syncthreads();
-#pragma unroll 8
-    for (int c = 0; c < 32; ++c) {
-      float av[R], bv[R];
 #pragma unroll
-      for (int a = 0; a < R; ++a) av[a] = sa[c][ty * R + a];
+    for (int kk = 0; kk < KC; kk += 16) {
+      uint32_t af[MI][4], bfr[NJ][2];
 #pragma unroll
-      for (int b = 0; b < R; ++b) bv[b] = sb[c][tx * R + b];
+      for (int i = 0; i < MI; ++i) {
+        const int r = wm * WT + i * 16 + g;
+        af[i][0] = *reinterpret_cast<const uint32_t*>(&sa[r][kk + 2 * q]);
+        af[i][1] = *reinterpret_cast<const uint32_t*>(&sa[r + 8][kk + 2 * q]);
+        af[i][2] = *reinterpret_cast<const uint32_t*>(&sa[r][kk + 8 + 2 * q]);
+        af[i][3] = *reinterpret_cast<const uint32_t*>(&sa[r + 8][kk + 8 + 2 * q]);
+      }
 #pragma unroll
-      for (int a = 0; a < R; ++a)
+      for (int j = 0; j < NJ; ++j) {
+        const int n = wn * WT + j * 8 + g;
+        bfr[j][0] = *reinterpret_cast<const uint32_t*>(&sb[n][kk + 2 * q]);
+        bfr[j][1] = *reinterpret_cast<const uint32_t*>(&sb[n][kk + 8 + 2 * q]);
+      }
 #pragma unroll
-        for (int b = 0; b < R; ++b) acc[a][b] = __fmaf_rn(av[a], bv[b], acc[a][b]);
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+              "{%0,%1,%2,%3};\n"
+              : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+              : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]), "r"(bfr[j][1]));
+        }
     }
   }
 #pragma unroll
-  for (int a = 0; a < R; ++a) {
-    const long long gi = i0 + ty * R + a;
-    if (gi >= M) continue;
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int b = 0; b < R; ++b) {
-      const int gj = j0 + tx * R + b;
-      if (gj < N) C[gi * ldc + gj] = acc[a][b];
-    }
-  }
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const long long gi = i0 + wm * WT + i * 16 + g + (e >> 1) * 8;
+        const int gj = j0 + wn * WT + j * 8 + 2 * q + (e & 1);
+        if (gi < M && gj < N) C[gi * ldc + gj] = acc[i][j][e];
+      }
 }
 
 // Z += bias; optionally A = bf16(relu(Z)).
@@ -269,20 +293,22 @@ __global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, 
   if (conf_out) conf_out[q] = best;
 }
 
-template <typename TA, typename TB>
-cudaError_t gemm(const TA* A, long long a_r, long long a_c, const TB* B, long long b_r, long long b_c, float* C,
-                 long long ldc, long long M, int N, int K, cudaStream_t s) {
+// Every MLP product (forward, dW = X^T.dZ, dX = dZ.W^T) has bf16 operands and
+// runs on the tensor cores; 32 x 32 tiles when 64 x 64 tiles would fill fewer
+// than two CTAs per SM (e.g. 1,310 x 128 outputs: 42 tiles of 64, 164 of 32).
+cudaError_t gemm(const bf16* A, long long a_r, long long a_c, const bf16* B, long long b_r, long long b_c,
+                 float* C, long long ldc, long long M, int N, int K, cudaStream_t s) {
   if (M == 0 || N == 0) return cudaSuccess;
   const long long tiles64 = ((N + 63) / 64) * ((M + 63) / 64);
-  if (tiles64 < 2 * 148) {  // e.g. 1,310 x 128 outputs: 42 tiles of 64 x 64, 164 of 32 x 32
+  if (tiles64 < 2 * 148) {
     dim3 grid(static_cast<unsigned>((N + 31) / 32), static_cast<unsigned>((M + 31) / 32));
     if (grid.y > 65535) return cudaErrorInvalidValue;
-    gemm_kernel<TA, TB, 32><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
+    gemm_bf16_tc_kernel<32><<<grid, 128, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
     return cudaGetLastError();
   }
   dim3 grid(static_cast<unsigned>((N + 63) / 64), static_cast<unsigned>((M + 63) / 64));
   if (grid.y > 65535) return cudaErrorInvalidValue;
-  gemm_kernel<TA, TB, 64><<<grid, 256, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
+  gemm_bf16_tc_kernel<64><<<grid, 128, 0, s>>>(A, a_r, a_c, B, b_r, b_c, C, ldc, M, N, K);
   return cudaGetLastError();
 }
 
@@ -307,6 +333,7 @@ struct tq_probe_mlp {
   // scratch
   vcb::DeviceBuffer d_x, d_raw, d_top, d_labels, d_targets, d_loss, d_out;
   vcb::DeviceBuffer z[5], a[5], dz[5];  // per linear layer (n_layers <= 4)
+  vcb::DeviceBuffer dzb;                 // bf16 copy of one layer's dZ (the products' operand)
 
   ~tq_probe_mlp() {
     if (stream) {
@@ -324,6 +351,7 @@ struct tq_probe_mlp {
       z[l].reserve(m * fan_out[l] * 4);
       a[l].reserve(m * fan_out[l] * 2);
       dz[l].reserve(m * fan_out[l] * 4);
+      dzb.reserve(m * fan_out[l] * 2);
     }
     d_loss.reserve(m * 4);
   }
@@ -368,14 +396,18 @@ struct tq_probe_mlp {
     for (int l = L - 1; l >= 0; --l) {
       const int K = fan_in[l], N = fan_out[l];
       const vcb::bf16* in = l == 0 ? d_x.as<vcb::bf16>() : a[l - 1].as<vcb::bf16>();
+      // The products take dZ in bf16 (fp32 accumulation); the bias gradient
+      // sums the fp32 dZ.
+      vcb::to_bf16_kernel<<<vcb::blocks(M * N), 256, 0, s>>>(dz[l].as<float>(), dzb.as<vcb::bf16>(), M * N);
+      vcb::check(cudaGetLastError(), "bf16 kernel");
       // dW = in^T . dZ  (K x N)
-      vcb::check(vcb::gemm(in, 1, K, dz[l].as<float>(), N, 1, g + w_off[l], N, K, N, static_cast<int>(M), s),
+      vcb::check(vcb::gemm(in, 1, K, dzb.as<vcb::bf16>(), N, 1, g + w_off[l], N, K, N, static_cast<int>(M), s),
                  "mlp gemm");
       vcb::colsum_kernel<<<vcb::blocks(N), 256, 0, s>>>(dz[l].as<float>(), M, N, g + b_off[l]);
       vcb::check(cudaGetLastError(), "colsum kernel");
       if (l > 0) {
         // dA_{l-1} = dZ . W^T (M x K), then the ReLU mask of layer l-1.
-        vcb::check(vcb::gemm(dz[l].as<float>(), N, 1, wbf(l), 1, N, dz[l - 1].as<float>(), K, M, K, N, s),
+        vcb::check(vcb::gemm(dzb.as<vcb::bf16>(), N, 1, wbf(l), 1, N, dz[l - 1].as<float>(), K, M, K, N, s),
                    "mlp gemm");
         vcb::relu_grad_kernel<<<vcb::blocks(M * K), 256, 0, s>>>(dz[l - 1].as<float>(), z[l - 1].as<float>(),
                                                                  M * K);

@@ -2,19 +2,20 @@
 // bucketed indexes on one GPU. No counterpart in the reference.
 //
 // A request (index, nq host queries, k, n_probe) waits in a FIFO queue. A
-// worker thread owns S slots; each slot has its own CUDA stream, pinned host
-// staging, device query / result buffers and search scratch, so batches in
-// different slots run concurrently on the device. Whenever a slot is free the
-// worker admits the oldest waiting request together with every later waiting
-// request it can share a launch with (same index, k and n_probe) up to
-// max_batch queries — requests that arrive while others run join the next
-// launch — copies their queries into the slot, queues H2D copy, search and D2H
-// copy on the slot's stream, and marks the completion time from a host
-// callback queued after the copy. Slots are created at start() only while the
-// device memory in use (resident indexes included) stays within the HBM
-// budget; each slot's scratch is grown there, by one full-size warm-up search
-// per index (and a two-query one for the batch-split scan of small flat
-// batches), so serving itself allocates nothing.
+// worker thread owns S slots; each slot has its own CUDA streams, pinned host
+// staging and device query / result buffers, so batches in different slots
+// run concurrently on the device. Search scratch (query LUTs, routing scores,
+// candidate lists, ...) comes from one device arena sized by the HBM budget:
+// whenever a slot is free, the worker forms a batch from the oldest waiting
+// request and every later waiting request it can share a launch with (same
+// index, k and n_probe) up to max_batch queries, sizes the batch's scratch
+// exactly by a dry run of the same search code (no device work), and takes
+// that many bytes from the arena. A batch that does not fit waits — and the
+// requests behind it with it — until running batches return their scratch;
+// so requests are admitted as slots and memory free up. The launch queues the
+// H2D copy, search and D2H copy on the slot's stream and marks the completion
+// time from a host callback queued after the copy. Serving allocates no device
+// memory: the arena, the slots' buffers and every kernel are set up at start().
 //
 // Every query's result is computed independently of the other queries of its
 // batch (per-query LUTs and an exact top-k), so a result is the same whether
@@ -27,6 +28,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <random>
@@ -82,8 +84,10 @@ struct Slot {
   float* h_s = nullptr;
   uint64_t* h_i = nullptr;
   vcb::DeviceBuffer d_q, d_s, d_i;
-  vcb::FlatScratchStore flat;
-  vcb::BucketScratch* bkt = nullptr;
+  vcb::FlatScratchStore flat;          // bound to `region` per batch
+  vcb::BucketScratch* bkt = nullptr;   // bound to `region` per batch
+  vcb::ScratchArena region;            // this batch's piece of the server's arena
+  size_t region_off = 0, region_bytes = 0;
   std::vector<Request*> batch;
   size_t k_eff = 0, nq = 0;
   bool busy = false;
@@ -103,6 +107,50 @@ struct Slot {
 
 void CUDART_CB mark_done(void* p) { static_cast<Slot*>(p)->done_ns.store(now_ns()); }
 
+// First-fit allocator of byte ranges of the scratch arena; freed ranges merge
+// with their free neighbours.
+class ArenaPool {
+ public:
+  void reset(size_t size) {
+    free_.clear();
+    if (size) free_[0] = size;
+    used_ = 0;
+  }
+  bool take(size_t bytes, size_t* off) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      *off = it->first;
+      const size_t rest = it->second - bytes, next_off = it->first + bytes;
+      free_.erase(it);
+      if (rest) free_[next_off] = rest;
+      used_ += bytes;
+      return true;
+    }
+    return false;
+  }
+  void give(size_t off, size_t bytes) {
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t used() const { return used_; }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t used_ = 0;
+};
+
 }  // namespace
 
 struct tq_server {
@@ -112,6 +160,16 @@ struct tq_server {
   std::vector<std::unique_ptr<Slot>> slots;
   size_t max_dim = 0, max_k = 0;
   size_t slot_bytes = 0, resident_bytes = 0;
+  // Scratch arena: every batch's scratch is a range of it, sized by a dry run.
+  vcb::DeviceBuffer arena;
+  size_t arena_bytes = 0, arena_peak = 0, max_need = 0;
+  ArenaPool pool;
+  vcb::ScratchArena sizer;            // measure-mode arena of the dry runs
+  vcb::FlatScratchStore sizer_flat;   // scratch the dry runs size
+  vcb::BucketScratch* sizer_bkt = nullptr;
+  uint64_t memory_waits = 0;          // batches that waited for arena memory
+  uint64_t blocked_head = 0;          // id of the request heading a waiting batch (0: none)
+  size_t blocked_nq = 0, blocked_need = 0;
 
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -125,7 +183,38 @@ struct tq_server {
   uint64_t batches = 0, queries = 0, completed = 0;
   size_t peak_inflight = 0;
 
-  ~tq_server() { stop(); }
+  ~tq_server() {
+    stop();
+    slots.clear();
+    if (sizer_bkt) vcb::bucket_scratch_delete(sizer_bkt);
+  }
+
+  // The search of one batch on stream s with the given scratch (a dry run
+  // when vcb::dry_run_flag() is set); returns k_eff.
+  size_t run_search(const Target& t, const float* d_q, size_t nq, size_t k, size_t n_probe, float* d_s,
+                    uint64_t* d_i, cudaStream_t s, vcb::FlatScratchStore& flat, vcb::BucketScratch& bkt) {
+    if (t.flat) {
+      const size_t ke = std::min(k, t.flat->n);
+      t.flat->search_device(d_q, nq, k, d_s, d_i, ke, s, flat.ref());
+      return ke;
+    }
+    const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
+    return vcb::bucketed_search_with(t.bkt, d_q, nq, k, n_probe, t.mlp ? &lp : nullptr, d_s, d_i, s, bkt);
+  }
+
+  // Exact scratch bytes of a batch: the same host code with no device work,
+  // its scratch buffers drawing placeholder pieces from a measuring arena.
+  size_t batch_need(const Target& t, size_t nq, size_t k, size_t n_probe) {
+    sizer.reset(nullptr, 0, true);
+    sizer_flat.bind(&sizer);
+    vcb::bucket_scratch_bind(sizer_bkt, &sizer);
+    struct DryRun {
+      DryRun() { vcb::dry_run_flag() = true; }
+      ~DryRun() { vcb::dry_run_flag() = false; }
+    } dry;
+    run_search(t, nullptr, nq, k, n_probe, nullptr, nullptr, nullptr, sizer_flat, *sizer_bkt);
+    return sizer.used;
+  }
 
   void stop() {
     {
@@ -152,16 +241,8 @@ struct tq_server {
     // soon as running flat CTAs retire instead of after the whole flat scan.
     cudaStream_t s = t.flat ? sl.stream : sl.stream_hi;
     vcb::check(cudaMemcpyAsync(sl.d_q.get(), sl.h_q, row * t.dim_in * 4, cudaMemcpyHostToDevice, s), "H2D");
-    size_t ke;
-    if (t.flat) {
-      ke = std::min(r0->k, t.flat->n);
-      t.flat->search_device(sl.d_q.as<float>(), row, r0->k, sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), ke, s,
-                            sl.flat.ref());
-    } else {
-      const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
-      ke = vcb::bucketed_search_with(t.bkt, sl.d_q.as<float>(), row, r0->k, r0->n_probe, t.mlp ? &lp : nullptr,
-                                     sl.d_s.as<float>(), sl.d_i.as<uint64_t>(), s, *sl.bkt);
-    }
+    const size_t ke = run_search(t, sl.d_q.as<float>(), row, r0->k, r0->n_probe, sl.d_s.as<float>(),
+                                 sl.d_i.as<uint64_t>(), s, sl.flat, *sl.bkt);
     sl.k_eff = ke;
     vcb::check(cudaMemcpyAsync(sl.h_s, sl.d_s.get(), row * ke * 4, cudaMemcpyDeviceToHost, s), "D2H");
     vcb::check(cudaMemcpyAsync(sl.h_i, sl.d_i.get(), row * ke * 8, cudaMemcpyDeviceToHost, s), "D2H");
@@ -172,7 +253,13 @@ struct tq_server {
     queries += row;
   }
 
+  void free_region(Slot& sl) {
+    if (sl.region_bytes) pool.give(sl.region_off, sl.region_bytes);
+    sl.region_bytes = 0;
+  }
+
   void retire(Slot& sl) {
+    free_region(sl);
     size_t row = 0;
     const int64_t t = sl.done_ns.load();
     for (Request* r : sl.batch) {
@@ -188,22 +275,103 @@ struct tq_server {
     sl.busy = false;
   }
 
-  // Oldest waiting request plus later compatible ones, up to max_batch queries.
-  void take_batch(Slot& sl) {
+  // Oldest waiting request plus later compatible ones, up to max_batch
+  // queries (left in the queue until the batch is admitted).
+  std::vector<Request*> peek_batch(size_t* total) const {
+    std::vector<Request*> b;
     Request* r0 = pending.front();
-    pending.pop_front();
-    sl.batch.push_back(r0);
-    size_t total = r0->nq;
-    for (auto it = pending.begin(); it != pending.end();) {
+    b.push_back(r0);
+    *total = r0->nq;
+    for (auto it = std::next(pending.begin()); it != pending.end(); ++it) {
       Request* r = *it;
-      if (r->target == r0->target && r->k == r0->k && r->n_probe == r0->n_probe && total + r->nq <= max_batch) {
-        sl.batch.push_back(r);
-        total += r->nq;
-        it = pending.erase(it);
-      } else {
-        ++it;
+      if (r->target == r0->target && r->k == r0->k && r->n_probe == r0->n_probe && *total + r->nq <= max_batch) {
+        b.push_back(r);
+        *total += r->nq;
       }
     }
+    return b;
+  }
+
+  void unqueue(const std::vector<Request*>& b) {
+    for (Request* r : b) pending.erase(std::find(pending.begin(), pending.end(), r));
+  }
+
+  void fail_batch(const std::vector<Request*>& b, int status, const std::string& why) {
+    for (Request* r : b) {
+      r->status = status;
+      r->error = why;
+      r->done = true;
+    }
+    cv_done.notify_all();
+  }
+
+  // Admits the batch at the head of the queue into the free slot sl when its
+  // scratch fits in the arena. Returns false when it must wait for memory.
+  bool admit(Slot& sl) {
+    size_t nq = 0;
+    std::vector<Request*> b = peek_batch(&nq);
+    Request* r0 = b.front();
+    const Target& t = targets[r0->target];
+    size_t need = 0;
+    if (blocked_head == r0->id && blocked_nq == nq) {
+      need = blocked_need;  // sized while it waited
+    } else {
+      try {
+        need = batch_need(t, nq, r0->k, r0->n_probe);
+      } catch (const std::exception& ex) {
+        unqueue(b);
+        fail_batch(b, TQ_ERR_CUDA, ex.what());
+        return true;
+      }
+    }
+    if (need > arena_bytes && b.size() > 1) {
+      // The merged batch is too large for the arena: the oldest request alone.
+      b.resize(1);
+      nq = r0->nq;
+      try {
+        need = batch_need(t, nq, r0->k, r0->n_probe);
+      } catch (const std::exception& ex) {
+        unqueue(b);
+        fail_batch(b, TQ_ERR_CUDA, ex.what());
+        return true;
+      }
+    }
+    if (need > arena_bytes) {
+      unqueue(b);
+      fail_batch(b, TQ_ERR_OUT_OF_MEMORY,
+                 "batch scratch of " + std::to_string(need) + " bytes exceeds the serving arena (" +
+                     std::to_string(arena_bytes) + " bytes)");
+      return true;
+    }
+    size_t off = 0;
+    if (!pool.take(need, &off)) {
+      if (blocked_head != r0->id) ++memory_waits;
+      blocked_head = r0->id;
+      blocked_nq = nq;
+      blocked_need = need;
+      return false;
+    }
+    blocked_head = 0;
+    unqueue(b);
+    sl.batch = std::move(b);
+    sl.region_off = off;
+    sl.region_bytes = need;
+    sl.region.reset(static_cast<unsigned char*>(arena.get()) + off, need, false);
+    sl.flat.bind(&sl.region);
+    vcb::bucket_scratch_bind(sl.bkt, &sl.region);
+    arena_peak = std::max(arena_peak, pool.used());
+    try {
+      launch(sl);
+    } catch (const std::exception& ex) {
+      // Work queued before the failure may still read the region: free it
+      // only after the slot's streams drain.
+      cudaStreamSynchronize(sl.stream);
+      cudaStreamSynchronize(sl.stream_hi);
+      free_region(sl);
+      fail_batch(sl.batch, TQ_ERR_CUDA, ex.what());
+      sl.batch.clear();
+    }
+    return true;
   }
 
   void run() {
@@ -221,11 +389,8 @@ struct tq_server {
             progress = true;
           } else if (e != cudaErrorNotReady) {
             worker_error = cudaGetErrorString(e);
-            for (Request* r : sl.batch) {
-              r->status = TQ_ERR_CUDA;
-              r->error = worker_error;
-              r->done = true;
-            }
+            free_region(sl);
+            fail_batch(sl.batch, TQ_ERR_CUDA, worker_error);
             sl.batch.clear();
             sl.busy = false;
             progress = true;
@@ -233,22 +398,17 @@ struct tq_server {
         }
       }
       if (progress) cv_done.notify_all();
+      // Free slots take batches in arrival order while their scratch fits;
+      // a batch that must wait for memory holds back the ones behind it.
+      bool memory_wait = false;
       for (auto& sp : slots) {
         Slot& sl = *sp;
-        if (!sl.busy && !pending.empty()) {
-          take_batch(sl);
-          try {
-            launch(sl);
-          } catch (const std::exception& ex) {
-            for (Request* r : sl.batch) {
-              r->status = TQ_ERR_CUDA;
-              r->error = ex.what();
-              r->done = true;
-            }
-            sl.batch.clear();
-            cv_done.notify_all();
+        if (!sl.busy && !pending.empty() && !memory_wait) {
+          if (admit(sl)) {
+            progress = true;
+          } else {
+            memory_wait = true;
           }
-          progress = true;
         }
         inflight += sl.busy ? 1 : 0;
       }
@@ -278,13 +438,14 @@ struct tq_server {
     std::normal_distribution<float> nd;
     for (float& v : warm) v = nd(rng);
     {
-      // One small search per index with throwaway scratch first: kernels are
-      // loaded on their first launch, and that device memory must not be
-      // counted as a slot's.
+      // Full-size and two-query searches per index with throwaway scratch:
+      // kernels are loaded on their first launch, and that device memory is
+      // resident, not part of the scratch arena.
       vcb::DeviceBuffer q, sc_s, sc_i;
       vcb::FlatScratchStore fs;
+      fs.range_cap = kServingRangeVectors;
       vcb::BucketScratch* bs = vcb::bucket_scratch_new();
-      const size_t m = std::min<size_t>(max_batch, 64);
+      const size_t m = max_batch;
       q.reserve(m * max_dim * 4);
       sc_s.reserve(m * max_k * 4);
       sc_i.reserve(m * max_k * 8);
@@ -305,9 +466,6 @@ struct tq_server {
       vcb::check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
       vcb::bucket_scratch_delete(bs);
     }
-    size_t free_b = 0, total_b = 0;
-    vcb::check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    resident_bytes = total_b - free_b;
     for (size_t s = 0; s < max_slots; ++s) {
       auto sl = std::make_unique<Slot>();
       vcb::check(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -324,32 +482,30 @@ struct tq_server {
       sl->d_s.reserve(max_batch * max_k * 4);
       sl->d_i.reserve(max_batch * max_k * 8);
       sl->bkt = vcb::bucket_scratch_new();
-      vcb::check(cudaMemcpy(sl->d_q.get(), warm.data(), warm.size() * 4, cudaMemcpyHostToDevice), "H2D");
-      for (const Target& t : targets) {
-        if (t.flat) {
-          const size_t ke = std::min(t.max_k, t.flat->n);
-          t.flat->search_device(sl->d_q.as<float>(), max_batch, t.max_k, sl->d_s.as<float>(), sl->d_i.as<uint64_t>(),
-                                ke, sl->stream, sl->flat.ref());
-          // grows the batch-split scratch that one- and two-query batches use
-          t.flat->search_device(sl->d_q.as<float>(), std::min<size_t>(max_batch, 2), t.max_k, sl->d_s.as<float>(),
-                                sl->d_i.as<uint64_t>(), ke, sl->stream, sl->flat.ref());
-        } else {
-          const vcb::LearnedProbe lp{t.mlp, t.coverage, t.min_conf};
-          vcb::bucketed_search_with(t.bkt, sl->d_q.as<float>(), max_batch, t.max_k, t.max_probe,
-                                    t.mlp ? &lp : nullptr, sl->d_s.as<float>(), sl->d_i.as<uint64_t>(), sl->stream,
-                                    *sl->bkt);
-        }
-      }
-      vcb::check(cudaStreamSynchronize(sl->stream), "cudaStreamSynchronize");
-      vcb::check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-      const size_t used = total_b - free_b;
-      if (s == 0) slot_bytes = used - resident_bytes;
-      if (used > budget && !slots.empty()) break;  // this slot does not fit: drop it
       slots.push_back(std::move(sl));
-      if (used + slot_bytes > budget) break;
     }
-    vcb::require(!slots.empty() && total_b - free_b <= budget, TQ_ERR_OUT_OF_MEMORY,
-                 "the HBM budget does not hold the resident indexes plus one serving slot");
+    slot_bytes = max_batch * (max_dim * 4 + max_k * 12);
+    size_t free_b = 0, total_b = 0;
+    vcb::check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    resident_bytes = total_b - free_b;  // indexes, kernels, context and the slots' buffers
+    // The largest scratch any admissible batch needs: full batches at the
+    // largest k and n_probe (and one- and two-query batches, which may take
+    // the batch-split scan).
+    sizer_flat.range_cap = kServingRangeVectors;
+    sizer_bkt = vcb::bucket_scratch_new();
+    for (const Target& t : targets) {
+      for (size_t m : {max_batch, std::min<size_t>(max_batch, 2), size_t{1}}) {
+        max_need = std::max(max_need, batch_need(t, m, t.max_k, t.max_probe));
+      }
+    }
+    if (budget <= resident_bytes || budget - resident_bytes < max_need) {
+      vcb::fail(TQ_ERR_OUT_OF_MEMORY, "the HBM budget does not hold the resident indexes plus the scratch of one "
+                                      "full batch (" + std::to_string(resident_bytes + max_need) + " bytes needed)");
+    }
+    arena_bytes = std::min(budget - resident_bytes, max_slots * max_need);
+    arena_bytes = arena_bytes / vcb::ScratchArena::kAlign * vcb::ScratchArena::kAlign;
+    arena.reserve(arena_bytes);
+    pool.reset(arena_bytes);
     started = true;
     worker = std::thread([this] { run(); });
   }
@@ -496,6 +652,34 @@ int tq_server_wait(tq_server* h, uint64_t request, size_t* k_eff, double* latenc
     if (latency_us) *latency_us = static_cast<double>(r->t_done - r->t_arrive) / 1e3;
     h->requests.erase(it);
     if (status != TQ_OK) vcb::fail(status, err);
+  });
+}
+
+int tq_server_memory(tq_server* h, size_t* arena_bytes, size_t* arena_peak, size_t* max_batch_bytes,
+                     uint64_t* memory_waits) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(h->started, TQ_ERR_STATE, "start() the server first");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (arena_bytes) *arena_bytes = h->arena_bytes;
+    if (arena_peak) *arena_peak = h->arena_peak;
+    if (max_batch_bytes) *max_batch_bytes = h->max_need;
+    if (memory_waits) *memory_waits = h->memory_waits;
+  });
+}
+
+int tq_server_batch_bytes(tq_server* h, int target, size_t nq, size_t k, size_t n_probe, size_t* bytes) {
+  return vcb::guarded([&] {
+    checked(h);
+    require(h->started, TQ_ERR_STATE, "start() the server first");
+    require(bytes != nullptr, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(target >= 0 && target < static_cast<int>(h->targets.size()), TQ_ERR_INVALID_ARGUMENT, "no such index");
+    const Target& t = h->targets[target];
+    require(nq >= 1 && nq <= h->max_batch, TQ_ERR_INVALID_ARGUMENT, "nq must be in [1, max_batch]");
+    require(k >= 1 && k <= t.max_k, TQ_ERR_INVALID_ARGUMENT, "k must be in [1, max_k of the index]");
+    vcb::DeviceGuard g(h->device);
+    std::lock_guard<std::mutex> lk(h->mu);
+    *bytes = h->batch_need(t, nq, k, t.flat ? 0 : (n_probe ? n_probe : t.max_probe));
   });
 }
 

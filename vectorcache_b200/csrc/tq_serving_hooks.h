@@ -19,6 +19,9 @@ struct LearnedProbe {
 
 BucketScratch* bucket_scratch_new();
 void bucket_scratch_delete(BucketScratch* sc);
+// Later reserves of every buffer of sc draw from a (nullptr: cudaMalloc).
+struct ScratchArena;
+void bucket_scratch_bind(BucketScratch* sc, ScratchArena* a);
 size_t bucketed_dim_in(const tq_bucketed* h);
 size_t bucketed_size(const tq_bucketed* h);
 bool bucketed_prepared(const tq_bucketed* h);

@@ -40,6 +40,8 @@ def _declare_server(lib):
         "tq_server_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                       C.POINTER(_SZ)]),
         "tq_server_replay": (C.c_int, [_P, C.POINTER(_ReplayItem), _SZ, _P, C.POINTER(C.c_double)]),
+        "tq_server_memory": (C.c_int, [_P, C.POINTER(_SZ), C.POINTER(_SZ), C.POINTER(_SZ), C.POINTER(C.c_uint64)]),
+        "tq_server_batch_bytes": (C.c_int, [_P, C.c_int, _SZ, _SZ, _SZ, C.POINTER(_SZ)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -110,6 +112,19 @@ class Server:
         ns, sb, rb = _SZ(), _SZ(), _SZ()
         _check(self._lib.tq_server_info(self._h, C.byref(ns), C.byref(sb), C.byref(rb)))
         return {"slots": ns.value, "slot_bytes": sb.value, "resident_bytes": rb.value}
+
+    def memory(self) -> dict:
+        """Scratch arena: size, peak use, largest batch scratch, batches that waited for memory."""
+        a, p, m = _SZ(), _SZ(), _SZ()
+        w = C.c_uint64()
+        _check(self._lib.tq_server_memory(self._h, C.byref(a), C.byref(p), C.byref(m), C.byref(w)))
+        return {"arena_bytes": a.value, "arena_peak": p.value, "max_batch_bytes": m.value, "memory_waits": w.value}
+
+    def batch_bytes(self, target: int, nq: int, k: int, n_probe: int = 0) -> int:
+        """Arena bytes the scratch of one batch of nq queries takes."""
+        b = _SZ()
+        _check(self._lib.tq_server_batch_bytes(self._h, target, nq, k, n_probe, C.byref(b)))
+        return b.value
 
     def stats(self) -> dict:
         b, q, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
