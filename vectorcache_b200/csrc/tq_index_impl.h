@@ -384,10 +384,19 @@ struct tq_index {
       a.cand_score = sc.cand_s->as<float>();
       a.cand_id = sc.cand_i->as<uint32_t>();
       if (plan.split_batches > 1 && sc.partial) {
-        sc.partial->reserve(m * static_cast<size_t>(plan.split_batches) * cap * 4);
+        // Batch sums, then one arrival counter per (query group, block),
+        // zeroed for this launch.
+        const size_t sums = m * static_cast<size_t>(plan.split_batches) * cap;
+        const size_t counters = static_cast<size_t>((m + plan.q_per_cta - 1) / plan.q_per_cta) *
+                                ((n + vcb::kScanBlockVectors - 1) / vcb::kScanBlockVectors);
+        sc.partial->reserve((sums + counters) * 4);
         a.partial = sc.partial->as<uint32_t>();
         a.partial_stride = static_cast<long long>(cap);
         a.partial_batches = plan.split_batches;
+        a.arrive = a.partial + sums;
+        if (!vcb::dry_run_flag()) {
+          vcb::check(cudaMemsetAsync(a.arrive, 0, counters * 4, s), "cudaMemsetAsync");
+        }
       }
       launch(kScan, s, "scan kernel", [&] { return vcb::launch_scan(a, plan, s); });
       if (!vcb::dry_run_flag()) {

@@ -99,6 +99,10 @@ struct ScanArgs {
   uint32_t* partial = nullptr;
   long long partial_stride = 0;
   int partial_batches = 0;
+  // With `partial`: one zeroed counter per (query group, block); the CTA that
+  // stores a block's last batch sums flushes that block in the same launch.
+  // nullptr: a second launch flushes every block.
+  unsigned* arrive = nullptr;
 };
 
 struct MergeArgs {

@@ -17,6 +17,7 @@
 // sign of a LUT byte, which is 0 because LUT bytes are <= 127. Four prmt give
 // the four per-vector byte sums (<= 254), and dp4a adds each byte into its
 // vector's 32-bit accumulator.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 
@@ -143,7 +144,9 @@ struct RegTopK {
 // over an index of few blocks, the work splits by 256-group batch instead:
 // MODE 1 scans only batch blockIdx.z of one block and stores the integer sums
 // in a.partial; MODE 2 then flushes those sums in batch order (the same f32
-// arithmetic as MODE 0) and keeps the top k, without lookups.
+// arithmetic as MODE 0) and keeps the top k, without lookups. MODE 3 is MODE 1
+// followed, in the CTA that stores a block's last batch (a counter per block,
+// threadfence-reduction style, no waiting), by MODE 2 for that block.
 template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
   static_assert(PF % 2 == 0, "byte groups are consumed in pairs");
@@ -206,10 +209,11 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
   };
 
   // Byte groups this CTA scans: all (MODE 0), one batch (MODE 1), none (MODE 2).
-  const int g_first = MODE == 1 ? static_cast<int>(blockIdx.z) * kFlushGroups : 0;
-  const int g_last = MODE == 1 ? min(g_first + kFlushGroups, nbg) : (MODE == 2 ? 0 : nbg);
+  constexpr bool kBatch = MODE == 1 || MODE == 3;  // scans one 256-group batch
+  const int g_first = kBatch ? static_cast<int>(blockIdx.z) * kFlushGroups : 0;
+  const int g_last = kBatch ? min(g_first + kFlushGroups, nbg) : (MODE == 2 ? 0 : nbg);
   const bool resident = MODE != 0 || chunk >= nbg;
-  if constexpr (MODE == 1) {
+  if constexpr (kBatch) {
     load_lut_chunk(g_first, g_last - g_first);
     __syncthreads();
   } else if constexpr (MODE == 0) {
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         load_lut_chunk(gb, min(chunk, nbg - gb));
         __syncthreads();
       }
-      const int chunk_base = MODE == 1 ? g_first : (resident ? 0 : (gb / chunk) * chunk);
+      const int chunk_base = kBatch ? g_first : (resident ? 0 : (gb / chunk) * chunk);
       uint2 ring[PF];
 #pragma unroll
       for (int u = 0; u < PF; ++u) {
@@ -328,8 +332,8 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         }
       }
     }
-    if constexpr (MODE == 1) {
-      // The batch's integer sums of this lane's 8 vectors, for MODE 2.
+    if constexpr (kBatch) {
+      // The batch's integer sums of this lane's 8 vectors, for the flush.
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         if (q0 + q >= a.nq) break;
@@ -338,10 +342,25 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         dst[0] = make_uint4(acc[q][0], acc[q][1], acc[q][2], acc[q][3]);
         dst[1] = make_uint4(acc[q][4], acc[q][5], acc[q][6], acc[q][7]);
       }
-      continue;
+      if constexpr (MODE == 1) continue;
+      if constexpr (MODE == 3) {
+        // Publish the sums, then count this batch in; only the CTA that
+        // completes the block goes on (no CTA ever waits for another).
+        __shared__ unsigned s_last;
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          unsigned* c = a.arrive + static_cast<long long>(blockIdx.x) * gridDim.y + blockIdx.y;
+          s_last = atomicAdd(c, 1u) == static_cast<unsigned>(a.partial_batches - 1) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+      }
     }
-    if constexpr (MODE == 2) {
-      // The same flushes as MODE 0, batch by batch in order, from the stored sums.
+    if constexpr (MODE == 2 || MODE == 3) {
+      // The same flushes as MODE 0, batch by batch in order, from the stored
+      // sums (read past L1: other CTAs wrote them).
       for (int b = 0; b < a.partial_batches; ++b) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -349,8 +368,8 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           if (q0 + q < a.nq) {
             const uint4* src = reinterpret_cast<const uint4*>(
                 a.partial + ((q0 + q) * a.partial_batches + b) * a.partial_stride + vbase);
-            s0 = src[0];
-            s1 = src[1];
+            s0 = __ldcg(src);
+            s1 = __ldcg(src + 1);
           }
           const uint32_t sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
 #pragma unroll
@@ -707,6 +726,18 @@ cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t
   s.lut_chunk_groups = kFlushGroups;
   s.partial_batches = plan.split_batches;
   const size_t smem1 = static_cast<size_t>(Q) * kFlushGroups * 32;
+  if (a.arrive && plan.n_ranges == blocks) {
+    // One launch: the CTA completing a block flushes it (its lists are the
+    // plan's ranges, one block each). The LUT area also holds the merge.
+    const size_t smem3 = std::max(smem1, static_cast<size_t>(Q) * kScanWarps * kWarp * 8);
+    cudaError_t e3 = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, 2, N8, kPf, 3>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem3));
+    if (e3 != cudaSuccess) return e3;
+    scan_kernel<Q, kRegTopK, 2, N8, kPf, 3><<<dim3(qgroups, static_cast<unsigned>(blocks),
+                                                   static_cast<unsigned>(plan.split_batches)),
+                                              kScanWarps * 32, smem3, stream>>>(s);
+    return cudaGetLastError();
+  }
   cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, 2, N8, kPf, 1>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem1));
   if (e != cudaSuccess) return e;
