@@ -818,7 +818,7 @@ def run_bucketed(args, world, rank, local):
     fixed = sweep[p_op]
     recall_fixed = fixed["recall_at_10"]
     fixed_ms = fixed["ms_per_step"]
-    classes = tuple(c for c in PROBE_CLASSES if c <= p_op)
+    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,)  # the operating point is the largest class
 
     # labels from the plain index (reference n_probe = the operating point) and GPU training
     t0 = time.perf_counter()
@@ -957,7 +957,7 @@ def run_serving(args, world, rank, local):
         if recall_rows(bkt.search(test_q, k, n_probe=p).ids, ex_test, k).mean() >= RECALL_TARGET:
             p_op = p
             break
-    classes = tuple(c for c in PROBE_CLASSES if c <= p_op)
+    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,)  # the operating point is the largest class
     labels, rec = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
     objective = args.probe_objective
     mlp, _ = train_probe_mlp(bkt, train_q, labels, rec, classes, objective, args.epochs, device, local)
