@@ -127,7 +127,7 @@ def test_requests_wait_for_memory_and_run_when_it_frees(indexes):
     need = roomy.batch_bytes(fid, 4096, 64)
     mem = roomy.memory()
     roomy.close()
-    assert need > (32 << 20) and mem["max_batch_bytes"] >= need
+    assert need > (16 << 20) and mem["max_batch_bytes"] >= need
     srv = vcb.Server(hbm_budget_bytes=resident + need + need // 2, max_slots=4, max_batch=4096)
     fid = srv.add_flat(flat, 64)
     srv.start()

@@ -6,6 +6,7 @@
 // the rounding contract.
 #include <type_traits>
 
+#include "tq_host_math.h"
 #include "tq_kernels.h"
 #include "tq_device.cuh"
 
@@ -345,7 +346,7 @@ __device__ __forceinline__ int pipe_elem(int r, int lane) {
 
 struct PipeLayout {
   int stride;         // floats per row slot (>= dim + 1, == 8 mod 32)
-  size_t off_bk, off_ss, off_cen, off_src, off_bnd, off_rows, total;
+  size_t off_bk, off_ss, off_cen, off_grid, off_src, off_bnd, off_rows, total;
 };
 
 __host__ __device__ inline PipeLayout pipe_layout(int dim, int r_regs, bool tqplus, int warps, int rows) {
@@ -361,6 +362,8 @@ __host__ __device__ inline PipeLayout pipe_layout(int dim, int r_regs, bool tqpl
   o += tqplus ? slots * 8 : 0;
   L.off_cen = o;
   o += 16 * 8;
+  L.off_grid = o;
+  o += static_cast<size_t>(CodeGrid::kCells) * 8;
   L.off_src = o;
   o += slots * 4;
   L.off_bnd = o;
@@ -383,7 +386,18 @@ __device__ __forceinline__ unsigned pipe_code(float v, const float* __restrict__
   return idx;
 }
 
-template <int R, int E, int BITS, int ROWS, int MAXW>
+// The code of v from the host-built grid (CodeGrid in tq_host_math.h): one
+// fused multiply-add picks a cell holding at most one boundary, so the count
+// of boundaries strictly below v is the cell's base plus one compare.
+__device__ __forceinline__ unsigned grid_code(float v, const uint2* __restrict__ grid, float lo, float hi, float ga,
+                                              float gk) {
+  const float c = fminf(fmaxf(v, lo), hi);  // NaN -> lo: code 0, as v > b is false for every b
+  const int cell = __float_as_int(__fmaf_rn(c, ga, gk)) - 0x4B400000;
+  const uint2 e = grid[cell];
+  return e.x + (c > __uint_as_float(e.y) ? 1u : 0u);
+}
+
+template <int R, int E, int BITS, int ROWS, int MAXW, bool TQ>
 __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a) {
   static_assert(R % E == 0, "segments of E registers");
   constexpr int SEG = R / E;
@@ -403,6 +417,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
   double2* s_bk = reinterpret_cast<double2*>(smem + L.off_bk);   // {inv_scale, shift} (TQ+)
   float2* s_ss = reinterpret_cast<float2*>(smem + L.off_ss);     // {shift, scale} (TQ+)
   double* s_cen = reinterpret_cast<double*>(smem + L.off_cen);
+  uint2* s_grid = reinterpret_cast<uint2*>(smem + L.off_grid);     // {base code, inner boundary bits}
   uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + L.off_src);
   float* s_bnd = reinterpret_cast<float*>(smem + L.off_bnd);
   float* rows = reinterpret_cast<float*>(smem + L.off_rows) + static_cast<size_t>(warp) * ROWS * L.stride;
@@ -433,6 +448,8 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
     s_cen[threadIdx.x] = static_cast<double>(a.centroids[threadIdx.x]);
     s_bnd[threadIdx.x] = threadIdx.x < 15 ? a.boundaries[threadIdx.x] : 0.f;
   }
+  for (int j = threadIdx.x; j < CodeGrid::kCells; j += blockDim.x) s_grid[j] = a.grid[j];
+  const float g_lo = a.grid_lo, g_hi = a.grid_hi, g_a = a.grid_a, g_k = a.grid_k;
   for (int j = lane; j < ROWS; j += 32) rows[j * L.stride + dim] = 0.f;
 
   const long long n_groups = (a.n + ROWS - 1) / ROWS;
@@ -453,7 +470,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
   cp_async_commit();
   __syncthreads();
 
-  const bool tq = a.tqplus;
+  constexpr bool tq = TQ;
   for (; grp < n_groups; grp += g_step) {
     cp_async_wait_all();
     __syncwarp();
@@ -562,15 +579,15 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
           const int r = sgi * E + e;
           unsigned code;
           double term;
-          if (tq) {
+          if constexpr (tq) {
             const float2 ss = s_ss[r * 32 + lane];
             const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
-            code = pipe_code<BITS>(c, s_bnd);
+            code = grid_code(c, s_grid, g_lo, g_hi, g_a, g_k);
             const double2 bk = s_bk[r * 32 + lane];
             const double back = __dsub_rn(__dmul_rn(s_cen[code], bk.x), bk.y);
             term = __dmul_rn(static_cast<double>(y[r]), back);
           } else {
-            code = pipe_code<BITS>(y[r], s_bnd);
+            code = grid_code(y[r], s_grid, g_lo, g_hi, g_a, g_k);
             term = __dmul_rn(static_cast<double>(y[r]), s_cen[code]);
           }
           est = __dadd_rn(est, term);
@@ -608,7 +625,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
                 const int r = sgi * E + e;
                 if (pipe_elem<E>(r, lane) < dim) {
                   double back;
-                  if (tq) {
+                  if constexpr (tq) {
                     const float2 ss = s_ss[r * 32 + lane];
                     const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
                     const unsigned code = pipe_code<BITS>(c, s_bnd);
@@ -650,28 +667,34 @@ bool pipe_shape(int dim, int* r_out, int* e_out) {
   return false;
 }
 
-template <int R, int E, int BITS, int ROWS, int MAXW>
+template <int R, int E, int BITS, int ROWS, int MAXW, bool TQ>
 cudaError_t launch_pipe_t(const EncodeArgs& a, int sms, int max_smem, cudaStream_t stream) {
   int warps = MAXW;
   while (warps > 1 && pipe_layout(a.dim, R, a.tqplus, warps, ROWS).total > static_cast<size_t>(max_smem)) --warps;
   const size_t smem = pipe_layout(a.dim, R, a.tqplus, warps, ROWS).total;
   if (smem > static_cast<size_t>(max_smem)) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(encode_pipe_kernel<R, E, BITS, ROWS, MAXW>,
+  cudaError_t e = cudaFuncSetAttribute(encode_pipe_kernel<R, E, BITS, ROWS, MAXW, TQ>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   const long long groups = (a.n + ROWS - 1) / ROWS;
   long long ctas = (groups + warps - 1) / warps;
   if (ctas > sms) ctas = sms;
-  encode_pipe_kernel<R, E, BITS, ROWS, MAXW><<<static_cast<unsigned>(ctas), warps * 32, smem, stream>>>(a);
+  encode_pipe_kernel<R, E, BITS, ROWS, MAXW, TQ><<<static_cast<unsigned>(ctas), warps * 32, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
 template <int R, int E, int ROWS, int MAXW>
 cudaError_t launch_pipe_bits(const EncodeArgs& a, int sms, int max_smem, cudaStream_t stream) {
   switch (a.bits) {
-    case 2: return launch_pipe_t<R, E, 2, ROWS, MAXW>(a, sms, max_smem, stream);
-    case 3: return launch_pipe_t<R, E, 3, ROWS, MAXW>(a, sms, max_smem, stream);
-    case 4: return launch_pipe_t<R, E, 4, ROWS, MAXW>(a, sms, max_smem, stream);
+    case 2:
+      return a.tqplus ? launch_pipe_t<R, E, 2, ROWS, MAXW, true>(a, sms, max_smem, stream)
+                      : launch_pipe_t<R, E, 2, ROWS, MAXW, false>(a, sms, max_smem, stream);
+    case 3:
+      return a.tqplus ? launch_pipe_t<R, E, 3, ROWS, MAXW, true>(a, sms, max_smem, stream)
+                      : launch_pipe_t<R, E, 3, ROWS, MAXW, false>(a, sms, max_smem, stream);
+    case 4:
+      return a.tqplus ? launch_pipe_t<R, E, 4, ROWS, MAXW, true>(a, sms, max_smem, stream)
+                      : launch_pipe_t<R, E, 4, ROWS, MAXW, false>(a, sms, max_smem, stream);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -707,7 +730,7 @@ cudaError_t launch_encode(const EncodeArgs& a, int sms, cudaStream_t stream) {
   if (a.n == 0) return cudaSuccess;
   if (a.dim > kRegisterRowMaxDim) return launch_encode_big(a, sms, stream);
   int pr = 0, pe = 0;
-  if (pipe_shape(a.dim, &pr, &pe)) {
+  if (a.grid && pipe_shape(a.dim, &pr, &pe)) {
     int device = 0, max_smem = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);

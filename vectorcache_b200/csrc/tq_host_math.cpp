@@ -10,6 +10,8 @@
 
 #include <array>
 #include <cmath>
+#include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -257,6 +259,68 @@ TqplusAnchor tqplus_anchor(std::size_t n, std::size_t bits, std::size_t dim) {
   out.qc_lo = -c_outer;
   out.qc_span = c_outer - (-c_outer);
   return out;
+}
+
+namespace {
+
+// Cell of c as the device computes it: t = fmaf(c, a, k) rounded once to
+// float; returns false when the exact value of c * a + k lies too close to a
+// float rounding tie for the long-double evaluation to decide it.
+bool grid_cell(float c, float a, float k, int* cell) {
+  const long double exact = static_cast<long double>(c) * static_cast<long double>(a) + static_cast<long double>(k);
+  // t in [2^23, 2^24): one float ulp is 1, so the rounding point is the
+  // nearest integer; stay away from .5 by far more than the long double error.
+  const long double frac = exact - std::floor(exact);
+  if (std::fabs(frac - 0.5L) < 1e-6L) return false;
+  const float t = static_cast<float>(exact);
+  if (!(t >= 8388608.f && t < 16777216.f)) return false;
+  std::uint32_t bits;
+  std::memcpy(&bits, &t, 4);
+  *cell = static_cast<int>(bits) - 0x4B400000;
+  return true;
+}
+
+}  // namespace
+
+bool make_code_grid(const std::vector<float>& b, CodeGrid* out) {
+  if (b.empty()) return false;
+  const float first = b.front(), last = b.back();
+  const float span = last - first;
+  if (!(span > 0.f)) return false;
+  CodeGrid g;
+  g.lo = first - span / 8.f;
+  g.hi = last + span / 8.f;
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    // About kCells - 4 cells across [lo, hi], cell(lo) near 1; the slope
+    // changes a little between attempts to move every value off a rounding
+    // tie (k is an integer: floats near 2^23 have unit spacing).
+    g.a = static_cast<float>((CodeGrid::kCells - 4.0 - 0.013 * attempt) / (static_cast<double>(g.hi) - g.lo));
+    g.k = static_cast<float>(std::floor(12582912.0 + 1.25 - static_cast<double>(g.lo) * g.a));
+    int c_lo = 0, c_hi = 0;
+    if (!grid_cell(g.lo, g.a, g.k, &c_lo) || !grid_cell(g.hi, g.a, g.k, &c_hi)) continue;
+    if (c_lo < 0 || c_hi > CodeGrid::kCells - 1) continue;
+    bool ok = true;
+    int prev = -1;
+    std::vector<int> cells(b.size());
+    for (std::size_t i = 0; i < b.size() && ok; ++i) {
+      ok = grid_cell(b[i], g.a, g.k, &cells[i]) && cells[i] > prev && cells[i] >= c_lo && cells[i] <= c_hi;
+      prev = cells[i];
+    }
+    if (!ok) continue;
+    const float inf = std::numeric_limits<float>::infinity();
+    std::size_t next = 0;
+    for (int j = 0; j < CodeGrid::kCells; ++j) {
+      g.base[j] = static_cast<std::uint32_t>(next);
+      g.inner[j] = inf;
+      if (next < b.size() && cells[next] == j) {
+        g.inner[j] = b[next];
+        ++next;
+      }
+    }
+    *out = g;
+    return true;
+  }
+  return false;
 }
 
 }  // namespace vcb

@@ -37,6 +37,23 @@ struct Codebook {
 // (codebook.cpp:135-226). Memoized and thread-safe.
 const Codebook& codebook(std::size_t bits, std::size_t dim);
 
+// A table that turns the code of a value (the count of codebook boundaries
+// strictly below it, encode.cpp:126-140) into one fused multiply-add, one
+// table read and one compare. The device computes, for c clamped to
+// [lo, hi], t = fmaf(c, a, k) in [2^23, 2^24) and the cell j = bits(t) -
+// bits(2^23 + 2^22): a monotone function of c, so every cell is an interval.
+// The host evaluates that same rounding exactly for every boundary and keeps
+// at most one boundary per cell; then code(c) = base[j] + (c > inner[j]),
+// exactly the count for every float c (NaN: 0).
+struct CodeGrid {
+  static constexpr int kCells = 64;
+  float lo = 0.f, hi = 0.f, a = 0.f, k = 0.f;
+  std::uint32_t base[kCells] = {};  // boundaries in earlier cells
+  float inner[kCells] = {};         // the boundary inside the cell, or +inf
+};
+// False when no grid separates the boundaries (callers keep the binary search).
+bool make_code_grid(const std::vector<float>& boundaries, CodeGrid* out);
+
 // Regularized incomplete beta I_t(a, a) (encode.cpp:95-112).
 double beta_cdf_aa(double a, double t);
 

@@ -173,7 +173,7 @@ int tq_index_create(size_t dim, size_t bits, uint32_t flags, int device, tq_inde
     require(vcb::bits_supported(bits), TQ_ERR_INVALID_ARGUMENT, "bits must be 2, 3, or 4");
     require(flags == 0, TQ_ERR_INVALID_ARGUMENT, "flags must be 0");
     require(vcb::encode_dim_supported(static_cast<int>(dim)), TQ_ERR_UNSUPPORTED,
-            "dim > 2048 is not supported by the device kernels yet");
+            "dim is not supported by the device kernels");
     int count = 0;
     vcb::check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
     require(device >= 0 && device < count, TQ_ERR_INVALID_ARGUMENT, "no such CUDA device");
@@ -201,6 +201,16 @@ int tq_index_create(size_t dim, size_t bits, uint32_t flags, int device, tq_inde
     h->upload(h->d_perm_sign.get(), ps.data(), dim * 4);
     h->upload(h->d_bnd.get(), bnd.data(), 64);
     h->upload(h->d_cen.get(), cen.data(), 64);
+    if (vcb::make_code_grid(h->cb.boundaries, &h->grid)) {
+      std::vector<uint32_t> cells(2 * vcb::CodeGrid::kCells);
+      for (int j = 0; j < vcb::CodeGrid::kCells; ++j) {
+        cells[2 * j] = h->grid.base[j];
+        std::memcpy(&cells[2 * j + 1], &h->grid.inner[j], 4);
+      }
+      h->d_grid.reserve(cells.size() * 4);
+      h->upload(h->d_grid.get(), cells.data(), cells.size() * 4);
+      h->has_grid = true;
+    }
     vcb::check(cudaMemsetAsync(h->d_counter.get(), 0, 8, h->stream), "cudaMemsetAsync");
     h->sync();
     *out = h.release();

@@ -166,6 +166,8 @@ struct tq_index {
   size_t dim = 0, bits = 0, nbg = 0, block = 0;
   float inv_sqrt_block = 0.f;
   vcb::Codebook cb;
+  vcb::CodeGrid grid;     // the codebook's code grid (encode), when has_grid
+  bool has_grid = false;
   bool calibrated = false;
   std::vector<float> shift, scale;
   bool prepared = false;
@@ -173,7 +175,7 @@ struct tq_index {
   size_t staged_n = 0;   // rows waiting for prepare()
   size_t cap = 0;        // layout capacity in vectors (multiple of kScanBlockVectors)
 
-  vcb::DeviceBuffer d_perm_sign, d_bnd, d_cen, d_shift, d_scale, d_inv_scale;
+  vcb::DeviceBuffer d_perm_sign, d_bnd, d_cen, d_grid, d_shift, d_scale, d_inv_scale;
   vcb::DeviceBuffer d_codes, d_alpha, d_staged, d_flat, d_counter;
   // search scratch
   vcb::DeviceBuffer d_queries, d_luts, d_qf, d_cand_s, d_cand_i, d_out_s, d_out_i, d_qrot, d_partial;
@@ -292,6 +294,13 @@ struct tq_index {
       a.flat_stride = static_cast<int>(stride);
       a.out_alpha = d_alpha.as<float>() + n + done;
       a.replay_count = d_counter.as<unsigned long long>();
+      if (has_grid) {
+        a.grid = d_grid.as<uint2>();
+        a.grid_lo = grid.lo;
+        a.grid_hi = grid.hi;
+        a.grid_a = grid.a;
+        a.grid_k = grid.k;
+      }
       launch(kEncode, s, "encode kernel", [&] { return vcb::launch_encode(a, sms, s); });
       vcb::RelayoutArgs r{};
       r.flat = d_flat.as<uint8_t>();

@@ -34,6 +34,11 @@ struct EncodeArgs {
   int flat_stride;
   float* out_alpha;
   unsigned long long* replay_count;  // optional: vectors whose alpha needed the exact replay
+  // Code grid of the boundaries (CodeGrid in tq_host_math.h): CodeGrid::kCells
+  // entries {base code, inner boundary bits} and its parameters. nullptr: the
+  // per-warp row kernel with the binary search encodes.
+  const uint2* grid = nullptr;
+  float grid_lo = 0.f, grid_hi = 0.f, grid_a = 0.f, grid_k = 0.f;
 };
 
 struct RelayoutArgs {
@@ -103,6 +108,9 @@ struct ScanArgs {
   // stores a block's last batch sums flushes that block in the same launch.
   // nullptr: a second launch flushes every block.
   unsigned* arrive = nullptr;
+  // Always 1: the one- and two-query kernels add byte sums as multiply-adds
+  // by this value, which the compiler cannot fold into plain additions.
+  uint32_t one = 1;
 };
 
 struct MergeArgs {

@@ -157,6 +157,36 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [Q][chunk][2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+  // One or two queries per CTA leave the ALU pipe (lookups) the bottleneck
+  // with the FMA pipe mostly idle: there the selector shifts run as mul.hi
+  // and the byte-sum additions as multiply-adds by an opaque 1 (a.one), both
+  // on the FMA pipe. With four queries the dp4a accumulation already keeps the
+  // FMA pipe busy and both stay ALU integer operations.
+  constexpr bool kFmaSide = Q <= 2;
+  const uint32_t one = a.one;
+  auto hi16 = [&](uint32_t x) -> uint32_t {
+    if constexpr (kFmaSide) {
+      return __umulhi(x, 0x10000u);
+    } else {
+      return x >> 16;
+    }
+  };
+  auto add2 = [&](uint32_t x, uint32_t y) -> uint32_t {
+    if constexpr (kFmaSide) {
+      uint32_t d;
+      asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(x), "r"(one), "r"(y));
+      return d;
+    } else {
+      return x + y;
+    }
+  };
+  auto add4 = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t {
+    if constexpr (kFmaSide) {
+      return add2(x, add2(y, add2(z, w)));
+    } else {
+      return x + y + z + w;
+    }
+  };
   const long long q0 = static_cast<long long>(blockIdx.x) * Q;
   const int range = blockIdx.y;
   const long long v_begin = static_cast<long long>(range) * a.range_vectors;
@@ -270,17 +300,17 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         for (int u = 0; u < PF; u += 2) {
           if (g + u >= g_stop) break;
           const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
-          const uint32_t a0h = a0 >> 16, a1h = a1 >> 16, b0h = b0 >> 16, b1h = b1 >> 16;
+          const uint32_t a0h = hi16(a0), a1h = hi16(a1), b0h = hi16(b0), b1h = hi16(b1);
           uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
           if constexpr (!NIBBLE8) {
             ta0 = a0 ^ 0x88888888u;
             ta1 = a1 ^ 0x88888888u;
             tb0 = b0 ^ 0x88888888u;
             tb1 = b1 ^ 0x88888888u;
-            ta0h = ta0 >> 16;
-            ta1h = ta1 >> 16;
-            tb0h = tb0 >> 16;
-            tb1h = tb1 >> 16;
+            ta0h = hi16(ta0);
+            ta1h = hi16(ta1);
+            tb0h = hi16(tb0);
+            tb1h = hi16(tb1);
           }
           const LutHalf* lg = s_lut + (g + u - chunk_base) * 2;
 #pragma unroll
@@ -292,19 +322,19 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
             uint32_t lo0, hi0, lo1, hi1;
             if constexpr (NIBBLE8) {
               // 3-bit codes: every nibble is < 8, entries 8..15 are never used.
-              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sb.w[0], Sb.w[1], b0);
-              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fb.w[0], Fb.w[1], b0h);
-              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sb.w[0], Sb.w[1], b1);
-              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fb.w[0], Fb.w[1], b1h);
+              lo0 = add2(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sb.w[0], Sb.w[1], b0));
+              hi0 = add2(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fb.w[0], Fb.w[1], b0h));
+              lo1 = add2(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sb.w[0], Sb.w[1], b1));
+              hi1 = add2(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fb.w[0], Fb.w[1], b1h));
             } else {
-              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sa.w[2], Sa.w[3], ta0) +
-                    prmt(Sb.w[0], Sb.w[1], b0) + prmt(Sb.w[2], Sb.w[3], tb0);
-              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fa.w[2], Fa.w[3], ta0h) +
-                    prmt(Fb.w[0], Fb.w[1], b0h) + prmt(Fb.w[2], Fb.w[3], tb0h);
-              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sa.w[2], Sa.w[3], ta1) +
-                    prmt(Sb.w[0], Sb.w[1], b1) + prmt(Sb.w[2], Sb.w[3], tb1);
-              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fa.w[2], Fa.w[3], ta1h) +
-                    prmt(Fb.w[0], Fb.w[1], b1h) + prmt(Fb.w[2], Fb.w[3], tb1h);
+              lo0 = add4(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sa.w[2], Sa.w[3], ta0), prmt(Sb.w[0], Sb.w[1], b0),
+                         prmt(Sb.w[2], Sb.w[3], tb0));
+              hi0 = add4(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fa.w[2], Fa.w[3], ta0h), prmt(Fb.w[0], Fb.w[1], b0h),
+                         prmt(Fb.w[2], Fb.w[3], tb0h));
+              lo1 = add4(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sa.w[2], Sa.w[3], ta1), prmt(Sb.w[0], Sb.w[1], b1),
+                         prmt(Sb.w[2], Sb.w[3], tb1));
+              hi1 = add4(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fa.w[2], Fa.w[3], ta1h), prmt(Fb.w[0], Fb.w[1], b1h),
+                         prmt(Fb.w[2], Fb.w[3], tb1h));
             }
             // [lo.b0, hi.b0, lo.b1, hi.b1] and [lo.b2, hi.b2, lo.b3, hi.b3]
             const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
