@@ -678,10 +678,11 @@ BUCKETED_METRIC = "QPS at Recall@10 >= 0.95 (bucketed 1.2Mx100 4-bit cosine, lea
 PROBE_CLASSES = (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048)
 FIXED_PROBES = (64, 128, 256, 384, 512, 768, 1024, 1536, 2048)
 FINE_STEP = 16  # fixed n_probe grid step below the first coarse point reaching the target
+LEARNED_ABOVE = (512, 640, 768)  # learned-probe classes above the fixed operating point
 RECALL_TARGET = 0.95
 # Prediction-rule sweeps of the learned n_probe, fewest buckets first:
 # trade-offs (recall objective) and coverages (classes objective).
-PROBE_RULES = {"recall": (0.3, 0.2, 0.15, 0.12, 0.1, 0.08, 0.06, 0.04, 0.02),
+PROBE_RULES = {"recall": (0.3, 0.2, 0.15, 0.12, 0.1, 0.08, 0.06, 0.04, 0.03, 0.02, 0.015, 0.01, 0.005),
                "classes": (0.5, 0.7, 0.8, 0.9, 0.95, 0.98)}
 
 
@@ -818,7 +819,12 @@ def run_bucketed(args, world, rank, local):
     fixed = sweep[p_op]
     recall_fixed = fixed["recall_at_10"]
     fixed_ms = fixed["ms_per_step"]
-    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,)  # the operating point is the largest class
+    # Candidate n_probe values: the listed ones below the operating point, the
+    # operating point itself, and a few above it, so that the recall objective
+    # can spend more buckets on hard queries than the fixed path does.
+    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,) + tuple(
+        c for c in LEARNED_ABOVE if c > p_op)
+    p_max = classes[-1]
 
     # labels from the plain index (reference n_probe = the operating point) and GPU training
     t0 = time.perf_counter()
@@ -839,13 +845,13 @@ def run_bucketed(args, world, rank, local):
         def learned_step(rule=rule):
             # one routing pass feeds the network and the probes
             idx.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, min_confidence=0.0,
-                                      fallback_n_probe=p_op, stream=stream)
+                                      fallback_n_probe=p_max, stream=stream)
 
         ms = timed(learned_step)
         r = float(recall_rows(d_i.cpu().numpy(), ex_test, k).mean())
         # the per-query probe counts of that search (recomputed outside the timed region)
         idx.route_device(d_q, 256, te_s, te_i, stream=stream)
-        mlp.predict_device(te_s, nq, 256, npq, coverage=rule, min_confidence=0.0, fallback=p_op, stream=stream)
+        mlp.predict_device(te_s, nq, 256, npq, coverage=rule, min_confidence=0.0, fallback=p_max, stream=stream)
         mean_probe = float(npq.float().mean().item())
         cand = {"rule": rule, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
                 "mean_n_probe": mean_probe}
@@ -871,7 +877,7 @@ def run_bucketed(args, world, rank, local):
     fixed["kernel_ms"] = kernel_ms(lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, stream=stream))
     if best:
         best["kernel_ms"] = kernel_ms(lambda: idx.search_learned_device(
-            d_q, k, mlp, d_s, d_i, coverage=best["rule"], min_confidence=0.0, fallback_n_probe=p_op,
+            d_q, k, mlp, d_s, d_i, coverage=best["rule"], min_confidence=0.0, fallback_n_probe=p_max,
             stream=stream))
     clk.__exit__()
     line = {

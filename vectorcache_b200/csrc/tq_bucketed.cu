@@ -393,14 +393,14 @@ struct tq_bucketed {
 
   // Queries per pass: routing scores (nb floats per query) within 256 MiB and
   // candidate lists (max_probe lists of kscan (score, id) per query) within
-  // 4 GiB — 10,485 queries at 512 probes and a re-rank of 100. Every pass
+  // 8 GiB — 13,981 queries at 768 probes and a re-rank of 100. Every pass
   // repeats the routing, pair and floor launches on a smaller grid: at 1 GiB
   // with two lists per probe the same search ran in 8 passes and took 1.7x
   // as long for 64 probes per query under a 512-probe cap.
   size_t pass_queries(size_t max_probe = 1, size_t kscan = 1) const {
     const size_t by_route = std::max<size_t>(1, (size_t{256} << 20) / (static_cast<size_t>(nb) * 4));
     const size_t by_cand =
-        std::max<size_t>(1, (size_t{4} << 30) / (max_probe * vcb::kBsListsPerProbe * kscan * 8));
+        std::max<size_t>(1, (size_t{8} << 30) / (max_probe * vcb::kBsListsPerProbe * kscan * 8));
     return std::min<size_t>({16384, by_route, by_cand});
   }
 

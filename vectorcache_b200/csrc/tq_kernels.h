@@ -108,9 +108,6 @@ struct ScanArgs {
   // stores a block's last batch sums flushes that block in the same launch.
   // nullptr: a second launch flushes every block.
   unsigned* arrive = nullptr;
-  // Always 1: the one- and two-query kernels add byte sums as multiply-adds
-  // by this value, which the compiler cannot fold into plain additions.
-  uint32_t one = 1;
 };
 
 struct MergeArgs {

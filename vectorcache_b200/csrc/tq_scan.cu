@@ -158,12 +158,12 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   // One or two queries per CTA leave the ALU pipe (lookups) the bottleneck
-  // with the FMA pipe mostly idle: there the selector shifts run as mul.hi
-  // and the byte-sum additions as multiply-adds by an opaque 1 (a.one), both
-  // on the FMA pipe. With four queries the dp4a accumulation already keeps the
-  // FMA pipe busy and both stay ALU integer operations.
+  // with the FMA-heavy pipe lightly used: there the selector shifts run as
+  // mul.hi on the FMA-heavy pipe. (Moving the byte-sum additions there too, as
+  // multiply-adds, overloaded it: measured 0.187 -> 0.195 ms at 1M x 1536.)
+  // With four queries the dp4a accumulation keeps that pipe busy and the
+  // shifts stay ALU operations.
   constexpr bool kFmaSide = Q <= 2;
-  const uint32_t one = a.one;
   auto hi16 = [&](uint32_t x) -> uint32_t {
     if constexpr (kFmaSide) {
       return __umulhi(x, 0x10000u);
@@ -171,22 +171,8 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
       return x >> 16;
     }
   };
-  auto add2 = [&](uint32_t x, uint32_t y) -> uint32_t {
-    if constexpr (kFmaSide) {
-      uint32_t d;
-      asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(x), "r"(one), "r"(y));
-      return d;
-    } else {
-      return x + y;
-    }
-  };
-  auto add4 = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t {
-    if constexpr (kFmaSide) {
-      return add2(x, add2(y, add2(z, w)));
-    } else {
-      return x + y + z + w;
-    }
-  };
+  auto add2 = [&](uint32_t x, uint32_t y) -> uint32_t { return x + y; };
+  auto add4 = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t { return x + y + z + w; };
   const long long q0 = static_cast<long long>(blockIdx.x) * Q;
   const int range = blockIdx.y;
   const long long v_begin = static_cast<long long>(range) * a.range_vectors;
