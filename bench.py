@@ -680,6 +680,7 @@ FIXED_PROBES = (64, 128, 256, 384, 512, 768, 1024, 1536, 2048)
 FINE_STEP = 16  # fixed n_probe grid step below the first coarse point reaching the target
 LEARNED_ABOVE = (512, 640, 768)  # learned-probe classes above the fixed operating point
 RECALL_TARGET = 0.95
+BISECT_STEPS = 5  # trade-off bisection steps of the learned n_probe
 # Prediction-rule sweeps of the learned n_probe, fewest buckets first:
 # trade-offs (recall objective) and coverages (classes objective).
 PROBE_RULES = {"recall": (0.3, 0.2, 0.15, 0.12, 0.1, 0.08, 0.06, 0.04, 0.03, 0.02, 0.015, 0.01, 0.005),
@@ -841,8 +842,12 @@ def run_bucketed(args, world, rank, local):
     npq = torch.empty(nq, dtype=torch.int32, device=device)
     best = None
     learned_sweep = []
-    for rule in PROBE_RULES[objective]:
-        def learned_step(rule=rule):
+    target = min(RECALL_TARGET, recall_fixed)
+
+    def learned_point(rule):
+        nonlocal best
+
+        def learned_step():
             # one routing pass feeds the network and the probes
             idx.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, min_confidence=0.0,
                                       fallback_n_probe=p_max, stream=stream)
@@ -856,8 +861,27 @@ def run_bucketed(args, world, rank, local):
         cand = {"rule": rule, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
                 "mean_n_probe": mean_probe}
         learned_sweep.append(cand)
-        if r >= min(RECALL_TARGET, recall_fixed) and (best is None or cand["qps"] > best["qps"]):
+        if r >= target and (best is None or cand["qps"] > best["qps"]):
             best = cand
+        return cand
+
+    for rule in PROBE_RULES[objective]:
+        learned_point(rule)
+    # The recall falls as the trade-off grows: bisect between the largest grid
+    # value that meets the target and the next larger one that misses it.
+    meets = [c["rule"] for c in learned_sweep if c["recall_at_10"] >= target]
+    misses = [c["rule"] for c in learned_sweep if c["recall_at_10"] < target]
+    if meets and misses and objective == "recall":
+        lo = max(meets)
+        above = [r for r in misses if r > lo]
+        if above:
+            hi = min(above)
+            for _ in range(BISECT_STEPS):
+                mid = 0.5 * (lo + hi)
+                if learned_point(mid)["recall_at_10"] >= target:
+                    lo = mid
+                else:
+                    hi = mid
     qps_fixed = nq / (fixed_ms / 1e3)
 
     # Device time per kernel class of one search at each operating point.

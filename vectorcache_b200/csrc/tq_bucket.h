@@ -167,6 +167,7 @@ struct BucketScanArgs {
   const float* offsets;
   const uint4* items;
   const unsigned long long* n_items;
+  unsigned long long* next_item;  // work counter (zeroed by launch_bucket_scan)
   int nbg, bits, k, max_probe;
   float* cand_score;         // (nq * max_probe * kBsListsPerProbe) lists of k
   uint32_t* cand_id;
@@ -179,6 +180,7 @@ struct BucketScanArgs {
   // counts them. nullptr: one -inf padded list of k per (query, probe, tile set).
   uint32_t* append_count = nullptr;
 };
+// `grid`: a bound of the item count; the launch runs min(grid, resident CTAs).
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
 // floor[q] = the k-th score of the merged top k of the first probes (a lower
 // bound of the k-th best over all probes), -inf when that top k is not full

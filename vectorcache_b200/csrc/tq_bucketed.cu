@@ -453,7 +453,7 @@ struct tq_bucketed {
       sc.pairs.reserve(m * max_probe * 4);
       sc.off.reserve(m * max_probe * 4);
       sc.items.reserve(static_cast<size_t>(items) * 16);
-      sc.nitems.reserve(8);
+      sc.nitems.reserve(16);  // item count, then the scan's work counter
       vcb::PairArgs pa{};
       pa.probes = sc.top_i.as<uint32_t>();
       pa.probe_stride = ptop;
@@ -497,6 +497,7 @@ struct tq_bucketed {
       ba.offsets = pa.offsets;
       ba.items = pa.items;
       ba.n_items = pa.n_items;
+      ba.next_item = pa.n_items + 1;
       ba.nbg = static_cast<int>(nbg);
       ba.bits = static_cast<int>(bits);
       ba.k = static_cast<int>(kscan);

@@ -45,9 +45,6 @@ constexpr int kMaxClasses = 32;
 
 using bf16 = __nv_bfloat16;
 
-__device__ __forceinline__ float ld(const float* p, long long i) { return p[i]; }
-__device__ __forceinline__ float ld(const bf16* p, long long i) { return __bfloat162float(p[i]); }
-
 // Raw features -> standardized bf16 inputs. top: m x p (p <= 256) scores
 // best first; missing scores (p < 256 or -inf) repeat the last valid one.
 __global__ void features_kernel(const float* __restrict__ top, long long m, int p, const float* __restrict__ mu,

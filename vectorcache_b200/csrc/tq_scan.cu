@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <climits>
+#include <type_traits>
 
 #include "tq_kernels.h"
 #include "tq_device.cuh"
@@ -157,22 +158,13 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [Q][chunk][2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // One or two queries per CTA leave the ALU pipe (lookups) the bottleneck
-  // with the FMA-heavy pipe lightly used: there the selector shifts run as
-  // mul.hi on the FMA-heavy pipe. (Moving the byte-sum additions there too, as
-  // multiply-adds, overloaded it: measured 0.187 -> 0.195 ms at 1M x 1536.)
-  // With four queries the dp4a accumulation keeps that pipe busy and the
-  // shifts stay ALU operations.
-  constexpr bool kFmaSide = Q <= 2;
-  auto hi16 = [&](uint32_t x) -> uint32_t {
-    if constexpr (kFmaSide) {
-      return __umulhi(x, 0x10000u);
-    } else {
-      return x >> 16;
-    }
-  };
-  auto add2 = [&](uint32_t x, uint32_t y) -> uint32_t { return x + y; };
-  auto add4 = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t { return x + y + z + w; };
+  // Selector helpers. (Measured at 1M x 1536 one query: moving the shifts to
+  // the FMA-heavy pipe as mul.hi, 0.187 -> 0.191 ms, or the byte-sum additions
+  // as multiply-adds as well, -> 0.195 ms, only moved the bottleneck there:
+  // the dp4a accumulation and the compiler's own IMADs already use it.)
+  auto hi16 = [](uint32_t x) -> uint32_t { return x >> 16; };
+  auto add2 = [](uint32_t x, uint32_t y) -> uint32_t { return x + y; };
+  auto add4 = [](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t { return x + y + z + w; };
   const long long q0 = static_cast<long long>(blockIdx.x) * Q;
   const int range = blockIdx.y;
   const long long v_begin = static_cast<long long>(range) * a.range_vectors;
@@ -265,29 +257,20 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         __syncthreads();
       }
       const int chunk_base = kBatch ? g_first : (resident ? 0 : (gb / chunk) * chunk);
-      uint2 ring[PF];
-#pragma unroll
-      for (int u = 0; u < PF; ++u) {
-        ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
-      }
-      for (int g = gb; g < g_stop; g += PF) {
-        uint2 cur[PF];
-#pragma unroll
-        for (int u = 0; u < PF; ++u) {
-          cur[u] = ring[u];
-          const int gn = g + PF + u;
-          ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
-        }
-        // Byte groups in pairs (nbg and every 256-group batch are even): the
-        // second-half lookups of both groups add into one byte per vector
-        // (<= 2 * 127), the first-half lookups into another; one prmt
-        // interleaves the two bytes of each vector so a single dp4a adds both.
+      // The lookups of PF code groups held in `cur`, starting at group g
+      // (CHECKED: only those below g_stop). Byte groups in pairs (nbg and every 256-group
+      // batch are even): the second-half lookups of both groups add into one
+      // byte per vector (<= 2 * 127), the first-half lookups into another; one
+      // prmt interleaves the two bytes of each vector so a single dp4a adds both.
+      auto process = [&](const uint2 (&cur)[PF], int g, auto checked) {
 #pragma unroll
         for (int u = 0; u < PF; u += 2) {
-          if (g + u >= g_stop) break;
+          if constexpr (decltype(checked)::value) {
+            if (g + u >= g_stop) break;
+          }
           const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
           const uint32_t a0h = hi16(a0), a1h = hi16(a1), b0h = hi16(b0), b1h = hi16(b1);
-          uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
+          [[maybe_unused]] uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
           if constexpr (!NIBBLE8) {
             ta0 = a0 ^ 0x88888888u;
             ta1 = a1 ^ 0x88888888u;
@@ -334,6 +317,45 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
             acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
             acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
           }
+        }
+      };
+      uint2 ring[PF];
+      // One or two queries: whole rings (every 256-group batch of a 4- or
+      // 3-bit row of 512+ dims) run without bounds checks, loading at
+      // immediate offsets of a running pointer. Four queries keep the checked
+      // loop: the second copy of the lookup body does not fit their 128
+      // registers.
+      if (Q <= 2 && (g_stop - gb) % PF == 0) {
+        const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
+#pragma unroll
+        for (int u = 0; u < PF; ++u) ring[u] = src[u * kGroupStride];
+        src += PF * kGroupStride;
+        int g = gb;
+        for (; g + PF < g_stop; g += PF) {
+          uint2 cur[PF];
+#pragma unroll
+          for (int u = 0; u < PF; ++u) {
+            cur[u] = ring[u];
+            ring[u] = src[u * kGroupStride];
+          }
+          src += PF * kGroupStride;
+          process(cur, g, std::false_type{});
+        }
+        process(ring, g, std::false_type{});
+      } else {
+#pragma unroll
+        for (int u = 0; u < PF; ++u) {
+          ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
+        }
+        for (int g = gb; g < g_stop; g += PF) {
+          uint2 cur[PF];
+#pragma unroll
+          for (int u = 0; u < PF; ++u) {
+            cur[u] = ring[u];
+            const int gn = g + PF + u;
+            ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+          }
+          process(cur, g, std::true_type{});
         }
       }
       // f32 flush of this batch (search_avx2.cpp:24-48).
