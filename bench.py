@@ -896,13 +896,19 @@ def run_bucketed(args, world, rank, local):
         torch.cuda.synchronize()
         prof = eng.read_profile()
         eng.set_profiling(False)
-        return {"prep_route_pairs": prof["prep_ms"], "bucket_scan": prof["scan_ms"], "merge_rerank": prof["merge_ms"]}
+        return {"prep_route_pairs": prof["prep_ms"], "bucket_scan": prof["scan_ms"], "merge_rerank": prof["merge_ms"],
+                "by_launch": {name: round(ms, 4) for name, (ms, _) in prof["by_launch"].items()}}
 
     fixed["kernel_ms"] = kernel_ms(lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=p_op, stream=stream))
     if best:
         best["kernel_ms"] = kernel_ms(lambda: idx.search_learned_device(
             d_q, k, mlp, d_s, d_i, coverage=best["rule"], min_confidence=0.0, fallback_n_probe=p_max,
             stream=stream))
+        # the plain path at the swept n_probe nearest the learned mean: what the
+        # per-query counts cost beyond their mean
+        near = min(sweep, key=lambda p: abs(p - best["mean_n_probe"]))
+        sweep[near]["kernel_ms"] = kernel_ms(
+            lambda: idx.search_device(d_q, k, d_s, d_i, n_probe=near, stream=stream))
     clk.__exit__()
     line = {
         "metric": BUCKETED_METRIC, "value": best["qps"] if best else None, "unit": "queries/s", "n_gpus": 1,
@@ -981,32 +987,59 @@ def run_serving(args, world, rank, local):
     ex_test, ex_train = exact(test_q), exact(train_q)
     del x
     torch.cuda.empty_cache()
-    # fixed operating point: smallest n_probe with Recall@10 >= 0.95
+    # fixed operating point: smallest n_probe with Recall@10 >= 0.95 (the
+    # coarse grid, then steps of FINE_STEP below its first point reaching it)
+    def fixed_recall(p):
+        return recall_rows(bkt.search(test_q, k, n_probe=p).ids, ex_test, k).mean()
+
     p_op = FIXED_PROBES[-1]
     for p in FIXED_PROBES:
-        if recall_rows(bkt.search(test_q, k, n_probe=p).ids, ex_test, k).mean() >= RECALL_TARGET:
+        if fixed_recall(p) >= RECALL_TARGET:
             p_op = p
             break
-    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,)  # the operating point is the largest class
+    below = [p for p in FIXED_PROBES if p < p_op]
+    for p in range((below[-1] if below else 0) + FINE_STEP, p_op, FINE_STEP):
+        if fixed_recall(p) >= RECALL_TARGET:
+            p_op = p
+            break
+    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,) + tuple(
+        c for c in LEARNED_ABOVE if c > p_op)
+    p_max = classes[-1]
     labels, rec = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
     objective = args.probe_objective
     mlp, _ = train_probe_mlp(bkt, train_q, labels, rec, classes, objective, args.epochs, device, local)
-    # learned operating point: the rule with the fewest buckets whose Recall@10 reaches the target
-    cov_op = PROBE_RULES[objective][-1]
+    # learned operating point: the rule with the fewest buckets whose Recall@10
+    # reaches the target (grid, then bisection of the recall objective's trade-off)
     d_q = torch.from_numpy(test_q).to(device)
     d_s = torch.empty((nq, k), dtype=torch.float32, device=device)
     d_i = torch.empty((nq, k), dtype=torch.int64, device=device)
-    for rule in PROBE_RULES[objective]:
-        bkt.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, fallback_n_probe=p_op)
+
+    def learned_recall(rule):
+        bkt.search_learned_device(d_q, k, mlp, d_s, d_i, coverage=rule, fallback_n_probe=p_max)
         torch.cuda.synchronize()
-        if recall_rows(d_i.cpu().numpy(), ex_test, k).mean() >= RECALL_TARGET:
+        return recall_rows(d_i.cpu().numpy(), ex_test, k).mean()
+
+    rules = PROBE_RULES[objective]
+    cov_op, missed = rules[-1], None
+    for rule in rules:
+        if learned_recall(rule) >= RECALL_TARGET:
             cov_op = rule
             break
+        missed = rule
+    if objective == "recall" and missed is not None:
+        lo, hi = cov_op, missed
+        for _ in range(BISECT_STEPS):
+            mid = 0.5 * (lo + hi)
+            if learned_recall(mid) >= RECALL_TARGET:
+                lo = mid
+            else:
+                hi = mid
+        cov_op = lo
 
     srv = vcb.Server(device=local, hbm_budget_bytes=120 << 30, max_slots=4, max_batch=1024)
     t_flat = srv.add_flat(flat, 64)
     t_fixed = srv.add_bucketed(bkt, 64, p_op)
-    t_learn = srv.add_bucketed(bkt, 64, p_op, mlp=mlp, coverage=cov_op)
+    t_learn = srv.add_bucketed(bkt, 64, p_max, mlp=mlp, coverage=cov_op)
     srv.start()
     info = srv.info()
     rng = np.random.default_rng(11)
@@ -1055,8 +1088,8 @@ def run_serving(args, world, rank, local):
         "config": {"workload": f"serving: flat {flat_n}x{flat_dim} 3-bit + bucketed {n}x{dim} 4-bit, HBM budget "
                                f"120 GB, rates {list(SERVING_RATES)} q/s", "slots": info["slots"],
                    "slot_bytes": info["slot_bytes"], "resident_bytes": info["resident_bytes"],
-                   "fixed_n_probe": p_op, "learned_rule": cov_op, "probe_objective": objective,
-                   "flat_build_s": flat_build_s},
+                   "fixed_n_probe": p_op, "learned_max_n_probe": p_max, "learned_rule": cov_op,
+                   "probe_objective": objective, "flat_build_s": flat_build_s},
         "per_rate": per_rate, "server_stats": srv.stats(), "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

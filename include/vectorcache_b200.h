@@ -204,6 +204,13 @@ typedef struct tq_profile {
 
 int tq_index_set_profiling(tq_index* h, int enabled);
 int tq_index_read_profile(tq_index* h, tq_profile* out);
+/* The launches timed up to the last tq_index_read_profile, per launch name
+ * (e.g. "bucket scan kernel", "pair kernels", "probe network"), in first-seen
+ * order: entry i's name (truncated to name_cap - 1 bytes, NUL-terminated),
+ * device time and launch count. */
+int tq_index_profile_entries(const tq_index* h, size_t* n);
+int tq_index_profile_entry(const tq_index* h, size_t i, char* name, size_t name_cap, double* ms,
+                           uint64_t* launches);
 
 /* ---- bucketed (IVF) index ---------------------------------------------------
  * BucketedTurboQuantIndex / BucketParams of the reference's README

@@ -116,3 +116,19 @@ def test_against_oracle(oracle, case):
             ws, wi = oracle.topk(want_scores[:m], k)
             assert np.array_equal(res.ids, wi), (m, k)
             assert bits_equal(res.scores, ws), (m, k)
+
+
+def test_profile_by_launch():
+    """Profiling mode times every launch: per class and per launch name."""
+    db = power_law(3000, 256, seed=5)
+    idx = build_index(db, 4)
+    q = power_law(8, 256, seed=6)
+    idx.set_profiling(True)
+    idx.read_profile()
+    idx.search(q, 10)
+    prof = idx.read_profile()
+    idx.set_profiling(False)
+    by = prof["by_launch"]
+    assert by["scan kernel"][1] >= 1 and by["query prep kernel"][1] >= 1
+    assert sum(ms for ms, _ in by.values()) == pytest.approx(prof["prep_ms"] + prof["scan_ms"] + prof["merge_ms"])
+    assert idx.read_profile()["by_launch"] == {}

@@ -114,6 +114,9 @@ def _declare(lib):
         "tq_index_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
         "tq_index_set_profiling": (C.c_int, [_P, C.c_int]),
         "tq_index_read_profile": (C.c_int, [_P, C.POINTER(Profile)]),
+        "tq_index_profile_entries": (C.c_int, [_P, C.POINTER(_SZ)]),
+        "tq_index_profile_entry": (C.c_int, [_P, _SZ, C.c_char_p, _SZ, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -392,9 +395,21 @@ class TurboQuantIndex:
         _check(self._lib.tq_index_set_profiling(self._h, int(bool(enabled))))
 
     def read_profile(self) -> dict:
+        """Device time per launch class since the last read, and under
+        "by_launch" per launch name: {name: (ms, launches)}."""
         prof = Profile()
         _check(self._lib.tq_index_read_profile(self._h, C.byref(prof)))
-        return prof.as_dict()
+        out = prof.as_dict()
+        n = _SZ()
+        _check(self._lib.tq_index_profile_entries(self._h, C.byref(n)))
+        by = {}
+        name = C.create_string_buffer(64)
+        for i in range(n.value):
+            ms, cnt = C.c_double(), C.c_uint64()
+            _check(self._lib.tq_index_profile_entry(self._h, i, name, 64, C.byref(ms), C.byref(cnt)))
+            by[name.value.decode()] = (ms.value, cnt.value)
+        out["by_launch"] = by
+        return out
 
     def replay_count(self) -> int:
         c = C.c_uint64()

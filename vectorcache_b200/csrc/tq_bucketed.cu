@@ -559,8 +559,9 @@ struct tq_bucketed {
           pa.first_split = st == 0 ? 0 : 1;
           const long long step_items =
               vcb::max_items(static_cast<long long>(m), steps[st + 1] - steps[st], nb);
-          eng->launch(tq_index::kPrep, s, "pair kernels", [&] { return vcb::launch_build_pairs(pa, s); });
-          eng->launch(tq_index::kScan, s, "bucket scan kernel",
+          eng->launch(tq_index::kPrep, s, "pair kernels (first probes)",
+                      [&] { return vcb::launch_build_pairs(pa, s); });
+          eng->launch(tq_index::kScan, s, "bucket scan kernel (first probes)",
                       [&] { return vcb::launch_bucket_scan(ba, std::min(items, step_items), s); });
           eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
             cudaError_t e = vcb::launch_merge(fm, s);

@@ -497,11 +497,20 @@ int tq_index_read_profile(tq_index* h, tq_profile* out) {
     vcb::DeviceGuard g(h->device);
     tq_profile p{};
     double* ms[4] = {&p.prep_ms, &p.scan_ms, &p.merge_ms, &p.encode_ms};
+    h->last_by_name.clear();
     for (auto& t : h->timed_launches) {
       vcb::check(cudaEventSynchronize(t.stop), "cudaEventSynchronize");
       float e = 0.f;
       vcb::check(cudaEventElapsedTime(&e, t.start, t.stop), "cudaEventElapsedTime");
       *ms[t.kind] += e;
+      auto named = std::find_if(h->last_by_name.begin(), h->last_by_name.end(),
+                                [&](const tq_index::NamedTime& n) { return n.what == t.what; });
+      if (named == h->last_by_name.end()) {
+        h->last_by_name.push_back({t.what, 0.0, 0});
+        named = h->last_by_name.end() - 1;
+      }
+      named->ms += e;
+      ++named->launches;
       h->event_pool.push_back(t.start);
       h->event_pool.push_back(t.stop);
     }
@@ -516,6 +525,27 @@ int tq_index_read_profile(tq_index* h, tq_profile* out) {
     h->scan_stream_bytes = 0;
     h->scan_queries = 0;
     *out = p;
+  });
+}
+
+int tq_index_profile_entries(const tq_index* h, size_t* n) {
+  return vcb::guarded([&] {
+    require(h && n, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    *n = h->last_by_name.size();
+  });
+}
+
+int tq_index_profile_entry(const tq_index* h, size_t i, char* name, size_t name_cap, double* ms,
+                           uint64_t* launches) {
+  return vcb::guarded([&] {
+    require(h && name && ms && launches && name_cap > 0, TQ_ERR_INVALID_ARGUMENT, "null argument");
+    require(i < h->last_by_name.size(), TQ_ERR_INVALID_ARGUMENT, "profile entry out of range");
+    const auto& e = h->last_by_name[i];
+    const size_t len = std::min(e.what.size(), name_cap - 1);
+    std::memcpy(name, e.what.data(), len);
+    name[len] = '\0';
+    *ms = e.ms;
+    *launches = e.launches;
   });
 }
 

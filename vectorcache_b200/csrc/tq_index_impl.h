@@ -184,11 +184,18 @@ struct tq_index {
   enum Kind { kPrep = 0, kScan = 1, kMerge = 2, kEncode = 3 };
   struct Timed {
     int kind;
+    const char* what;  // a string literal naming the launch
     cudaEvent_t start, stop;
+  };
+  struct NamedTime {
+    std::string what;
+    double ms;
+    uint64_t launches;
   };
   bool profiling = false;
   std::vector<cudaEvent_t> event_pool;
   std::vector<Timed> timed_launches;
+  std::vector<NamedTime> last_by_name;  // per launch name, as of the last read
   uint64_t launches[4] = {0, 0, 0, 0};
   uint64_t scan_stream_bytes = 0, scan_queries = 0;
 
@@ -225,7 +232,7 @@ struct tq_index {
       vcb::check(fn(), what);
       return;
     }
-    Timed t{kind, take_event(), take_event()};
+    Timed t{kind, what, take_event(), take_event()};
     vcb::check(cudaEventRecord(t.start, s), "cudaEventRecord");
     vcb::check(fn(), what);
     vcb::check(cudaEventRecord(t.stop, s), "cudaEventRecord");
