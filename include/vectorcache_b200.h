@@ -176,12 +176,14 @@ int tq_index_replay_count(const tq_index* h, uint64_t* count);
 /* The scan plan a search of nq queries with this k would use: queries per
  * CTA, vector ranges (one CTA per query group and range), vectors per range
  * (a multiple of the 2048-vector scan block), and the number of 256-group
- * batches a one- or two-query scan splits into (1: no split). The reference
- * tiles its scan over <= 4 or <= 8 queries and block ranges
- * (src/search/search.cpp:600-758); this reports the device's tiling, for
- * tests that need a given tiling and for measurements. */
+ * batches a one- or two-query scan splits into (1: no split), and the
+ * shared-memory slots per warp its code stream goes through (0: a register
+ * prefetch ring). The reference tiles its scan over <= 4 or <= 8 queries and
+ * block ranges (src/search/search.cpp:600-758); this reports the device's
+ * tiling, for tests that need a given tiling and for measurements. Any out
+ * pointer may be null. */
 int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, int* n_ranges,
-                       uint64_t* range_vectors, int* split_batches);
+                       uint64_t* range_vectors, int* split_batches, int* stages);
 
 /* ---- measurement (no counterpart in the reference, which times with
  *      std::chrono around whole calls: tools/gpu-bench.cpp:155-190) ---------- */

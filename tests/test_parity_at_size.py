@@ -130,3 +130,67 @@ def test_multi_block_ranges(oracle, case):
         assert np.array_equal(res.ids, wi), (nq, k)
         assert bits_equal(res.scores, ws), (nq, k)
     idx.close()
+
+
+# One and two queries per CTA stream the codes through shared-memory slots:
+# split by 256-group batch (1536-d 4-bit: 3 batches; 768-d 3-bit: 2) or whole
+# rows with a resident LUT (128-d).
+STAGED = [
+    ("pl", 1536, 200_000, 4, True),
+    ("pl", 768, 200_000, 3, True),
+    ("mix", 128, 300_000, 4, True),
+]
+
+
+@pytest.mark.parametrize("case", STAGED, ids=lambda c: f"{c[0]}{c[1]}_n{c[2]}_b{c[3]}")
+def test_staged_one_and_two_queries(oracle, case):
+    gen, dim, n, bits, tq = case
+    db, q_all = data(gen, dim, n)
+    calib = db[:10_000] if tq else None
+    idx = build(db, bits, calib)
+    packed, alpha, shift, scale = check_codes(oracle, idx, db, bits, calib)
+    for nq in (1, 2):
+        for k in (10, 32):
+            plan = idx.scan_plan(nq, k)
+            assert plan["stages"] > 0 and plan["q_per_cta"] == nq, plan
+            assert (plan["split_batches"] > 1) == (dim > 256), plan
+            q = q_all[:nq]
+            res = idx.search(q, k)
+            ws, wi = oracle.search_flat(q, bits, packed, alpha, k, shift, scale)
+            assert np.array_equal(res.ids, wi), (nq, k)
+            assert bits_equal(res.scores, ws), (nq, k)
+    idx.close()
+
+
+def test_staged_streamed_lut_matches_dense_scores():
+    """1.3M x 1024 4-bit: too many blocks for the batch split and a LUT larger
+    than the slots leave room for, so one and two queries scan whole rows with
+    the LUT streamed in 256-group chunks. The top-10 must equal the top-10 of
+    every vector's score from the dense-scores kernel (checked against the
+    oracle in the other tests), ties by lower id."""
+    torch = pytest.importorskip("torch")
+    from vectorcache_b200.synthetic import power_law_torch
+
+    n, dim = 1_300_000, 1024
+    dev = torch.device("cuda", 0)
+    idx = vcb.TurboQuantIndex(dim, 4)
+    for s in range(0, n, 650_000):
+        x = power_law_torch(650_000, dim, seed=40 + s // 650_000, device=dev)
+        if s == 0:
+            idx.calibrate_device(x[:10_000])
+        idx.add_device(x)
+        del x
+    idx.prepare()
+    torch.cuda.empty_cache()
+    q = power_law(2, dim, seed=41)
+    ids = np.arange(n)
+    for nq in (1, 2):
+        plan = idx.scan_plan(nq, 10)
+        assert plan["stages"] > 0 and plan["split_batches"] == 1 and plan["q_per_cta"] == nq, plan
+        res = idx.search(q[:nq], 10)
+        _, scores = idx.dense_scores(q[:nq])
+        for i in range(nq):
+            top = np.lexsort((ids, -scores[i]))[:10]
+            assert np.array_equal(res.ids[i], top), (nq, i)
+            assert bits_equal(res.scores[i], scores[i][top]), (nq, i)
+    idx.close()

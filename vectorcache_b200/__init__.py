@@ -97,7 +97,7 @@ def _declare(lib):
         "tq_index_dense_scores": (C.c_int, [_P, _P, _SZ, _P, _P]),
         "tq_index_replay_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
         "tq_index_scan_plan": (C.c_int, [_P, _SZ, _SZ, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                         C.POINTER(C.c_uint64), C.POINTER(C.c_int)]),
+                                         C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "tq_index_save": (C.c_int, [_P, C.c_char_p]),
         "tq_index_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
         "tq_index_add_npy": (C.c_int, [_P, C.c_char_p]),
@@ -418,10 +418,12 @@ class TurboQuantIndex:
 
     def scan_plan(self, nq: int, k: int) -> dict:
         """The scan tiling a search of nq queries with this k uses."""
-        q, r, s = C.c_int(), C.c_int(), C.c_int()
+        q, r, s, st = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         rv = C.c_uint64()
-        _check(self._lib.tq_index_scan_plan(self._h, nq, k, C.byref(q), C.byref(r), C.byref(rv), C.byref(s)))
-        return {"q_per_cta": q.value, "n_ranges": r.value, "range_vectors": rv.value, "split_batches": s.value}
+        _check(self._lib.tq_index_scan_plan(self._h, nq, k, C.byref(q), C.byref(r), C.byref(rv), C.byref(s),
+                                            C.byref(st)))
+        return {"q_per_cta": q.value, "n_ranges": r.value, "range_vectors": rv.value, "split_batches": s.value,
+                "stages": st.value}
 
 
 def _dev(t, n: int | None = None):

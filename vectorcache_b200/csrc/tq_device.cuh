@@ -17,6 +17,21 @@ constexpr double kDegenerateInner = 1e-12;  // constants.hpp kDegenerateInnerEps
 
 __device__ __forceinline__ unsigned full_mask() { return 0xffffffffu; }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, L1 bypassed): the
+// bytes in flight occupy shared memory, not registers. A thread's copies are
+// complete after cp_async_wait<N> (at most N of its commit groups pending);
+// other threads see them after a barrier (__syncwarp / __syncthreads).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { cp_async_wait<0>(); }
+
 // Sum of squares with 8 interleaved chains (chain j % 8, in index order, one
 // fused multiply-add per step) combined as ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7))
 // (encode.cpp:16-26). Lane l of the warp owns chain l % 8 of row l / 8, so one

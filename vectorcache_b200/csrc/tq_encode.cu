@@ -331,13 +331,6 @@ __global__ void __launch_bounds__(256) order_stats_kernel(const float* __restric
 // stored in the same (register, lane) order, so every table read is one
 // conflict-free shared-memory access.
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // Index of the row element held by (lane, register r).
 template <int E>
 __device__ __forceinline__ int pipe_elem(int r, int lane) {

@@ -453,7 +453,7 @@ int tq_index_replay_count(const tq_index* h, uint64_t* count) {
 }
 
 int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, int* n_ranges,
-                       uint64_t* range_vectors, int* split_batches) {
+                       uint64_t* range_vectors, int* split_batches, int* stages) {
   return vcb::guarded([&] {
     require(h != nullptr, TQ_ERR_INVALID_ARGUMENT, "null index");
     require(h->prepared, TQ_ERR_STATE, "scan plan before prepare");
@@ -470,6 +470,7 @@ int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, i
     if (n_ranges) *n_ranges = plan.n_ranges;
     if (range_vectors) *range_vectors = static_cast<uint64_t>(plan.range_vectors);
     if (split_batches) *split_batches = std::max(1, plan.split_batches);
+    if (stages) *stages = plan.stages;
   });
 }
 

@@ -160,6 +160,9 @@ struct ScanPlan {
   // queries over few blocks (whole blocks per CTA would leave the last wave
   // of CTAs part-full); it needs ScanArgs::partial.
   int split_batches = 0;
+  // > 0: the code stream goes through this many shared-memory slots per warp
+  // (one or two queries per CTA, register top-k).
+  int stages = 0;
 };
 // max_range_vectors > 0 bounds the vectors one CTA scans (shorter CTAs let
 // higher-priority work on other streams start sooner).

@@ -139,6 +139,22 @@ struct RegTopK {
   }
 };
 
+// Staged code stream: group rows per slot, and slots per warp by queries per
+// CTA (shared memory: 8 warps x slots x 8 rows x 256 bytes = 96 KB at one
+// query, 80 KB at two, beside the LUTs, two CTAs per SM).
+constexpr int kStageGroups = 8;
+constexpr int stages_for(int q) { return q == 1 ? 6 : 5; }
+// Byte offset of the slots: after the LUT area, which the register top-k's
+// end-of-range merge also uses (Q x 8 warps x 32 lanes x 8 bytes).
+__host__ __device__ constexpr size_t scan_stage_offset(int q, int chunk) {
+  return static_cast<size_t>(q) * chunk * 32 > static_cast<size_t>(q) * kScanWarps * 32 * 8
+             ? static_cast<size_t>(q) * chunk * 32
+             : static_cast<size_t>(q) * kScanWarps * 32 * 8;
+}
+constexpr size_t scan_stage_bytes(int q) {
+  return static_cast<size_t>(kScanWarps) * stages_for(q) * kStageGroups * 256;
+}
+
 // PF: byte groups of codes in flight per thread. Few queries per CTA leave
 // the kernel memory-bound, where a deeper ring keeps more bytes in flight.
 // MODE 0 scans every byte group and keeps the top k. For one or two queries
@@ -148,15 +164,29 @@ struct RegTopK {
 // arithmetic as MODE 0) and keeps the top k, without lookups. MODE 3 is MODE 1
 // followed, in the CTA that stores a block's last batch (a counter per block,
 // threadfence-reduction style, no waiting), by MODE 2 for that block.
-template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0>
+//
+// STAGES > 0 (one or two queries, k <= 32, nbg a multiple of PF): the code
+// stream reaches the lookups through shared memory instead of a register
+// ring. Each warp owns STAGES slots of PF group rows (its 256-byte half of a
+// tile row each), filled by 16-byte cp.async copies STAGES - 1 slots ahead of
+// the lookups; the bytes in flight no longer cost registers, so a memory-bound
+// scan keeps more of them in flight (a wait_group and a __syncwarp per slot,
+// no spin loop).
+template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0, int STAGES = 0>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
   static_assert(PF % 2 == 0, "byte groups are consumed in pairs");
+  static_assert(STAGES == 0 || (STAGES >= 2 && KMAX <= kRegTopK && MODE != 1 && MODE != 2),
+                "staged code stream: register top-k, scanning modes");
   constexpr bool kReg = KMAX <= kRegTopK;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nbg = a.nbg;
   const int chunk = a.lut_chunk_groups;
   LutHalf* s_lut = reinterpret_cast<LutHalf*>(smem);  // [Q][chunk][2]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  [[maybe_unused]] uint2* s_stage = nullptr;  // this warp's STAGES x PF rows of 32 uint2
+  if constexpr (STAGES > 0) {
+    s_stage = reinterpret_cast<uint2*>(smem + scan_stage_offset(Q, chunk)) + warp * (STAGES * PF * 32);
+  }
 
   // Selector helpers. (Measured at 1M x 1536 one query: moving the shifts to
   // the FMA-heavy pipe as mul.hi, 0.187 -> 0.191 ms, or the byte-sum additions
@@ -249,6 +279,29 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
       }
     }
 
+    // Staged stream: slot st holds group rows g_first + st * PF .. + PF - 1.
+    [[maybe_unused]] int st = 0;
+    [[maybe_unused]] const int n_st = (g_last - g_first) / PF;
+    [[maybe_unused]] auto issue = [&](int s_idx) {
+      if constexpr (STAGES > 0) {
+        if (s_idx < n_st) {
+          const uint2* src = (wp - lane) + static_cast<long long>(g_first + s_idx * PF) * kGroupStride;
+          uint2* dst = s_stage + (s_idx % STAGES) * (PF * 32);
+#pragma unroll
+          for (int i = 0; i < PF / 2; ++i) {
+            const int c = lane + 32 * i;  // 16-byte chunk c: row c / 16, bytes 16 * (c % 16)
+            cp_async16(dst + (c >> 4) * 32 + (c & 15) * 2, src + (c >> 4) * kGroupStride + (c & 15) * 2);
+          }
+        }
+        cp_async_commit();  // empty groups past the end keep the wait counts uniform
+      }
+    };
+    if constexpr (STAGES > 0) {
+      __syncwarp();  // every lane is done reading the previous block's slots
+#pragma unroll
+      for (int s0 = 0; s0 < STAGES - 1; ++s0) issue(s0);
+    }
+
     for (int gb = g_first; gb < g_last; gb += kFlushGroups) {
       const int g_stop = min(gb + kFlushGroups, nbg);
       if (!resident && gb % chunk == 0) {
@@ -258,10 +311,11 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
       }
       const int chunk_base = kBatch ? g_first : (resident ? 0 : (gb / chunk) * chunk);
       // The lookups of PF code groups held in `cur`, starting at group g
-      // (CHECKED: only those below g_stop). Byte groups in pairs (nbg and every 256-group
-      // batch are even): the second-half lookups of both groups add into one
-      // byte per vector (<= 2 * 127), the first-half lookups into another; one
-      // prmt interleaves the two bytes of each vector so a single dp4a adds both.
+      // (CHECKED: only those below g_stop). Byte groups in pairs (nbg and
+      // every 256-group batch are even): the second-half lookups of both
+      // groups add into one byte per vector (<= 2 * 127), the first-half
+      // lookups into another; one prmt interleaves the two bytes of each
+      // vector so a single dp4a adds both.
       auto process = [&](const uint2 (&cur)[PF], int g, auto checked) {
 #pragma unroll
         for (int u = 0; u < PF; u += 2) {
@@ -319,43 +373,56 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           }
         }
       };
-      uint2 ring[PF];
-      // One or two queries: whole rings (every 256-group batch of a 4- or
-      // 3-bit row of 512+ dims) run without bounds checks, loading at
-      // immediate offsets of a running pointer. Four queries keep the checked
-      // loop: the second copy of the lookup body does not fit their 128
-      // registers.
-      if (Q <= 2 && (g_stop - gb) % PF == 0) {
-        const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
-#pragma unroll
-        for (int u = 0; u < PF; ++u) ring[u] = src[u * kGroupStride];
-        src += PF * kGroupStride;
-        int g = gb;
-        for (; g + PF < g_stop; g += PF) {
+      if constexpr (STAGES > 0) {
+        for (int g = gb; g < g_stop; g += PF, ++st) {
+          cp_async_wait<STAGES - 2>();  // slot st has landed (this lane's copies)
+          __syncwarp();                 // ... and every lane's; slot st - 1 is free
+          issue(st + STAGES - 1);
+          const uint2* slot = s_stage + (st % STAGES) * (PF * 32) + lane;
           uint2 cur[PF];
 #pragma unroll
-          for (int u = 0; u < PF; ++u) {
-            cur[u] = ring[u];
-            ring[u] = src[u * kGroupStride];
-          }
-          src += PF * kGroupStride;
+          for (int u = 0; u < PF; ++u) cur[u] = slot[u * 32];
           process(cur, g, std::false_type{});
         }
-        process(ring, g, std::false_type{});
       } else {
+        uint2 ring[PF];
+        // One or two queries: whole rings (every 256-group batch of a 4- or
+        // 3-bit row of 512+ dims) run without bounds checks, loading at
+        // immediate offsets of a running pointer. Four queries keep the checked
+        // loop: the second copy of the lookup body does not fit their 128
+        // registers.
+        if (Q <= 2 && (g_stop - gb) % PF == 0) {
+          const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
 #pragma unroll
-        for (int u = 0; u < PF; ++u) {
-          ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
-        }
-        for (int g = gb; g < g_stop; g += PF) {
-          uint2 cur[PF];
+          for (int u = 0; u < PF; ++u) ring[u] = src[u * kGroupStride];
+          src += PF * kGroupStride;
+          int g = gb;
+          for (; g + PF < g_stop; g += PF) {
+            uint2 cur[PF];
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+              cur[u] = ring[u];
+              ring[u] = src[u * kGroupStride];
+            }
+            src += PF * kGroupStride;
+            process(cur, g, std::false_type{});
+          }
+          process(ring, g, std::false_type{});
+        } else {
 #pragma unroll
           for (int u = 0; u < PF; ++u) {
-            cur[u] = ring[u];
-            const int gn = g + PF + u;
-            ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+            ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
           }
-          process(cur, g, std::true_type{});
+          for (int g = gb; g < g_stop; g += PF) {
+            uint2 cur[PF];
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+              cur[u] = ring[u];
+              const int gn = g + PF + u;
+              ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+            }
+            process(cur, g, std::true_type{});
+          }
         }
       }
       // f32 flush of this batch (search_avx2.cpp:24-48).
@@ -736,14 +803,14 @@ __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const fl
   if (out_score) out_score[idx] = __fadd_rn(__fmul_rn(fa, alpha[v]), 0.f);
 }
 
-template <int Q, int KMAX, int MINB, bool N8, int PF>
+template <int Q, int KMAX, int MINB, bool N8, int PF, int STAGES = 0>
 cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, KMAX, MINB, N8, PF>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(plan.smem_bytes));
+  auto kern = scan_kernel<Q, KMAX, MINB, N8, PF, 0, STAGES>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(plan.smem_bytes));
   if (e != cudaSuccess) return e;
   dim3 grid(static_cast<unsigned>((a.nq + Q - 1) / Q), static_cast<unsigned>(plan.n_ranges));
-  scan_kernel<Q, KMAX, MINB, N8, PF><<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
+  kern<<<grid, kScanWarps * 32, plan.smem_bytes, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -764,6 +831,17 @@ cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t
   s.lut_chunk_groups = kFlushGroups;
   s.partial_batches = plan.split_batches;
   const size_t smem1 = static_cast<size_t>(Q) * kFlushGroups * 32;
+  if (a.arrive && plan.n_ranges == blocks && plan.stages > 0) {
+    // As below, with the code stream staged through shared memory.
+    constexpr int kSt = stages_for(Q);
+    const size_t smem3 = scan_stage_offset(Q, kFlushGroups) + scan_stage_bytes(Q);
+    auto kern = scan_kernel<Q, kRegTopK, 2, N8, kStageGroups, 3, kSt>;
+    cudaError_t e3 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem3));
+    if (e3 != cudaSuccess) return e3;
+    kern<<<dim3(qgroups, static_cast<unsigned>(blocks), static_cast<unsigned>(plan.split_batches)), kScanWarps * 32,
+           smem3, stream>>>(s);
+    return cudaGetLastError();
+  }
   if (a.arrive && plan.n_ranges == blocks) {
     // One launch: the CTA completing a block flushes it (its lists are the
     // plan's ranges, one block each). The LUT area also holds the merge.
@@ -815,8 +893,16 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
     q >>= 1;
   }
   const size_t warp_total = kScanWarps * scan_warp_bytes(q, kmax);
+  // One or two queries with the register top-k stream the codes through
+  // shared-memory slots (nbg a multiple of the slot rows); the slots share
+  // the CTA's budget with the LUTs.
+  const bool staged = reg && q <= 2 && nbg % kStageGroups == 0;
+  const size_t stage_total = staged ? scan_stage_bytes(q) : 0;
+  auto lut_area = [&](int c) {
+    return staged ? scan_stage_offset(q, c) : static_cast<size_t>(q) * c * 32 + warp_total;
+  };
   int chunk = nbg;
-  while (static_cast<size_t>(q) * chunk * 32 + warp_total > budget) {
+  while (lut_area(chunk) + stage_total > budget) {
     if (chunk > kFlushGroups) {
       chunk = ((chunk - 1) / kFlushGroups) * kFlushGroups;
       if (chunk < kFlushGroups) chunk = kFlushGroups;
@@ -863,6 +949,8 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
     // the end-of-range merge of the 8 warp lists reuses the LUT area
     plan->smem_bytes = std::max(plan->smem_bytes, static_cast<size_t>(q) * kScanWarps * kWarp * 8);
   }
+  plan->stages = staged ? stages_for(q) : 0;
+  if (staged) plan->smem_bytes = scan_stage_offset(q, chunk) + stage_total;
   plan->lists_per_range = reg ? 1 : kScanWarps;
   // One or two queries over at most two waves of blocks: whole blocks per CTA
   // leave the last wave part-full (1M vectors = 489 blocks over 296 resident
@@ -882,6 +970,14 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
     if (a.partial_stride < span || a.partial_batches != plan.split_batches) return cudaErrorInvalidValue;
     if (q == 1) return n8 ? launch_split_t<1, true>(a, plan, stream) : launch_split_t<1, false>(a, plan, stream);
     return n8 ? launch_split_t<2, true>(a, plan, stream) : launch_split_t<2, false>(a, plan, stream);
+  }
+  if (plan.stages > 0 && km == kRegTopK && q <= 2) {
+    if (q == 1) {
+      return n8 ? launch_scan_t<1, kRegTopK, 2, true, kStageGroups, stages_for(1)>(a, plan, stream)
+                : launch_scan_t<1, kRegTopK, 2, false, kStageGroups, stages_for(1)>(a, plan, stream);
+    }
+    return n8 ? launch_scan_t<2, kRegTopK, 2, true, kStageGroups, stages_for(2)>(a, plan, stream)
+              : launch_scan_t<2, kRegTopK, 2, false, kStageGroups, stages_for(2)>(a, plan, stream);
   }
 #define VCB_SCAN(QQ, KK, MB)                                                             \
   if (q == QQ && km == KK) {                                                             \
