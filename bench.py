@@ -858,8 +858,9 @@ def run_bucketed(args, world, rank, local):
         idx.route_device(d_q, 256, te_s, te_i, stream=stream)
         mlp.predict_device(te_s, nq, 256, npq, coverage=rule, min_confidence=0.0, fallback=p_max, stream=stream)
         mean_probe = float(npq.float().mean().item())
+        counts = np.bincount(np.searchsorted(classes, npq.cpu().numpy()), minlength=len(classes))
         cand = {"rule": rule, "ms_per_step": ms, "qps": nq / (ms / 1e3), "recall_at_10": r,
-                "mean_n_probe": mean_probe}
+                "mean_n_probe": mean_probe, "n_probe_histogram": counts.tolist()}
         learned_sweep.append(cand)
         if r >= target and (best is None or cand["qps"] > best["qps"]):
             best = cand

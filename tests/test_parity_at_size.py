@@ -132,18 +132,18 @@ def test_multi_block_ranges(oracle, case):
     idx.close()
 
 
-# One and two queries per CTA stream the codes through shared-memory slots:
-# split by 256-group batch (1536-d 4-bit: 3 batches; 768-d 3-bit: 2) or whole
-# rows with a resident LUT (128-d).
-STAGED = [
+# One and two queries per CTA: split by 256-group batch over few blocks
+# (1536-d 4-bit: 3 batches; 768-d 3-bit: 2; register prefetch ring), or whole
+# rows with the codes streamed through shared-memory slots (128-d).
+ONE_TWO = [
     ("pl", 1536, 200_000, 4, True),
     ("pl", 768, 200_000, 3, True),
     ("mix", 128, 300_000, 4, True),
 ]
 
 
-@pytest.mark.parametrize("case", STAGED, ids=lambda c: f"{c[0]}{c[1]}_n{c[2]}_b{c[3]}")
-def test_staged_one_and_two_queries(oracle, case):
+@pytest.mark.parametrize("case", ONE_TWO, ids=lambda c: f"{c[0]}{c[1]}_n{c[2]}_b{c[3]}")
+def test_one_and_two_queries(oracle, case):
     gen, dim, n, bits, tq = case
     db, q_all = data(gen, dim, n)
     calib = db[:10_000] if tq else None
@@ -152,8 +152,8 @@ def test_staged_one_and_two_queries(oracle, case):
     for nq in (1, 2):
         for k in (10, 32):
             plan = idx.scan_plan(nq, k)
-            assert plan["stages"] > 0 and plan["q_per_cta"] == nq, plan
-            assert (plan["split_batches"] > 1) == (dim > 256), plan
+            split = plan["split_batches"] > 1
+            assert plan["q_per_cta"] == nq and split == (dim > 256) and (plan["stages"] > 0) == (not split), plan
             q = q_all[:nq]
             res = idx.search(q, k)
             ws, wi = oracle.search_flat(q, bits, packed, alpha, k, shift, scale)
@@ -162,20 +162,26 @@ def test_staged_one_and_two_queries(oracle, case):
     idx.close()
 
 
-def test_staged_streamed_lut_matches_dense_scores():
-    """1.3M x 1024 4-bit: too many blocks for the batch split and a LUT larger
-    than the slots leave room for, so one and two queries scan whole rows with
-    the LUT streamed in 256-group chunks. The top-10 must equal the top-10 of
-    every vector's score from the dense-scores kernel (checked against the
-    oracle in the other tests), ties by lower id."""
+# Whole-row staged scans too large for the oracle: top-10 against every
+# vector's score from the dense-scores kernel (itself checked against the
+# oracle above and in test_gpu_parity), ties by lower id.
+#   1.3M x 1024 4-bit: the LUT is streamed in 256-group chunks beside the slots;
+#   1.3M x 768 3-bit: resident LUT, 3-bit lookups;
+#   10M x 128 4-bit: several blocks per CTA (the slots carry over blocks).
+STAGED_LARGE = [(1_300_000, 1024, 4), (1_300_000, 768, 3), (10_000_000, 128, 4)]
+
+
+@pytest.mark.parametrize("case", STAGED_LARGE, ids=lambda c: f"n{c[0]}_d{c[1]}_b{c[2]}")
+def test_staged_whole_rows_match_dense_scores(case):
     torch = pytest.importorskip("torch")
     from vectorcache_b200.synthetic import power_law_torch
 
-    n, dim = 1_300_000, 1024
+    n, dim, bits = case
     dev = torch.device("cuda", 0)
-    idx = vcb.TurboQuantIndex(dim, 4)
-    for s in range(0, n, 650_000):
-        x = power_law_torch(650_000, dim, seed=40 + s // 650_000, device=dev)
+    idx = vcb.TurboQuantIndex(dim, bits)
+    part = 1_300_000 if n <= 1_300_000 else 2_000_000
+    for s in range(0, n, part):
+        x = power_law_torch(min(part, n - s), dim, seed=40 + s // part, device=dev)
         if s == 0:
             idx.calibrate_device(x[:10_000])
         idx.add_device(x)
@@ -187,6 +193,8 @@ def test_staged_streamed_lut_matches_dense_scores():
     for nq in (1, 2):
         plan = idx.scan_plan(nq, 10)
         assert plan["stages"] > 0 and plan["split_batches"] == 1 and plan["q_per_cta"] == nq, plan
+        if n > 5_000_000:
+            assert plan["range_vectors"] >= 2 * BLOCK, plan
         res = idx.search(q[:nq], 10)
         _, scores = idx.dense_scores(q[:nq])
         for i in range(nq):

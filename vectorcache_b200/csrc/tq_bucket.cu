@@ -1668,18 +1668,84 @@ cudaError_t launch_build_pairs(const PairArgs& a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-__global__ void probe_floor_kernel(const float* __restrict__ top_s, const uint64_t* __restrict__ top_i,
-                                   long long nq, int k, uint64_t pad, float* __restrict__ floor) {
-  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (q >= nq) return;
-  const long long last = q * k + (k - 1);
-  floor[q] = top_i[last] != pad ? top_s[last] : -INFINITY;
+// floor[q] = the k-th largest admitted score (above -inf, not NaN) among the
+// first count[q] entries of query q's candidate region, -inf when it has fewer
+// than k: the k-th score of the merged top k of those candidates (ties do not
+// change that value), found without sorting by a radix select over
+// order-preserving 32-bit keys, 8 bits per pass, one CTA of 256 threads per
+// query. The region is L2-resident (just written by the scan); each pass
+// re-reads it.
+__global__ void __launch_bounds__(256) kth_floor_kernel(const float* __restrict__ cand, long long stride,
+                                                        const uint32_t* __restrict__ count, int k,
+                                                        float* __restrict__ floor) {
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_digit, s_need, s_total;
+  const long long q = blockIdx.x;
+  const long long n = count[q];
+  const float* cs = cand + q * stride;
+  uint32_t prefix = 0, mask = 0, need = static_cast<uint32_t>(k);
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    hist[threadIdx.x] = 0u;
+    __syncthreads();
+    for (long long i = threadIdx.x; i < n; i += 256) {
+      const float v = cs[i];
+      if (v > -INFINITY) {
+        const uint32_t u = __float_as_uint(v);
+        const uint32_t key = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+        if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < kWarp) {
+      // lane l holds digits 255 - 8l down to 248 - 8l; counts from the top
+      const int lane = threadIdx.x;
+      uint32_t c[8], sum = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        c[j] = hist[255 - 8 * lane - j];
+        sum += c[j];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < kWarp; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(full_mask(), incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t excl = incl - sum;
+      if (shift == 24 && lane == kWarp - 1) s_total = incl;
+      if (excl < need && need <= incl) {
+        uint32_t above = excl;
+        int d = 255 - 8 * lane;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (above + c[j] >= need) {
+            d = 255 - 8 * lane - j;
+            break;
+          }
+          above += c[j];
+        }
+        s_digit = static_cast<uint32_t>(d);
+        s_need = need - above;
+      }
+    }
+    __syncthreads();
+    if (s_total < static_cast<uint32_t>(k)) {  // fewer than k admitted candidates
+      if (threadIdx.x == 0) floor[q] = -INFINITY;
+      return;
+    }
+    prefix |= s_digit << shift;
+    mask |= 255u << shift;
+    need = s_need;
+    __syncthreads();  // everyone has read s_digit / s_need before the next pass
+  }
+  if (threadIdx.x == 0) floor[q] = __uint_as_float((prefix & 0x80000000u) ? (prefix & 0x7fffffffu) : ~prefix);
 }
 
-cudaError_t launch_probe_floor(const float* top_s, const uint64_t* top_i, long long nq, int k, uint64_t pad,
-                               float* floor, cudaStream_t stream) {
+cudaError_t launch_kth_floor(const float* cand, long long stride, const uint32_t* count, long long nq, int k,
+                             float* floor, cudaStream_t stream) {
   if (nq <= 0) return cudaSuccess;
-  probe_floor_kernel<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, stream>>>(top_s, top_i, nq, k, pad, floor);
+  if (k < 1) return cudaErrorInvalidValue;
+  kth_floor_kernel<<<static_cast<unsigned>(nq), 256, 0, stream>>>(cand, stride, count, k, floor);
   return cudaGetLastError();
 }
 

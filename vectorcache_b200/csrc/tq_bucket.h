@@ -182,11 +182,12 @@ struct BucketScanArgs {
 };
 // `grid`: a bound of the item count; the launch runs min(grid, resident CTAs).
 cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStream_t stream);
-// floor[q] = the k-th score of the merged top k of the first probes (a lower
-// bound of the k-th best over all probes), -inf when that top k is not full
-// (its k-th id is `pad`).
-cudaError_t launch_probe_floor(const float* top_s, const uint64_t* top_i, long long nq, int k, uint64_t pad,
-                               float* floor, cudaStream_t stream);
+// floor[q] = the k-th largest score (above -inf) among the first count[q]
+// candidates of query q's region (cand + q * stride), -inf when there are
+// fewer than k: the k-th score of their merged top k, a lower bound of the
+// k-th best over all probes.
+cudaError_t launch_kth_floor(const float* cand, long long stride, const uint32_t* count, long long nq, int k,
+                             float* floor, cudaStream_t stream);
 
 // ---- multi-index persistent scan (tq_multi.cu) -----------------------------
 // One flat index of a multi-index launch: its scan layout, its queries' LUTs

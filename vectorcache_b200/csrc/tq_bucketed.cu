@@ -45,12 +45,12 @@ namespace vcb {
 // lists, re-rank) plus the flat engine's query scratch.
 struct BucketScratch {
   DeviceBuffer qh, route, top_s, top_i, counts, fill, pstart, istart, pairs, off, items, nitems, cand_s,
-      cand_i, rr_s, rr_i, np, floor, fl_s, fl_i, acount, encs;
+      cand_i, rr_s, rr_i, np, floor, acount, encs;
   FlatScratchStore flat;
   ProbeScratch probe;
   void bind(ScratchArena* a) {
     for (DeviceBuffer* b : {&qh, &route, &top_s, &top_i, &counts, &fill, &pstart, &istart, &pairs, &off, &items,
-                            &nitems, &cand_s, &cand_i, &rr_s, &rr_i, &np, &floor, &fl_s, &fl_i, &acount, &encs}) {
+                            &nitems, &cand_s, &cand_i, &rr_s, &rr_i, &np, &floor, &acount, &encs}) {
       b->bind(a);
     }
     flat.bind(a);
@@ -522,20 +522,8 @@ struct tq_bucketed {
           std::min(max_probe >= pa.wide_from ? vcb::kFloorProbesWide : vcb::kFloorProbes, max_probe);
       const bool two_phase = max_probe > vcb::kFloorProbes;
       if (two_phase) {
-        sc.fl_s.reserve(m * kscan * 4);
-        sc.fl_i.reserve(m * kscan * 8);
-        vcb::MergeArgs fm{};
-        fm.cand_score = ba.cand_score;
-        fm.cand_id = ba.cand_id;
-        fm.nq = static_cast<long long>(m);
-        fm.n_lists = first * vcb::kBsListsPerProbe;
-        fm.list_stride = max_probe * vcb::kBsListsPerProbe;
-        fm.k = static_cast<int>(kscan);
-        fm.k_out = static_cast<int>(kscan);
-        fm.out_score = sc.fl_s.as<float>();
-        fm.out_id = sc.fl_i.as<uint64_t>();
-        fm.entry_count = ba.append_count;
-        fm.pad_id = ~0ull;
+        // a query's candidate region: max_probe lists of kscan entries
+        const long long region = static_cast<long long>(max_probe) * vcb::kBsListsPerProbe * kscan;
         // Probe 0 alone, then probes 1..first-1 above probe 0's floor (the
         // first probes cost most without a floor), then the floor of all
         // first probes for the rest. Each floor is the k-th best of the
@@ -551,6 +539,11 @@ struct tq_bucketed {
           steps[2] = vcb::kFloorProbes;
           steps[3] = first;
           n_steps = 3;
+          // The steps are fixed now, so every query with more than 32 probes
+          // (per-query counts below the wide threshold included) takes 32
+          // first probes: its far probes then scan above the k-th best of 32
+          // probes instead of 8, at no extra launch.
+          pa.wide_from = vcb::kFloorProbesWide + 1;
         }
         for (int st = 0; st < n_steps; ++st) {
           pa.probe_begin = steps[st];
@@ -563,11 +556,9 @@ struct tq_bucketed {
                       [&] { return vcb::launch_build_pairs(pa, s); });
           eng->launch(tq_index::kScan, s, "bucket scan kernel (first probes)",
                       [&] { return vcb::launch_bucket_scan(ba, std::min(items, step_items), s); });
-          eng->launch(tq_index::kPrep, s, "floor kernels", [&] {
-            cudaError_t e = vcb::launch_merge(fm, s);
-            if (e != cudaSuccess) return e;
-            return vcb::launch_probe_floor(fm.out_score, fm.out_id, static_cast<long long>(m),
-                                           static_cast<int>(kscan), ~0ull, sc.floor.as<float>(), s);
+          eng->launch(tq_index::kPrep, s, "floor kernel", [&] {
+            return vcb::launch_kth_floor(ba.cand_score, region, ba.append_count, static_cast<long long>(m),
+                                         static_cast<int>(kscan), sc.floor.as<float>(), s);
           });
           ba.floor = sc.floor.as<float>();
         }

@@ -165,9 +165,9 @@ constexpr size_t scan_stage_bytes(int q) {
 // followed, in the CTA that stores a block's last batch (a counter per block,
 // threadfence-reduction style, no waiting), by MODE 2 for that block.
 //
-// STAGES > 0 (one or two queries, k <= 32, nbg a multiple of PF): the code
-// stream reaches the lookups through shared memory instead of a register
-// ring. Each warp owns STAGES slots of PF group rows (its 256-byte half of a
+// STAGES > 0 (whole-row scans of one or two queries, k <= 32, nbg a multiple
+// of PF): the code stream reaches the lookups through shared memory instead of
+// a register ring. Each warp owns STAGES slots of PF group rows (its 256-byte half of a
 // tile row each), filled by 16-byte cp.async copies STAGES - 1 slots ahead of
 // the lookups; the bytes in flight no longer cost registers, so a memory-bound
 // scan keeps more of them in flight (a wait_group and a __syncwarp per slot,
@@ -175,8 +175,8 @@ constexpr size_t scan_stage_bytes(int q) {
 template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0, int STAGES = 0>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
   static_assert(PF % 2 == 0, "byte groups are consumed in pairs");
-  static_assert(STAGES == 0 || (STAGES >= 2 && KMAX <= kRegTopK && MODE != 1 && MODE != 2),
-                "staged code stream: register top-k, scanning modes");
+  static_assert(STAGES == 0 || (STAGES >= 2 && KMAX <= kRegTopK && MODE == 0),
+                "staged code stream: register top-k, whole-row scans");
   constexpr bool kReg = KMAX <= kRegTopK;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nbg = a.nbg;
@@ -831,17 +831,6 @@ cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t
   s.lut_chunk_groups = kFlushGroups;
   s.partial_batches = plan.split_batches;
   const size_t smem1 = static_cast<size_t>(Q) * kFlushGroups * 32;
-  if (a.arrive && plan.n_ranges == blocks && plan.stages > 0) {
-    // As below, with the code stream staged through shared memory.
-    constexpr int kSt = stages_for(Q);
-    const size_t smem3 = scan_stage_offset(Q, kFlushGroups) + scan_stage_bytes(Q);
-    auto kern = scan_kernel<Q, kRegTopK, 2, N8, kStageGroups, 3, kSt>;
-    cudaError_t e3 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem3));
-    if (e3 != cudaSuccess) return e3;
-    kern<<<dim3(qgroups, static_cast<unsigned>(blocks), static_cast<unsigned>(plan.split_batches)), kScanWarps * 32,
-           smem3, stream>>>(s);
-    return cudaGetLastError();
-  }
   if (a.arrive && plan.n_ranges == blocks) {
     // One launch: the CTA completing a block flushes it (its lists are the
     // plan's ranges, one block each). The LUT area also holds the merge.
@@ -958,7 +947,15 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
   // 4-bit: 1M vectors scan 10 % faster split (one query 0.210 -> 0.191 ms);
   // at 2M (977 blocks) the split no longer pays for its extra CTA start-ups.
   const int n_batches = (nbg + kFlushGroups - 1) / kFlushGroups;
-  if (reg && q <= 2 && n_batches > 1 && blocks <= 2 * resident) plan->split_batches = n_batches;
+  if (reg && q <= 2 && n_batches > 1 && blocks <= 2 * resident) {
+    plan->split_batches = n_batches;
+    // A split CTA streams a single 256-group batch, too short to amortize
+    // filling the shared-memory slots: the split scans keep the register
+    // ring (1M x 1536 4-bit, one query: 0.173 ms with the ring, 0.185 staged;
+    // whole rows staged: 4M x 1536 0.659 -> 0.612 ms, 10M x 768 3-bit
+    // 0.633 -> 0.571 ms).
+    plan->stages = 0;
+  }
   return true;
 }
 
