@@ -71,7 +71,24 @@ def parse():
                         "(cumulative-probability rule)")
     p.add_argument("--bucketed-fixed-only", type=int, default=0,
                    help="bucketed: time the plain path at this n_probe only (no sweep, no learned probe)")
+    p.add_argument("--extra-classes", type=str, default="",
+                   help="learned n_probe: comma-separated candidate n_probe values added below the operating point")
+    p.add_argument("--learned-above", type=str, default=",".join(str(c) for c in LEARNED_ABOVE),
+                   help="learned n_probe: comma-separated candidate n_probe values above the operating point")
     return p.parse_args()
+
+
+def _int_list(text):
+    return tuple(int(v) for v in text.split(",") if v.strip())
+
+
+def learned_classes(args, p_op):
+    """Candidate n_probe values of the learned probe: the listed ones (and any
+    --extra-classes) below the fixed operating point, the operating point,
+    and the --learned-above values above it."""
+    below = sorted({c for c in PROBE_CLASSES + _int_list(args.extra_classes) if c < p_op})
+    above = sorted({c for c in _int_list(args.learned_above) if c > p_op})
+    return tuple(below) + (p_op,) + tuple(above)
 
 
 def load_peaks():
@@ -823,8 +840,7 @@ def run_bucketed(args, world, rank, local):
     # Candidate n_probe values: the listed ones below the operating point, the
     # operating point itself, and a few above it, so that the recall objective
     # can spend more buckets on hard queries than the fixed path does.
-    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,) + tuple(
-        c for c in LEARNED_ABOVE if c > p_op)
+    classes = learned_classes(args, p_op)
     p_max = classes[-1]
 
     # labels from the plain index (reference n_probe = the operating point) and GPU training
@@ -1003,8 +1019,7 @@ def run_serving(args, world, rank, local):
         if fixed_recall(p) >= RECALL_TARGET:
             p_op = p
             break
-    classes = tuple(c for c in PROBE_CLASSES if c < p_op) + (p_op,) + tuple(
-        c for c in LEARNED_ABOVE if c > p_op)
+    classes = learned_classes(args, p_op)
     p_max = classes[-1]
     labels, rec = probe_labels(lambda q, p: bkt.search(q, k, n_probe=p).ids, train_q, ex_train, classes, k, p_op)
     objective = args.probe_objective

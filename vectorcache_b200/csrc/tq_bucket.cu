@@ -317,15 +317,82 @@ __device__ __forceinline__ uint32_t select_key(float v) {
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
+// Bitonic sort of 256 * E 64-bit keys, largest first; thread t holds elements
+// t*E .. t*E+E-1. Strides below E exchange registers, strides below 32E (the
+// warp's elements) shuffle, only the longer ones go through `tmp` (256 * E
+// keys of shared memory) with two barriers each: 6 of the 55 stages at 1,024
+// keys instead of every stage.
+template <int E, int SIZE, int STRIDE>
+__device__ __forceinline__ void bitonic_stage(uint64_t (&k)[E], uint64_t* tmp) {
+  const int t = threadIdx.x;
+  if constexpr (STRIDE >= 32 * E) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) tmp[t * E + r] = k[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int e = t * E + r;
+      const uint64_t o = tmp[e ^ STRIDE];
+      const bool keep_max = ((e & STRIDE) == 0) == ((e & SIZE) == 0);
+      k[r] = keep_max ? (k[r] > o ? k[r] : o) : (k[r] < o ? k[r] : o);
+    }
+    __syncthreads();
+  } else if constexpr (STRIDE >= E) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int e = t * E + r;
+      const uint64_t o = __shfl_xor_sync(full_mask(), k[r], STRIDE / E);
+      const bool keep_max = ((e & STRIDE) == 0) == ((e & SIZE) == 0);
+      k[r] = keep_max ? (k[r] > o ? k[r] : o) : (k[r] < o ? k[r] : o);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      if ((r & STRIDE) == 0) {
+        const bool up = ((t * E + r) & SIZE) == 0;
+        const uint64_t a = k[r], b = k[r + STRIDE];
+        if (up ? a < b : a > b) {
+          k[r] = b;
+          k[r + STRIDE] = a;
+        }
+      }
+    }
+  }
+}
+
+// The stages of merge size SIZE from STRIDE down, then the larger sizes.
+template <int E, int SIZE, int STRIDE>
+__device__ __forceinline__ void bitonic_from(uint64_t (&k)[E], uint64_t* tmp) {
+  if constexpr (SIZE <= kRadixThreads * E) {
+    if constexpr (STRIDE == 0) {
+      bitonic_from<E, SIZE * 2, SIZE>(k, tmp);
+    } else {
+      bitonic_stage<E, SIZE, STRIDE>(k, tmp);
+      bitonic_from<E, SIZE, STRIDE / 2>(k, tmp);
+    }
+  }
+}
+
+// Bitonic sort of 256 * E 64-bit keys, largest first; thread t holds elements
+// t*E .. t*E+E-1. Strides below E exchange registers, strides below 32E (the
+// warp's elements) shuffle, only the longer ones go through `tmp` (256 * E
+// keys of shared memory) with two barriers each: 6 of the 55 stages at 1,024
+// keys instead of every stage.
+template <int E>
+__device__ __forceinline__ void cta_sort_keys(uint64_t (&k)[E], uint64_t* tmp) {
+  bitonic_from<E, 2, 1>(k, tmp);
+}
+
+// E = max(256, next power of two >= p) / 256 keys per thread in the final sort.
+template <int E>
 __global__ void __launch_bounds__(kRadixThreads) select_radix_kernel(const float* __restrict__ S, long long ld,
                                                                      int ncols, int p, float* __restrict__ out_s,
                                                                      uint32_t* __restrict__ out_i) {
   extern __shared__ __align__(16) unsigned char rad_smem[];
-  int p2 = 2;
-  while (p2 < p) p2 <<= 1;
-  float* bs = reinterpret_cast<float*>(rad_smem);
-  uint32_t* bi = reinterpret_cast<uint32_t*>(bs + p2);
-  uint32_t* keys = bi + p2;  // ncols
+  constexpr int N = kRadixThreads * E;
+  // selected (key << 32 | ~column): larger is better, ties to the lower column
+  uint64_t* ks = reinterpret_cast<uint64_t*>(rad_smem);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(ks + N);  // ncols
   __shared__ unsigned hist[256];
   __shared__ unsigned s_valid, s_eq, s_n, s_bin, s_above, s_warp[kRadixThreads / kWarp];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -407,8 +474,7 @@ __global__ void __launch_bounds__(kRadixThreads) select_radix_kernel(const float
     const uint32_t k = keys[c];
     if (k > T || (k == T && k != 0u && all_eq)) {
       const unsigned pos = atomicAdd(&s_n, 1u);
-      bs[pos] = sr[c];
-      bi[pos] = static_cast<uint32_t>(c);
+      ks[pos] = (static_cast<uint64_t>(k) << 32) | static_cast<uint32_t>(~c);
     }
   }
   if (!all_eq) {
@@ -426,24 +492,27 @@ __global__ void __launch_bounds__(kRadixThreads) select_radix_kernel(const float
       before += __popc(bal & ((1u << lane) - 1u));
       if (eq && before < rank) {
         const unsigned pos = atomicAdd(&s_n, 1u);
-        bs[pos] = sr[c];
-        bi[pos] = static_cast<uint32_t>(c);
+        ks[pos] = (static_cast<uint64_t>(T) << 32) | static_cast<uint32_t>(~c);
       }
       for (int w = 0; w < kRadixThreads / kWarp; ++w) base += s_warp[w];
     }
   }
   __syncthreads();
   const int n = static_cast<int>(s_n);
-  for (int t = n + threadIdx.x; t < p2; t += blockDim.x) {
-    bs[t] = -INFINITY;
-    bi[t] = 0xffffffffu;
-  }
+  for (int t = n + threadIdx.x; t < N; t += blockDim.x) ks[t] = 0ull;  // below every selected key
   __syncthreads();
-  cta_sort(bs, bi, p2);
-  for (int t = threadIdx.x; t < p; t += blockDim.x) {
-    const bool have = t < n;
-    out_s[row * p + t] = have ? bs[t] : -INFINITY;
-    out_i[row * p + t] = have ? bi[t] : 0xffffffffu;
+  uint64_t k8[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) k8[r] = ks[threadIdx.x * E + r];
+  cta_sort_keys<E>(k8, ks);
+#pragma unroll
+  for (int r = 0; r < E; ++r) {
+    const int t = threadIdx.x * E + r;
+    if (t >= p) break;
+    const bool have = k8[r] != 0ull;
+    const uint32_t c = ~static_cast<uint32_t>(k8[r]);
+    out_s[row * p + t] = have ? sr[c] : -INFINITY;
+    out_i[row * p + t] = have ? c : 0xffffffffu;
   }
 }
 
@@ -1532,13 +1601,17 @@ cudaError_t launch_select_top(const float* S, long long rows, long long ld, int 
   if (rows == 0) return cudaSuccess;
   if (p < 1 || p > kMaxProbe) return cudaErrorInvalidValue;
   if (ncols <= kRadixMaxCols) {
-    int p2 = 2;
-    while (p2 < p) p2 <<= 1;
-    const size_t rsmem = static_cast<size_t>(p2) * 8 + static_cast<size_t>(ncols) * 4;
-    cudaError_t e = cudaFuncSetAttribute(select_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(rsmem));
+    int n2 = kRadixThreads;
+    while (n2 < p) n2 <<= 1;
+    const size_t rsmem = static_cast<size_t>(n2) * 8 + static_cast<size_t>(ncols) * 4;
+    auto kern = n2 == kRadixThreads       ? select_radix_kernel<1>
+                : n2 == 2 * kRadixThreads ? select_radix_kernel<2>
+                : n2 == 4 * kRadixThreads ? select_radix_kernel<4>
+                                          : select_radix_kernel<8>;
+    static_assert(kMaxProbe <= 8 * kRadixThreads, "p fits the largest sort");
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(rsmem));
     if (e != cudaSuccess) return e;
-    select_radix_kernel<<<static_cast<unsigned>(rows), kRadixThreads, rsmem, stream>>>(S, ld, ncols, p, out_s, out_i);
+    kern<<<static_cast<unsigned>(rows), kRadixThreads, rsmem, stream>>>(S, ld, ncols, p, out_s, out_i);
     return cudaGetLastError();
   }
   const size_t smem = static_cast<size_t>(sel_cap(p)) * 8 + static_cast<size_t>(p) * 8;
