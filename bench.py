@@ -1084,8 +1084,11 @@ def run_serving(args, world, rank, local):
             total += nb_q
         row = {"rate_qps": rate, "queries": total, "requests": len(base)}
         for mode, target in (("fixed", t_fixed), ("learned", t_learn)):
+            # bucketed requests: the fixed n_probe, or the learned probe's own
+            # largest class (a request's n_probe caps the learned counts)
+            cap = p_op if mode == "fixed" else p_max
             trace = [(tt, t_flat if kind == "flat" else target, (flat_q if kind == "flat" else test_q)[rows], kk,
-                      0 if kind == "flat" else p_op) for tt, kind, rows, kk in base]
+                      0 if kind == "flat" else cap) for tt, kind, rows, kk in base]
             lat, wall, results = srv.replay(trace)
             lat_ms = lat / 1e3
             is_b = np.array([kind == "bkt" for _, kind, _, _ in base])

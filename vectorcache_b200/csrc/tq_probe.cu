@@ -33,6 +33,7 @@
 
 #include "../../include/vectorcache_b200.h"
 #include "tq_abi.h"
+#include "tq_device.cuh"
 #include "tq_index_impl.h"
 #include "tq_probe.h"
 
@@ -247,12 +248,10 @@ __global__ void to_bf16_kernel(const float* __restrict__ src, bf16* __restrict__
 }
 
 // Logits -> n_probe per query (see the file comment).
-__global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, const uint32_t* __restrict__ classes,
-                               int objective, float coverage, float min_conf, uint32_t fallback,
-                               uint32_t* __restrict__ out, float* __restrict__ conf_out) {
-  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (q >= M) return;
-  const float* z = Z + q * N;
+// The rule of one query's logits z[0..N): its n_probe, and its confidence
+// (largest predicted recall or class probability) in *conf.
+__device__ uint32_t predict_row(const float* z, int N, const uint32_t* __restrict__ classes, int objective,
+                                float coverage, float min_conf, uint32_t fallback, float* conf) {
   if (objective == TQ_PROBE_OBJECTIVE_RECALL) {
     const float per_probe = coverage / static_cast<float>(classes[N - 1]);
     float best = -INFINITY, top_r = 0.f;
@@ -266,9 +265,8 @@ __global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, 
       }
       top_r = fmaxf(top_r, r);
     }
-    out[q] = top_r < min_conf ? fallback : classes[pick];
-    if (conf_out) conf_out[q] = top_r;
-    return;
+    *conf = top_r;
+    return top_r < min_conf ? fallback : classes[pick];
   }
   float mx = -INFINITY;
   for (int j = 0; j < N; ++j) mx = fmaxf(mx, z[j]);
@@ -286,8 +284,183 @@ __global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, 
       picked = true;
     }
   }
-  out[q] = best < min_conf ? fallback : classes[pick];
-  if (conf_out) conf_out[q] = best;
+  *conf = best;
+  return best < min_conf ? fallback : classes[pick];
+}
+
+__global__ void predict_kernel(const float* __restrict__ Z, long long M, int N, const uint32_t* __restrict__ classes,
+                               int objective, float coverage, float min_conf, uint32_t fallback,
+                               uint32_t* __restrict__ out, float* __restrict__ conf_out) {
+  const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  float conf;
+  out[q] = predict_row(Z + q * N, N, classes, objective, coverage, min_conf, fallback, &conf);
+  if (conf_out) conf_out[q] = conf;
+}
+
+// ---------------------------------------------------------------------------
+// Fused prediction for the default shape (512 inputs, two hidden layers of
+// 128, at most 32 classes): the features, the three products with their bias
+// (and ReLU) epilogues, and the rule, for 64 queries per CTA of 4 warps (16
+// rows each), in one launch instead of eight. Every output is accumulated by
+// the same m16n8k16 sequence (k ascending in steps of 16, from zero) as in
+// gemm_bf16_tc_kernel, and the epilogues round as bias_act_kernel does, so the
+// logits and the picks are those of the unfused kernels.
+// ---------------------------------------------------------------------------
+constexpr int kFuseRows = 64, kFuseHidden = 128, kFuseKC = 32, kFusePad = 8;
+struct FusedSmem {
+  bf16 x[kFuseRows][kInputs + kFusePad];      // standardized inputs (rows 1,040 B apart)
+  bf16 h[kFuseRows][kFuseHidden + kFusePad];  // hidden activations
+  bf16 w[kFuseHidden][kFuseKC + kFusePad];    // one 32-deep chunk of a layer's weights, n-major
+  float z[kFuseRows][kMaxClasses + 1];        // logits
+};
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// acc (this warp's 16 rows x NJ*8 columns) = A (rows of lda bf16) . W, W the
+// layer's K x N bf16 weights (row-major, global); columns >= N get zeros.
+template <int NJ>
+__device__ __forceinline__ void fused_product(const bf16* A, int lda, int K, const bf16* __restrict__ W, int N,
+                                              FusedSmem& sm, float (&acc)[NJ][4]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const bf16 zero = __float2bfloat16_rn(0.f);
+#pragma unroll
+  for (int j = 0; j < NJ; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += kFuseKC) {
+    __syncthreads();  // the previous chunk is consumed (and A's rows are written)
+    for (int e = threadIdx.x; e < NJ * 8 * kFuseKC; e += blockDim.x) {
+      const int c = e / (NJ * 8), n = e % (NJ * 8);  // coalesced along n
+      sm.w[n][c] = n < N ? W[static_cast<long long>(k0 + c) * N + n] : zero;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kFuseKC; kk += 16) {
+      const int r = warp * 16 + g, k = k0 + kk + 2 * q;
+      uint32_t af[4];
+      af[0] = *reinterpret_cast<const uint32_t*>(A + r * lda + k);
+      af[1] = *reinterpret_cast<const uint32_t*>(A + (r + 8) * lda + k);
+      af[2] = *reinterpret_cast<const uint32_t*>(A + r * lda + k + 8);
+      af[3] = *reinterpret_cast<const uint32_t*>(A + (r + 8) * lda + k + 8);
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&sm.w[j * 8 + g][kk + 2 * q]);
+        const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&sm.w[j * 8 + g][kk + 8 + 2 * q]);
+        mma_bf16(acc[j], af, b0, b1);
+      }
+    }
+  }
+}
+
+// bias, ReLU, bf16 into this warp's rows of sm.h
+__device__ __forceinline__ void fused_hidden_epilogue(const float (&acc)[kFuseHidden / 8][4],
+                                                      const float* __restrict__ bias, FusedSmem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  __syncwarp();  // every lane of the warp is done reading its rows of sm.h
+#pragma unroll
+  for (int j = 0; j < kFuseHidden / 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int r = warp * 16 + g + (e >> 1) * 8, c = j * 8 + 2 * q + (e & 1);
+      const float zv = __fadd_rn(acc[j][e], bias[c]);
+      sm.h[r][c] = __float2bfloat16_rn(zv > 0.f ? zv : 0.f);
+    }
+}
+
+__global__ void __launch_bounds__(128) predict_fused_kernel(const float* __restrict__ top, long long m, int p,
+                                                            const float* __restrict__ mu,
+                                                            const float* __restrict__ inv_sd,
+                                                            const bf16* __restrict__ w0, const float* __restrict__ b0,
+                                                            const bf16* __restrict__ w1, const float* __restrict__ b1,
+                                                            const bf16* __restrict__ w2, const float* __restrict__ b2,
+                                                            int n_classes, const uint32_t* __restrict__ classes,
+                                                            int objective, float coverage, float min_conf,
+                                                            uint32_t fallback, uint32_t* __restrict__ out,
+                                                            float* __restrict__ conf_out) {
+  extern __shared__ __align__(16) unsigned char fused_smem[];
+  FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fused_smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long q0 = static_cast<long long>(blockIdx.x) * kFuseRows;
+  // Features of this warp's 16 queries; lane l holds scores 8l .. 8l+7.
+  for (int rr = 0; rr < 16; ++rr) {
+    const int r = warp * 16 + rr;
+    const long long qi = q0 + r;
+    float s[8];
+    int any = 0;
+    float last = 0.f;  // this lane's last valid score
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int i = lane * 8 + j;
+      s[j] = (qi < m && i < p) ? top[qi * p + i] : -INFINITY;
+      if (s[j] > -INFINITY) {
+        any = 1;
+        last = s[j];
+      }
+    }
+    // Missing scores repeat the last valid one before them (0 when there is
+    // none): an inclusive scan over lanes of "the last valid score so far",
+    // then this lane's carry-in from the lane before.
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+      const float lv = __shfl_up_sync(full_mask(), last, o);
+      const int la = __shfl_up_sync(full_mask(), any, o);
+      if (lane >= o && la && !any) {
+        last = lv;
+        any = 1;
+      }
+    }
+    const float carry = __shfl_up_sync(full_mask(), last, 1);
+    const int have = __shfl_up_sync(full_mask(), any, 1);
+    float cur = (lane >= 1 && have) ? carry : 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (s[j] > -INFINITY) {
+        cur = s[j];
+      } else {
+        s[j] = cur;
+      }
+    }
+    const float next = __shfl_down_sync(full_mask(), s[0], 1);  // score 8l + 8
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int i = lane * 8 + j;
+      const float gap = i + 1 < kRouteFeatures ? __fsub_rn(s[j], j < 7 ? s[j + 1] : next) : 0.f;
+      sm.x[r][i] = __float2bfloat16_rn(__fmul_rn(__fsub_rn(s[j], mu[i]), inv_sd[i]));
+      sm.x[r][kRouteFeatures + i] =
+          __float2bfloat16_rn(__fmul_rn(__fsub_rn(gap, mu[kRouteFeatures + i]), inv_sd[kRouteFeatures + i]));
+    }
+  }
+  float acc[kFuseHidden / 8][4];
+  fused_product<kFuseHidden / 8>(&sm.x[0][0], kInputs + kFusePad, kInputs, w0, kFuseHidden, sm, acc);
+  fused_hidden_epilogue(acc, b0, sm);
+  fused_product<kFuseHidden / 8>(&sm.h[0][0], kFuseHidden + kFusePad, kFuseHidden, w1, kFuseHidden, sm, acc);
+  fused_hidden_epilogue(acc, b1, sm);
+  float lz[kMaxClasses / 8][4];
+  fused_product<kMaxClasses / 8>(&sm.h[0][0], kFuseHidden + kFusePad, kFuseHidden, w2, n_classes, sm, lz);
+  {
+    const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int j = 0; j < kMaxClasses / 8; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = warp * 16 + g + (e >> 1) * 8, c = j * 8 + 2 * q + (e & 1);
+        if (c < n_classes) sm.z[r][c] = __fadd_rn(lz[j][e], b2[c]);
+      }
+  }
+  __syncthreads();
+  if (threadIdx.x < kFuseRows && q0 + threadIdx.x < m) {
+    const long long qi = q0 + threadIdx.x;
+    float conf;
+    out[qi] = predict_row(sm.z[threadIdx.x], n_classes, classes, objective, coverage, min_conf, fallback, &conf);
+    if (conf_out) conf_out[qi] = conf;
+  }
 }
 
 // Every MLP product (forward, dW = X^T.dZ, dX = dZ.W^T) has bf16 operands and
@@ -462,10 +635,31 @@ void probe_reserve(tq_probe_mlp* h, size_t m, ProbeScratch& sc) {
   sc.act1.reserve(m * widest * 2);
 }
 
+// The default shape (512 inputs, two hidden layers of 128) predicts in one
+// fused launch; false for other shapes.
+bool predict_fused(tq_probe_mlp* h, const float* d_top, long long M, int p, float coverage, float min_conf,
+                   uint32_t fallback, uint32_t* d_out, float* d_conf, cudaStream_t s) {
+  if (!(h->n_layers == 2 && h->fan_in[0] == kInputs && h->fan_out[0] == kFuseHidden &&
+        h->fan_out[1] == kFuseHidden && h->n_classes <= kMaxClasses)) {
+    return false;
+  }
+  constexpr size_t smem = sizeof(FusedSmem);
+  check(cudaFuncSetAttribute(predict_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)),
+        "fused predict attribute");
+  predict_fused_kernel<<<static_cast<unsigned>((M + kFuseRows - 1) / kFuseRows), 128, smem, s>>>(
+      d_top, M, p, h->d_mu.as<float>(), h->d_isd.as<float>(), h->wbf(0), h->bias(0), h->wbf(1), h->bias(1),
+      h->wbf(2), h->bias(2), h->n_classes, h->d_classes.as<uint32_t>(), h->objective, coverage, min_conf, fallback,
+      d_out, d_conf);
+  check(cudaGetLastError(), "fused predict kernel");
+  return true;
+}
+
 void probe_predict(tq_probe_mlp* h, const float* d_top, size_t m, int p, float coverage, float min_conf,
                    uint32_t fallback, uint32_t* d_out, cudaStream_t s, ProbeScratch& sc) {
   if (m == 0) return;
   const long long M = static_cast<long long>(m);
+  if (predict_fused(h, d_top, M, p, coverage, min_conf, fallback, d_out, nullptr, s)) return;
   probe_reserve(h, m, sc);
   features_kernel<<<static_cast<unsigned>(m), 256, 0, s>>>(d_top, M, p, h->d_mu.as<float>(), h->d_isd.as<float>(),
                                                            sc.x.as<bf16>(), nullptr);
@@ -771,6 +965,10 @@ int tq_probe_mlp_predict_device(tq_probe_mlp* h, const float* d_top_scores, size
     vcb::DeviceGuard g(h->device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
     if (s != h->stream) h->sync();
+    if (vcb::predict_fused(h, d_top_scores, static_cast<long long>(m), static_cast<int>(p), coverage,
+                           min_confidence, fallback, d_n_probe, d_confidence, s)) {
+      return;
+    }
     h->forward(d_top_scores, m, static_cast<int>(p), s);
     vcb::predict_kernel<<<vcb::blocks(static_cast<long long>(m)), 256, 0, s>>>(
         h->z[h->n_lin() - 1].as<float>(), static_cast<long long>(m), h->n_classes, h->d_classes.as<uint32_t>(),
