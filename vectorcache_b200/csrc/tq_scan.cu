@@ -252,18 +252,6 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
   const int g_last = kBatch ? min(g_first + kFlushGroups, nbg) : (MODE == 2 ? 0 : nbg);
   const bool resident = MODE != 0 || chunk >= nbg;
   constexpr long long kGroupStride = kTileWords / 2;  // uint2 per group row
-  // A batch-split CTA scans one 256-group batch of one block: its first ring
-  // of code loads goes out before the LUT batch is staged, so the two
-  // latencies overlap instead of adding up once per CTA.
-  [[maybe_unused]] uint2 pre[PF];
-  if constexpr (kBatch && STAGES == 0) {
-    const long long tile0 = v_begin / kTileVectors + (warp >> 1);
-    const uint2* wp0 = reinterpret_cast<const uint2*>(a.codes + tile0 * nbg * kTileWords + (warp & 1) * 64) + lane;
-#pragma unroll
-    for (int u = 0; u < PF; ++u) {
-      pre[u] = (g_first + u < g_last) ? wp0[static_cast<long long>(g_first + u) * kGroupStride] : make_uint2(0u, 0u);
-    }
-  }
   if constexpr (kBatch) {
     load_lut_chunk(g_first, g_last - g_first);
     __syncthreads();
@@ -406,13 +394,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         if (Q <= 2 && (g_stop - gb) % PF == 0) {
           const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
 #pragma unroll
-          for (int u = 0; u < PF; ++u) {
-            if constexpr (kBatch) {
-              ring[u] = pre[u];  // the CTA's only batch, loaded before the LUT
-            } else {
-              ring[u] = src[u * kGroupStride];
-            }
-          }
+          for (int u = 0; u < PF; ++u) ring[u] = src[u * kGroupStride];
           src += PF * kGroupStride;
           int g = gb;
           for (; g + PF < g_stop; g += PF) {
@@ -429,11 +411,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         } else {
 #pragma unroll
           for (int u = 0; u < PF; ++u) {
-            if constexpr (kBatch) {
-              ring[u] = pre[u];
-            } else {
-              ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
-            }
+            ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
           }
           for (int g = gb; g < g_stop; g += PF) {
             uint2 cur[PF];
