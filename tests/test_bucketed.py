@@ -270,4 +270,22 @@ def test_floor_schedules_at_many_buckets(oracle):
                                    tr["offsets"], 10)
         assert np.array_equal(whole.ids[sub], wi), n_probe
         assert bits_equal(whole.scores[sub], ws), n_probe
+    # Per-query counts under a 512 cap (the learned probe's form): in a pass of
+    # >= 4096 queries every query above 32 probes takes 32 first probes; in
+    # smaller passes only those from 256 on. Same top-k both ways, equal to the
+    # exhaustive scan of each query's own probes.
+    npq = np.random.default_rng(43).integers(1, 513, q.shape[0]).astype(np.uint32)
+    npq[:64] = np.arange(1, 65)  # every count around the 8 / 32 first-probe splits
+    whole = idx.search(q, 10, n_probe=512, n_probe_per_query=npq)
+    for s in range(0, q.shape[0], 1536):
+        part = idx.search(q[s:s + 1536], 10, n_probe=512, n_probe_per_query=npq[s:s + 1536])
+        assert np.array_equal(whole.ids[s:s + 1536], part.ids), s
+        assert bits_equal(whole.scores[s:s + 1536], part.scores), s
+    sub = slice(0, 512)
+    tr = idx.search_trace(q[sub], 10, n_probe=512, n_probe_per_query=npq[sub])
+    prep = oracle.prepare_queries(tr["q_hat"], 4)
+    ws, wi = oracle.ivf_search(prep, flat, alpha, slot_ids, starts, sizes, tr["probes"], npq[sub],
+                               tr["offsets"], 10)
+    assert np.array_equal(whole.ids[sub], wi)
+    assert bits_equal(whole.scores[sub], ws)
     idx.close()
