@@ -1093,7 +1093,10 @@ struct ItemQueries {
 // every other 256-slot tile set); QW = 2: 4 groups of 2 queries x 1 tile set
 // (a warp scans every tile set: half the registers for accumulators, so more
 // CTAs fit on an SM; the bucket scan takes this form).
-template <bool NIBBLE8, int QW = 4>
+// WHOLE: every 256-group batch of the item's index is a whole number of
+// kBsPrefetch-group rings (nbg a multiple of kBsPrefetch); the ring loop then
+// runs without bounds checks.
+template <bool NIBBLE8, int QW = 4, bool WHOLE = false>
 __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& iq, unsigned char* smem) {
   constexpr int kGroups = kItemQueries / QW;  // query groups per item
   constexpr int kTsets = kBsWarps / kGroups;  // tile sets scanned side by side
@@ -1175,69 +1178,51 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
       }
       if (!active) continue;
       const int chunk_base = resident ? 0 : gb;
+      const LutHalf* lq = s_lut + (quad * QW) * chunk * 2;  // this warp's queries
       uint2 ring[kBsPrefetch];
+      if constexpr (WHOLE) {
+        // Every batch is a whole number of rings: no bounds checks, loads at
+        // immediate offsets of a running pointer.
+        const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
 #pragma unroll
-      for (int u = 0; u < kBsPrefetch; ++u) {
-        ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
-      }
-      for (int g = gb; g < g_stop; g += kBsPrefetch) {
-        uint2 cur[kBsPrefetch];
+        for (int u = 0; u < kBsPrefetch; ++u) ring[u] = src[u * kGroupStride];
+        src += kBsPrefetch * kGroupStride;
+        int g = gb;
+        for (; g + kBsPrefetch < g_stop; g += kBsPrefetch) {
+          uint2 cur[kBsPrefetch];
 #pragma unroll
-        for (int u = 0; u < kBsPrefetch; ++u) {
-          cur[u] = ring[u];
-          const int gn = g + kBsPrefetch + u;
-          ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+          for (int u = 0; u < kBsPrefetch; ++u) {
+            cur[u] = ring[u];
+            ring[u] = src[u * kGroupStride];
+          }
+          src += kBsPrefetch * kGroupStride;
+#pragma unroll
+          for (int u = 0; u < kBsPrefetch; u += 2) {
+            lookup_group_pair<QW, NIBBLE8>(cur[u], cur[u + 1], lq + (g + u - chunk_base) * 2, chunk * 2, acc);
+          }
         }
-        // Groups in pairs (nbg and the 256-group batches are even).
 #pragma unroll
         for (int u = 0; u < kBsPrefetch; u += 2) {
-          if (g + u >= g_stop) break;
-          const uint32_t a0 = cur[u].x, a1 = cur[u].y, b0 = cur[u + 1].x, b1 = cur[u + 1].y;
-          const uint32_t a0h = a0 >> 16, a1h = a1 >> 16, b0h = b0 >> 16, b1h = b1 >> 16;
-          uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
-          if constexpr (!NIBBLE8) {
-            ta0 = a0 ^ 0x88888888u;
-            ta1 = a1 ^ 0x88888888u;
-            tb0 = b0 ^ 0x88888888u;
-            tb1 = b1 ^ 0x88888888u;
-            ta0h = ta0 >> 16;
-            ta1h = ta1 >> 16;
-            tb0h = tb0 >> 16;
-            tb1h = tb1 >> 16;
-          }
-          const LutHalf* lg = s_lut + (quad * QW) * chunk * 2 + (g + u - chunk_base) * 2;
+          lookup_group_pair<QW, NIBBLE8>(ring[u], ring[u + 1], lq + (g + u - chunk_base) * 2, chunk * 2, acc);
+        }
+      } else {
 #pragma unroll
-          for (int q = 0; q < QW; ++q) {
-            const LutHalf Fa = lg[q * chunk * 2];
-            const LutHalf Sa = lg[q * chunk * 2 + 1];
-            const LutHalf Fb = lg[q * chunk * 2 + 2];
-            const LutHalf Sb = lg[q * chunk * 2 + 3];
-            uint32_t lo0, hi0, lo1, hi1;
-            if constexpr (NIBBLE8) {
-              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sb.w[0], Sb.w[1], b0);
-              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fb.w[0], Fb.w[1], b0h);
-              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sb.w[0], Sb.w[1], b1);
-              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fb.w[0], Fb.w[1], b1h);
-            } else {
-              lo0 = prmt(Sa.w[0], Sa.w[1], a0) + prmt(Sa.w[2], Sa.w[3], ta0) + prmt(Sb.w[0], Sb.w[1], b0) +
-                    prmt(Sb.w[2], Sb.w[3], tb0);
-              hi0 = prmt(Fa.w[0], Fa.w[1], a0h) + prmt(Fa.w[2], Fa.w[3], ta0h) + prmt(Fb.w[0], Fb.w[1], b0h) +
-                    prmt(Fb.w[2], Fb.w[3], tb0h);
-              lo1 = prmt(Sa.w[0], Sa.w[1], a1) + prmt(Sa.w[2], Sa.w[3], ta1) + prmt(Sb.w[0], Sb.w[1], b1) +
-                    prmt(Sb.w[2], Sb.w[3], tb1);
-              hi1 = prmt(Fa.w[0], Fa.w[1], a1h) + prmt(Fa.w[2], Fa.w[3], ta1h) + prmt(Fb.w[0], Fb.w[1], b1h) +
-                    prmt(Fb.w[2], Fb.w[3], tb1h);
-            }
-            const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
-            const uint32_t m10 = prmt(lo1, hi1, 0x5140u), m11 = prmt(lo1, hi1, 0x7362u);
-            acc[q][0] = __dp4a(m00, 0x00000101u, acc[q][0]);
-            acc[q][1] = __dp4a(m00, 0x01010000u, acc[q][1]);
-            acc[q][2] = __dp4a(m01, 0x00000101u, acc[q][2]);
-            acc[q][3] = __dp4a(m01, 0x01010000u, acc[q][3]);
-            acc[q][4] = __dp4a(m10, 0x00000101u, acc[q][4]);
-            acc[q][5] = __dp4a(m10, 0x01010000u, acc[q][5]);
-            acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
-            acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
+        for (int u = 0; u < kBsPrefetch; ++u) {
+          ring[u] = (gb + u < g_stop) ? wp[(gb + u) * kGroupStride] : make_uint2(0u, 0u);
+        }
+        for (int g = gb; g < g_stop; g += kBsPrefetch) {
+          uint2 cur[kBsPrefetch];
+#pragma unroll
+          for (int u = 0; u < kBsPrefetch; ++u) {
+            cur[u] = ring[u];
+            const int gn = g + kBsPrefetch + u;
+            ring[u] = (gn < g_stop) ? wp[gn * kGroupStride] : make_uint2(0u, 0u);
+          }
+          // Groups in pairs (nbg and the 256-group batches are even).
+#pragma unroll
+          for (int u = 0; u < kBsPrefetch; u += 2) {
+            if (g + u >= g_stop) break;
+            lookup_group_pair<QW, NIBBLE8>(cur[u], cur[u + 1], lq + (g + u - chunk_base) * 2, chunk * 2, acc);
           }
         }
       }
@@ -1426,7 +1411,7 @@ __device__ __forceinline__ void scan_item(const ItemView& v, const ItemQueries& 
 }
 
 // One work item (a bucket and up to kItemQueries of its probing queries).
-template <bool NIBBLE8>
+template <bool NIBBLE8, bool WHOLE>
 __device__ __forceinline__ void bucket_scan_item(const BucketScanArgs& a, const uint4 it, ItemQueries& iq,
                                                  unsigned char* smem) {
   const int b = static_cast<int>(it.x);
@@ -1457,7 +1442,7 @@ __device__ __forceinline__ void bucket_scan_item(const BucketScanArgs& a, const 
   const ItemView v{a.codes, a.alpha, a.slot_ids, static_cast<long long>(a.slot_start[b]),
                    static_cast<int>(a.bucket_size[b]), a.nbg, a.luts, a.k, pc, a.cand_score, a.cand_id,
                    a.append_count};
-  scan_item<NIBBLE8, kBsQueriesPerWarp>(v, iq, smem);
+  scan_item<NIBBLE8, kBsQueriesPerWarp, WHOLE>(v, iq, smem);
 }
 
 // kBsQueriesPerWarp = 2: 96 registers, 5 CTAs per SM (20 warps; 4 queries per
@@ -1467,7 +1452,7 @@ __device__ __forceinline__ void bucket_scan_item(const BucketScanArgs& a, const 
 // (per-query probe counts up to a large maximum) costs no empty CTAs. (A fixed
 // stride over the items instead measured 9 % slower than one item per CTA:
 // items are uneven; pulling balances them as the block scheduler does.)
-template <bool NIBBLE8>
+template <bool NIBBLE8, bool WHOLE>
 __global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketScanArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ ItemQueries iq;
@@ -1479,7 +1464,7 @@ __global__ void __launch_bounds__(kBsWarps * 32, 5) bucket_scan_kernel(BucketSca
     __syncthreads();
     const unsigned long long item = s_item;
     if (item >= n_items) return;
-    bucket_scan_item<NIBBLE8>(a, a.items[item], iq, smem);
+    bucket_scan_item<NIBBLE8, WHOLE>(a, a.items[item], iq, smem);
   }
 }
 
@@ -1861,7 +1846,10 @@ cudaError_t launch_bucket_scan(const BucketScanArgs& a, long long grid, cudaStre
   const size_t smem =
       static_cast<size_t>(kItemQueries) * chunk * 32 +
       static_cast<size_t>(kBsWarps) * (static_cast<size_t>(kBsQueriesPerWarp) * kmax * 8 + kBsBuf * 8);
-  auto kern = a.bits == 3 ? bucket_scan_kernel<true> : bucket_scan_kernel<false>;
+  // Whole rings when nbg is a multiple of the ring (no bounds checks).
+  const bool whole = a.nbg % kBsPrefetch == 0;
+  auto kern = a.bits == 3 ? (whole ? bucket_scan_kernel<true, true> : bucket_scan_kernel<true, false>)
+                          : (whole ? bucket_scan_kernel<false, true> : bucket_scan_kernel<false, false>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   // Resident CTAs of this shape, cached per thread (device, variant, size).

@@ -181,6 +181,74 @@ struct __align__(16) LutHalf {
   uint32_t w[4];
 };
 
+// The lookups of one pair of byte groups (codes ca = group g, cb = group g + 1,
+// 8 vectors of a lane) for Q queries, added into acc. The LUT halves of query
+// q start at lg + q * q_stride: [F(g), S(g), F(g+1), S(g+1)], F the 16 entries
+// of the high nibble (first half of the group's codes), S of the low nibble.
+// The second-half lookups of both groups add into one byte per vector
+// (<= 2 * 127), the first-half lookups into another; one prmt interleaves the
+// two bytes of each vector so a single dp4a adds both. Measured and rejected
+// (bit-exact, slower or equal): the selector shifts on the FMA pipe as mul.hi
+// (1M x 1536 one query 0.187 -> 0.191 ms), every byte-sum addition as a
+// multiply-add (-> 0.195 ms), the last addition of each four-lookup sum as a
+// multiply-add with four queries per CTA (10k queries 870.0 -> 876.0 ms with
+// the unchecked 4-group ring, 853.6 vs 853.3 ms with the 8-group ring).
+template <int Q, bool NIBBLE8>
+__device__ __forceinline__ void lookup_group_pair(uint2 ca, uint2 cb, const LutHalf* lg, int q_stride,
+                                                  uint32_t (&acc)[Q][8]) {
+  auto hi16 = [](uint32_t x) -> uint32_t { return x >> 16; };
+  auto add2 = [](uint32_t x, uint32_t y) -> uint32_t { return x + y; };
+  auto add4 = [](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t { return x + y + z + w; };
+  const uint32_t a0 = ca.x, a1 = ca.y, b0 = cb.x, b1 = cb.y;
+  const uint32_t a0h = hi16(a0), a1h = hi16(a1), b0h = hi16(b0), b1h = hi16(b1);
+  [[maybe_unused]] uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
+  if constexpr (!NIBBLE8) {
+    ta0 = a0 ^ 0x88888888u;
+    ta1 = a1 ^ 0x88888888u;
+    tb0 = b0 ^ 0x88888888u;
+    tb1 = b1 ^ 0x88888888u;
+    ta0h = hi16(ta0);
+    ta1h = hi16(ta1);
+    tb0h = hi16(tb0);
+    tb1h = hi16(tb1);
+  }
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const LutHalf Fa = lg[q * q_stride];      // group g: entries 0..15 (high nibble)
+    const LutHalf Sa = lg[q * q_stride + 1];  //          entries 16..31 (low nibble)
+    const LutHalf Fb = lg[q * q_stride + 2];  // group g + 1
+    const LutHalf Sb = lg[q * q_stride + 3];
+    uint32_t lo0, hi0, lo1, hi1;
+    if constexpr (NIBBLE8) {
+      // 3-bit codes: every nibble is < 8, entries 8..15 are never used.
+      lo0 = add2(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sb.w[0], Sb.w[1], b0));
+      hi0 = add2(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fb.w[0], Fb.w[1], b0h));
+      lo1 = add2(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sb.w[0], Sb.w[1], b1));
+      hi1 = add2(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fb.w[0], Fb.w[1], b1h));
+    } else {
+      lo0 = add4(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sa.w[2], Sa.w[3], ta0), prmt(Sb.w[0], Sb.w[1], b0),
+                 prmt(Sb.w[2], Sb.w[3], tb0));
+      hi0 = add4(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fa.w[2], Fa.w[3], ta0h), prmt(Fb.w[0], Fb.w[1], b0h),
+                 prmt(Fb.w[2], Fb.w[3], tb0h));
+      lo1 = add4(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sa.w[2], Sa.w[3], ta1), prmt(Sb.w[0], Sb.w[1], b1),
+                 prmt(Sb.w[2], Sb.w[3], tb1));
+      hi1 = add4(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fa.w[2], Fa.w[3], ta1h), prmt(Fb.w[0], Fb.w[1], b1h),
+                 prmt(Fb.w[2], Fb.w[3], tb1h));
+    }
+    // [lo.b0, hi.b0, lo.b1, hi.b1] and [lo.b2, hi.b2, lo.b3, hi.b3]
+    const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
+    const uint32_t m10 = prmt(lo1, hi1, 0x5140u), m11 = prmt(lo1, hi1, 0x7362u);
+    acc[q][0] = __dp4a(m00, 0x00000101u, acc[q][0]);
+    acc[q][1] = __dp4a(m00, 0x01010000u, acc[q][1]);
+    acc[q][2] = __dp4a(m01, 0x00000101u, acc[q][2]);
+    acc[q][3] = __dp4a(m01, 0x01010000u, acc[q][3]);
+    acc[q][4] = __dp4a(m10, 0x00000101u, acc[q][4]);
+    acc[q][5] = __dp4a(m10, 0x01010000u, acc[q][5]);
+    acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
+    acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
+  }
+}
+
 // Warp-cooperative bitonic sort of p (a power of two) entries in
 // shared memory, best first under `better`.
 __device__ __forceinline__ void warp_sort_best_first(float* s, uint32_t* id, int p, int lane) {

@@ -139,83 +139,6 @@ struct RegTopK {
   }
 };
 
-// The lookups of one pair of byte groups (codes ca = group g, cb = group g + 1,
-// 8 vectors of a lane) for Q queries, added into acc. The LUT halves of query
-// q start at lg + q * q_stride: [F(g), S(g), F(g+1), S(g+1)], F the 16 entries
-// of the high nibble (first half of the group's codes), S of the low nibble.
-// The second-half lookups of both groups add into one byte per vector
-// (<= 2 * 127), the first-half lookups into another; one prmt interleaves the
-// two bytes of each vector so a single dp4a adds both. `one` is 1 at run
-// time: with four or more queries the last addition of each four-lookup sum
-// is a multiply-add by it, which moves it from the integer pipe (busy with
-// prmt) to the FMA pipe (1000.1 -> 992.1 ms at 10k queries x 1M x 1536).
-// Measured at 1M x 1536 one query: moving the selector shifts to the FMA pipe
-// as mul.hi (0.187 -> 0.191 ms) or every byte-sum addition (-> 0.195 ms) only
-// moved the bottleneck there.
-template <int Q, bool NIBBLE8>
-__device__ __forceinline__ void lookup_group_pair(uint2 ca, uint2 cb, const LutHalf* lg, int q_stride, uint32_t one,
-                                                  uint32_t (&acc)[Q][8]) {
-  auto hi16 = [](uint32_t x) -> uint32_t { return x >> 16; };
-  auto add2 = [](uint32_t x, uint32_t y) -> uint32_t { return x + y; };
-  auto add4 = [one](uint32_t x, uint32_t y, uint32_t z, uint32_t w) -> uint32_t {
-    if constexpr (Q >= 4) {
-      uint32_t r;
-      asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(w), "r"(one), "r"(x + y + z));
-      return r;
-    } else {
-      return x + y + z + w;
-    }
-  };
-  const uint32_t a0 = ca.x, a1 = ca.y, b0 = cb.x, b1 = cb.y;
-  const uint32_t a0h = hi16(a0), a1h = hi16(a1), b0h = hi16(b0), b1h = hi16(b1);
-  [[maybe_unused]] uint32_t ta0 = 0, ta1 = 0, tb0 = 0, tb1 = 0, ta0h = 0, ta1h = 0, tb0h = 0, tb1h = 0;
-  if constexpr (!NIBBLE8) {
-    ta0 = a0 ^ 0x88888888u;
-    ta1 = a1 ^ 0x88888888u;
-    tb0 = b0 ^ 0x88888888u;
-    tb1 = b1 ^ 0x88888888u;
-    ta0h = hi16(ta0);
-    ta1h = hi16(ta1);
-    tb0h = hi16(tb0);
-    tb1h = hi16(tb1);
-  }
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const LutHalf Fa = lg[q * q_stride];      // group g: entries 0..15 (high nibble)
-    const LutHalf Sa = lg[q * q_stride + 1];  //          entries 16..31 (low nibble)
-    const LutHalf Fb = lg[q * q_stride + 2];  // group g + 1
-    const LutHalf Sb = lg[q * q_stride + 3];
-    uint32_t lo0, hi0, lo1, hi1;
-    if constexpr (NIBBLE8) {
-      // 3-bit codes: every nibble is < 8, entries 8..15 are never used.
-      lo0 = add2(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sb.w[0], Sb.w[1], b0));
-      hi0 = add2(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fb.w[0], Fb.w[1], b0h));
-      lo1 = add2(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sb.w[0], Sb.w[1], b1));
-      hi1 = add2(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fb.w[0], Fb.w[1], b1h));
-    } else {
-      lo0 = add4(prmt(Sa.w[0], Sa.w[1], a0), prmt(Sa.w[2], Sa.w[3], ta0), prmt(Sb.w[0], Sb.w[1], b0),
-                 prmt(Sb.w[2], Sb.w[3], tb0));
-      hi0 = add4(prmt(Fa.w[0], Fa.w[1], a0h), prmt(Fa.w[2], Fa.w[3], ta0h), prmt(Fb.w[0], Fb.w[1], b0h),
-                 prmt(Fb.w[2], Fb.w[3], tb0h));
-      lo1 = add4(prmt(Sa.w[0], Sa.w[1], a1), prmt(Sa.w[2], Sa.w[3], ta1), prmt(Sb.w[0], Sb.w[1], b1),
-                 prmt(Sb.w[2], Sb.w[3], tb1));
-      hi1 = add4(prmt(Fa.w[0], Fa.w[1], a1h), prmt(Fa.w[2], Fa.w[3], ta1h), prmt(Fb.w[0], Fb.w[1], b1h),
-                 prmt(Fb.w[2], Fb.w[3], tb1h));
-    }
-    // [lo.b0, hi.b0, lo.b1, hi.b1] and [lo.b2, hi.b2, lo.b3, hi.b3]
-    const uint32_t m00 = prmt(lo0, hi0, 0x5140u), m01 = prmt(lo0, hi0, 0x7362u);
-    const uint32_t m10 = prmt(lo1, hi1, 0x5140u), m11 = prmt(lo1, hi1, 0x7362u);
-    acc[q][0] = __dp4a(m00, 0x00000101u, acc[q][0]);
-    acc[q][1] = __dp4a(m00, 0x01010000u, acc[q][1]);
-    acc[q][2] = __dp4a(m01, 0x00000101u, acc[q][2]);
-    acc[q][3] = __dp4a(m01, 0x01010000u, acc[q][3]);
-    acc[q][4] = __dp4a(m10, 0x00000101u, acc[q][4]);
-    acc[q][5] = __dp4a(m10, 0x01010000u, acc[q][5]);
-    acc[q][6] = __dp4a(m11, 0x00000101u, acc[q][6]);
-    acc[q][7] = __dp4a(m11, 0x01010000u, acc[q][7]);
-  }
-}
-
 // Staged code stream: group rows per slot, and slots per warp by queries per
 // CTA (shared memory: 8 warps x slots x 8 rows x 256 bytes = 96 KB at one
 // query, 80 KB at two, beside the LUTs, two CTAs per SM).
@@ -249,7 +172,7 @@ constexpr size_t scan_stage_bytes(int q) {
 // the lookups; the bytes in flight no longer cost registers, so a memory-bound
 // scan keeps more of them in flight (a wait_group and a __syncwarp per slot,
 // no spin loop).
-template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0, int STAGES = 0>
+template <int Q, int KMAX, int MIN_BLOCKS, bool NIBBLE8, int PF, int MODE = 0, int STAGES = 0, bool WHOLE = false>
 __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanArgs a) {
   static_assert(PF % 2 == 0, "byte groups are consumed in pairs");
   static_assert(STAGES == 0 || (STAGES >= 2 && KMAX <= kRegTopK && MODE == 0),
@@ -265,7 +188,6 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
     s_stage = reinterpret_cast<uint2*>(smem + scan_stage_offset(Q, chunk)) + warp * (STAGES * PF * 32);
   }
 
-  const uint32_t one = (static_cast<uint32_t>(a.nbg) >> 31) ^ 1u;  // 1, opaque to the compiler
   const long long q0 = static_cast<long long>(blockIdx.x) * Q;
   const int range = blockIdx.y;
   const long long v_begin = static_cast<long long>(range) * a.range_vectors;
@@ -390,7 +312,7 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           if constexpr (decltype(checked)::value) {
             if (g + u >= g_stop) break;
           }
-          lookup_group_pair<Q, NIBBLE8>(cur[u], cur[u + 1], s_lut + (g + u - chunk_base) * 2, chunk * 2, one, acc);
+          lookup_group_pair<Q, NIBBLE8>(cur[u], cur[u + 1], s_lut + (g + u - chunk_base) * 2, chunk * 2, acc);
         }
       };
       if constexpr (STAGES > 0) {
@@ -406,12 +328,14 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
         }
       } else {
         uint2 ring[PF];
-        // One or two queries: whole rings (every 256-group batch of a 4- or
-        // 3-bit row of 512+ dims) run without bounds checks, loading at
-        // immediate offsets of a running pointer. Four queries keep the checked
-        // loop: the second copy of the lookup body does not fit their 128
-        // registers.
-        if (Q <= 2 && (g_stop - gb) % PF == 0) {
+        // Whole rings (every batch a multiple of PF groups) run without bounds
+        // checks, loading at immediate offsets of a running pointer: one or two
+        // queries decide per batch; four queries take the WHOLE instance
+        // (launched when nbg is a multiple of PF), which holds no checked copy
+        // of the lookup body — both copies do not fit their 128 registers.
+        // At 10k queries x 1M x 1536 the unchecked ring scans in 870.0 ms,
+        // the checked one in 992.7 ms (same 4-group ring).
+        if (WHOLE || (Q <= 2 && (g_stop - gb) % PF == 0)) {
           const uint2* src = wp + static_cast<long long>(gb) * kGroupStride;
 #pragma unroll
           for (int u = 0; u < PF; ++u) ring[u] = src[u * kGroupStride];
@@ -823,9 +747,9 @@ __global__ void dense_scores_kernel(const uint32_t* __restrict__ codes, const fl
   if (out_score) out_score[idx] = __fadd_rn(__fmul_rn(fa, alpha[v]), 0.f);
 }
 
-template <int Q, int KMAX, int MINB, bool N8, int PF, int STAGES = 0>
+template <int Q, int KMAX, int MINB, bool N8, int PF, int STAGES = 0, bool WHOLE = false>
 cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  auto kern = scan_kernel<Q, KMAX, MINB, N8, PF, 0, STAGES>;
+  auto kern = scan_kernel<Q, KMAX, MINB, N8, PF, 0, STAGES, WHOLE>;
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(plan.smem_bytes));
   if (e != cudaSuccess) return e;
@@ -835,8 +759,10 @@ cudaError_t launch_scan_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t 
 }
 
 // Prefetch depth per queries-per-CTA: the one-query kernel is memory-bound and
-// keeps 16 byte groups in flight per thread, the 4-query kernel is issue-bound.
-constexpr int prefetch_for(int q) { return q == 1 ? 16 : (q == 2 ? 8 : 4); }
+// keeps 16 byte groups in flight per thread; the 4-query kernel is issue-bound
+// and keeps 8 (10k queries x 1M x 1536 with the unchecked ring: 4 groups
+// 870.0 ms, 8 groups 853.3 ms, 16 groups 935.4 ms, register spills).
+constexpr int prefetch_for(int q) { return q == 1 ? 16 : (q == 2 ? 8 : 8); }
 
 // Batch-split scan: (block, batch) CTAs store integer sums, then one CTA per
 // (query group, range) flushes them in batch order and keeps the top k.
@@ -1000,6 +926,15 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
   if (q == QQ && km == KK) {                                                             \
     return n8 ? launch_scan_t<QQ, KK, MB, true, prefetch_for(QQ)>(a, plan, stream)       \
               : launch_scan_t<QQ, KK, MB, false, prefetch_for(QQ)>(a, plan, stream);     \
+  }
+  // Four queries over batches that are whole rings: the unchecked instance.
+  if (q == 4 && km == 32 && a.nbg % prefetch_for(4) == 0) {
+    return n8 ? launch_scan_t<4, 32, 2, true, prefetch_for(4), 0, true>(a, plan, stream)
+              : launch_scan_t<4, 32, 2, false, prefetch_for(4), 0, true>(a, plan, stream);
+  }
+  if (q == 4 && km == 64 && a.nbg % prefetch_for(4) == 0) {
+    return n8 ? launch_scan_t<4, 64, 1, true, prefetch_for(4), 0, true>(a, plan, stream)
+              : launch_scan_t<4, 64, 1, false, prefetch_for(4), 0, true>(a, plan, stream);
   }
   VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
   VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
