@@ -202,3 +202,38 @@ def test_staged_whole_rows_match_dense_scores(case):
             assert np.array_equal(res.ids[i], top), (nq, i)
             assert bits_equal(res.scores[i], scores[i][top]), (nq, i)
     idx.close()
+
+
+# One query over 1M rows splits by 256-group batch on four CTAs per SM (8 code
+# groups in flight per thread); smaller split scans keep two CTAs per SM. The
+# top-10 of one and of two queries against every vector's score from the
+# dense-scores kernel, ties by lower id.
+ONE_QUERY_SPLIT = [(1_000_000, 1536, 4), (1_000_000, 768, 3)]
+
+
+@pytest.mark.parametrize("case", ONE_QUERY_SPLIT, ids=lambda c: f"n{c[0]}_d{c[1]}_b{c[2]}")
+def test_one_query_split_matches_dense_scores(case):
+    torch = pytest.importorskip("torch")
+    from vectorcache_b200.synthetic import power_law_torch
+
+    n, dim, bits = case
+    dev = torch.device("cuda", 0)
+    idx = vcb.TurboQuantIndex(dim, bits)
+    x = power_law_torch(n, dim, seed=52, device=dev)
+    idx.calibrate_device(x[:10_000])
+    idx.add_device(x)
+    idx.prepare()
+    del x
+    torch.cuda.empty_cache()
+    q = power_law(2, dim, seed=53)
+    ids = np.arange(n)
+    for nq in (1, 2):
+        plan = idx.scan_plan(nq, 10)
+        assert plan["split_batches"] > 1 and plan["q_per_cta"] == nq, plan
+        res = idx.search(q[:nq], 10)
+        _, scores = idx.dense_scores(q[:nq])
+        for i in range(nq):
+            top = np.lexsort((ids, -scores[i]))[:10]
+            assert np.array_equal(res.ids[i], top), (nq, i)
+            assert bits_equal(res.scores[i], scores[i][top]), (nq, i)
+    idx.close()

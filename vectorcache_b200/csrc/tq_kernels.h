@@ -160,6 +160,10 @@ struct ScanPlan {
   // queries over few blocks (whole blocks per CTA would leave the last wave
   // of CTAs part-full); it needs ScanArgs::partial.
   int split_batches = 0;
+  // CTAs per SM of the one-query batch-split scan: 4 (8 groups in flight,
+  // 64 registers) or 2 (16 groups in flight), whichever wastes less of its
+  // last wave.
+  int split_ctas_per_sm = 2;
   // > 0: the code stream goes through this many shared-memory slots per warp
   // (one or two queries per CTA, register top-k).
   int stages = 0;

@@ -766,10 +766,8 @@ constexpr int prefetch_for(int q) { return q == 1 ? 16 : (q == 2 ? 8 : 8); }
 
 // Batch-split scan: (block, batch) CTAs store integer sums, then one CTA per
 // (query group, range) flushes them in batch order and keeps the top k.
-template <int Q, bool N8>
-cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
-  constexpr int kPf = prefetch_for(Q);
-  const long long blocks = (a.n + kScanBlockVectors - 1) / kScanBlockVectors;
+template <int Q, bool N8, int PF, int MINB>
+cudaError_t launch_split_mode(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream, long long blocks) {
   const unsigned qgroups = static_cast<unsigned>((a.nq + Q - 1) / Q);
   ScanArgs s = a;
   s.range_vectors = kScanBlockVectors;
@@ -781,30 +779,41 @@ cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t
     // One launch: the CTA completing a block flushes it (its lists are the
     // plan's ranges, one block each). The LUT area also holds the merge.
     const size_t smem3 = std::max(smem1, static_cast<size_t>(Q) * kScanWarps * kWarp * 8);
-    cudaError_t e3 = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, 2, N8, kPf, 3>,
+    cudaError_t e3 = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, MINB, N8, PF, 3>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem3));
     if (e3 != cudaSuccess) return e3;
-    scan_kernel<Q, kRegTopK, 2, N8, kPf, 3><<<dim3(qgroups, static_cast<unsigned>(blocks),
+    scan_kernel<Q, kRegTopK, MINB, N8, PF, 3><<<dim3(qgroups, static_cast<unsigned>(blocks),
                                                    static_cast<unsigned>(plan.split_batches)),
                                               kScanWarps * 32, smem3, stream>>>(s);
     return cudaGetLastError();
   }
-  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, 2, N8, kPf, 1>,
+  cudaError_t e = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, MINB, N8, PF, 1>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem1));
   if (e != cudaSuccess) return e;
-  scan_kernel<Q, kRegTopK, 2, N8, kPf, 1><<<dim3(qgroups, static_cast<unsigned>(blocks),
+  scan_kernel<Q, kRegTopK, MINB, N8, PF, 1><<<dim3(qgroups, static_cast<unsigned>(blocks),
                                                  static_cast<unsigned>(plan.split_batches)),
                                             kScanWarps * 32, smem1, stream>>>(s);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   ScanArgs c = a;
   c.partial_batches = plan.split_batches;
   const size_t smem2 = static_cast<size_t>(Q) * kScanWarps * kWarp * 8;  // the top-k merge area
-  e = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, 2, N8, kPf, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(scan_kernel<Q, kRegTopK, MINB, N8, PF, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem2));
   if (e != cudaSuccess) return e;
-  scan_kernel<Q, kRegTopK, 2, N8, kPf, 2><<<dim3(qgroups, static_cast<unsigned>(plan.n_ranges)), kScanWarps * 32,
+  scan_kernel<Q, kRegTopK, MINB, N8, PF, 2><<<dim3(qgroups, static_cast<unsigned>(plan.n_ranges)), kScanWarps * 32,
                                             smem2, stream>>>(c);
   return cudaGetLastError();
+}
+
+template <int Q, bool N8>
+cudaError_t launch_split_t(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream) {
+  constexpr int kPf = prefetch_for(Q);
+  const long long blocks = (a.n + kScanBlockVectors - 1) / kScanBlockVectors;
+  if (Q == 1 && plan.split_ctas_per_sm == 4) {
+    // One query, four CTAs per SM: 8 groups in flight within 64 registers.
+    return launch_split_mode<1, N8, 8, 4>(a, plan, stream, blocks);
+  }
+  return launch_split_mode<Q, N8, kPf, 2>(a, plan, stream, blocks);
 }
 
 size_t scan_warp_bytes(int q, int kmax) {
@@ -901,6 +910,19 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
     // whole rows staged: 4M x 1536 0.659 -> 0.612 ms, 10M x 768 3-bit
     // 0.633 -> 0.571 ms).
     plan->stages = 0;
+    // One query: 4 CTAs per SM (8 groups in flight, 64 registers) stream
+    // about 1.3x faster per resident wave than 2 (16 groups in flight, 111
+    // registers), but hold twice the CTAs per wave; take the shape with the
+    // smaller (waves x CTAs per SM / relative rate). Measured, one query:
+    // 1M x 1536 4-bit 0.174 -> 0.160 ms and 1M x 768 3-bit 0.105 -> 0.089 ms
+    // with 4; 500k x 1536 0.093 ms with 2 against 0.102 with 4.
+    if (q == 1) {
+      const long long ctas = qgroups * blocks * n_batches;
+      auto waves = [&](long long per_sm) { return (ctas + per_sm * sms - 1) / (per_sm * sms); };
+      const double cost2 = static_cast<double>(waves(2)) * 2.0;
+      const double cost4 = static_cast<double>(waves(4)) * 4.0 / 1.3;
+      plan->split_ctas_per_sm = cost4 < cost2 ? 4 : 2;
+    }
   }
   return true;
 }
