@@ -153,7 +153,10 @@ def test_one_and_two_queries(oracle, case):
         for k in (10, 32):
             plan = idx.scan_plan(nq, k)
             split = plan["split_batches"] > 1
-            assert plan["q_per_cta"] == nq and split == (dim > 256) and (plan["stages"] > 0) == (not split), plan
+            # whole rows: shared-memory slots, except one query over 2- or
+            # 4-bit codes (a register ring on four CTAs per SM)
+            staged = not split and (nq == 2 or bits == 3)
+            assert plan["q_per_cta"] == nq and split == (dim > 256) and (plan["stages"] > 0) == staged, plan
             q = q_all[:nq]
             res = idx.search(q, k)
             ws, wi = oracle.search_flat(q, bits, packed, alpha, k, shift, scale)
@@ -162,9 +165,11 @@ def test_one_and_two_queries(oracle, case):
     idx.close()
 
 
-# Whole-row staged scans too large for the oracle: top-10 against every
-# vector's score from the dense-scores kernel (itself checked against the
-# oracle above and in test_gpu_parity), ties by lower id.
+# Whole-row scans too large for the oracle: top-10 against every vector's
+# score from the dense-scores kernel (itself checked against the oracle above
+# and in test_gpu_parity), ties by lower id. Two queries (and one query over
+# 3-bit codes) stream through shared-memory slots, one query over 4-bit codes
+# keeps a register ring on four CTAs per SM.
 #   1.3M x 1024 4-bit: the LUT is streamed in 256-group chunks beside the slots;
 #   1.3M x 768 3-bit: resident LUT, 3-bit lookups;
 #   10M x 128 4-bit: several blocks per CTA (the slots carry over blocks).
@@ -172,7 +177,7 @@ STAGED_LARGE = [(1_300_000, 1024, 4), (1_300_000, 768, 3), (10_000_000, 128, 4)]
 
 
 @pytest.mark.parametrize("case", STAGED_LARGE, ids=lambda c: f"n{c[0]}_d{c[1]}_b{c[2]}")
-def test_staged_whole_rows_match_dense_scores(case):
+def test_whole_rows_match_dense_scores(case):
     torch = pytest.importorskip("torch")
     from vectorcache_b200.synthetic import power_law_torch
 
@@ -192,7 +197,8 @@ def test_staged_whole_rows_match_dense_scores(case):
     ids = np.arange(n)
     for nq in (1, 2):
         plan = idx.scan_plan(nq, 10)
-        assert plan["stages"] > 0 and plan["split_batches"] == 1 and plan["q_per_cta"] == nq, plan
+        staged = nq == 2 or bits == 3
+        assert (plan["stages"] > 0) == staged and plan["split_batches"] == 1 and plan["q_per_cta"] == nq, plan
         if n > 5_000_000:
             assert plan["range_vectors"] >= 2 * BLOCK, plan
         res = idx.search(q[:nq], 10)

@@ -463,7 +463,7 @@ int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, i
     const size_t m = std::min<size_t>(nq, size_t{1} << 16);
     vcb::ScanPlan plan;
     if (!vcb::plan_scan(static_cast<long long>(h->n), static_cast<long long>(m), static_cast<int>(h->nbg),
-                        static_cast<int>(std::min(k, h->n)), h->sms, &plan)) {
+                        static_cast<int>(std::min(k, h->n)), h->sms, &plan, 0, static_cast<int>(h->bits))) {
       vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
     }
     if (q_per_cta) *q_per_cta = plan.q_per_cta;
@@ -622,7 +622,7 @@ extern "C" int tq_index_search_device_noalloc(tq_index* h, const float* d_querie
     }
     vcb::ScanPlan plan;
     if (!vcb::plan_scan(static_cast<long long>(h->n), static_cast<long long>(nq), static_cast<int>(h->nbg),
-                        static_cast<int>(ke), h->sms, &plan)) {
+                        static_cast<int>(ke), h->sms, &plan, 0, static_cast<int>(h->bits))) {
       vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
     }
     // Fewer vector ranges if their candidate lists would not fit.

@@ -375,7 +375,7 @@ struct tq_index {
       prep_queries(d_q + q0 * dim, m, s, nullptr, sc);
       vcb::ScanPlan plan;
       if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
-                          static_cast<int>(k_eff), sms, &plan, sc.range_cap)) {
+                          static_cast<int>(k_eff), sms, &plan, sc.range_cap, static_cast<int>(bits))) {
         vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
       }
       const size_t lists = static_cast<size_t>(plan.n_ranges) * plan.lists_per_range;

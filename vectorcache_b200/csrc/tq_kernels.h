@@ -170,7 +170,11 @@ struct ScanPlan {
 };
 // max_range_vectors > 0 bounds the vectors one CTA scans (shorter CTAs let
 // higher-priority work on other streams start sooner).
-bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors = 0);
+// bits: the index's code width (one-query whole-row scans of 2- and 4-bit
+// codes take the register ring on four CTAs per SM, 3-bit codes the
+// shared-memory slots).
+bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors = 0,
+               int bits = 4);
 cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 

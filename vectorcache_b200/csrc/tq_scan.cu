@@ -823,7 +823,8 @@ size_t scan_warp_bytes(int q, int kmax) {
 
 }  // namespace
 
-bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors) {
+bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* plan, long long max_range_vectors,
+               int bits) {
   if (k < 1 || k > kMaxK || n <= 0 || nq <= 0) return false;
   const int kmax = k <= kRegTopK ? kRegTopK : (k <= 64 ? 64 : 256);
   const bool reg = kmax <= kRegTopK;
@@ -839,8 +840,12 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
   const size_t warp_total = kScanWarps * scan_warp_bytes(q, kmax);
   // One or two queries with the register top-k stream the codes through
   // shared-memory slots (nbg a multiple of the slot rows); the slots share
-  // the CTA's budget with the LUTs.
-  const bool staged = reg && q <= 2 && nbg % kStageGroups == 0;
+  // the CTA's budget with the LUTs. One query over 2- or 4-bit codes instead
+  // keeps an 8-group register ring on four CTAs per SM (one query, 4M x 1536
+  // 4-bit: 0.612 ms staged, 0.562 ms ring); the lighter 3-bit lookups gain
+  // more from the slots' bytes in flight (10M x 768: 0.568 ms staged, 0.583
+  // ms ring).
+  const bool staged = reg && q <= 2 && nbg % kStageGroups == 0 && !(q == 1 && bits != 3);
   const size_t stage_total = staged ? scan_stage_bytes(q) : 0;
   auto lut_area = [&](int c) {
     return staged ? scan_stage_offset(q, c) : static_cast<size_t>(q) * c * 32 + warp_total;
@@ -958,6 +963,8 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
     return n8 ? launch_scan_t<4, 64, 1, true, prefetch_for(4), 0, true>(a, plan, stream)
               : launch_scan_t<4, 64, 1, false, prefetch_for(4), 0, true>(a, plan, stream);
   }
+  // One query over 2- or 4-bit codes: the 8-group ring on four CTAs per SM.
+  if (q == 1 && km == 32 && !n8) return launch_scan_t<1, 32, 4, false, 8>(a, plan, stream);
   VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
   VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
   VCB_SCAN(1, 256, 1) VCB_SCAN(2, 256, 1)
