@@ -193,7 +193,9 @@ struct __align__(16) LutHalf {
 // multiply-add (-> 0.195 ms), the last addition of each four-lookup sum as a
 // multiply-add with four queries per CTA (10k queries 870.0 -> 876.0 ms with
 // the unchecked 4-group ring, 853.6 vs 853.3 ms with the 8-group ring).
-template <int Q, bool NIBBLE8>
+// DIRECT: vectors 0..3 add their two bytes with two dp4a instead of the
+// interleave prmt (see below).
+template <int Q, bool NIBBLE8, bool DIRECT = (Q >= 4 && !NIBBLE8)>
 __device__ __forceinline__ void lookup_group_pair(uint2 ca, uint2 cb, const LutHalf* lg, int q_stride,
                                                   uint32_t (&acc)[Q][8]) {
   auto hi16 = [](uint32_t x) -> uint32_t { return x >> 16; };
@@ -242,8 +244,9 @@ __device__ __forceinline__ void lookup_group_pair(uint2 ca, uint2 cb, const LutH
     // x 1M x 1536: 853.3 -> 840.2 ms; all eight vectors this way: 878.3 ms).
     // The 3-bit lookups (one prmt per nibble) leave the ALU pipe room, and
     // there the extra dp4a only cost (the multi-index workload, whose largest
-    // index is 3-bit: 103.6 -> 111.0 ms).
-    if constexpr (Q >= 4 && !NIBBLE8) {
+    // index is 3-bit: 103.6 -> 111.0 ms), as they did with k = 64 (one CTA of
+    // shared-memory lists per SM: 1M x 1536 4-bit 10,678 -> 10,561 QPS).
+    if constexpr (DIRECT) {
       acc[q][0] = __dp4a(hi0, 0x00000001u, __dp4a(lo0, 0x00000001u, acc[q][0]));
       acc[q][1] = __dp4a(hi0, 0x00000100u, __dp4a(lo0, 0x00000100u, acc[q][1]));
       acc[q][2] = __dp4a(hi0, 0x00010000u, __dp4a(lo0, 0x00010000u, acc[q][2]));

@@ -312,7 +312,9 @@ __global__ void __launch_bounds__(kScanWarps * 32, MIN_BLOCKS) scan_kernel(ScanA
           if constexpr (decltype(checked)::value) {
             if (g + u >= g_stop) break;
           }
-          lookup_group_pair<Q, NIBBLE8>(cur[u], cur[u + 1], s_lut + (g + u - chunk_base) * 2, chunk * 2, acc);
+          lookup_group_pair<Q, NIBBLE8, (Q >= 4 && !NIBBLE8 && kReg)>(cur[u], cur[u + 1],
+                                                                     s_lut + (g + u - chunk_base) * 2, chunk * 2,
+                                                                     acc);
         }
       };
       if constexpr (STAGES > 0) {
