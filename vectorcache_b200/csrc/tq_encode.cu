@@ -354,7 +354,7 @@ __host__ __device__ inline PipeLayout pipe_layout(int dim, int r_regs, bool tqpl
   L.off_ss = o;
   o += tqplus ? slots * 8 : 0;
   L.off_cen = o;
-  o += 16 * 8;
+  o += 16 * 8;  // 16 float centroids, padded to keep the grid 8-byte aligned
   L.off_grid = o;
   o += static_cast<size_t>(CodeGrid::kCells) * 8;
   L.off_src = o;
@@ -412,7 +412,9 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
   // element), and {shift, scale}.
   float* s_bk = reinterpret_cast<float*>(smem + L.off_bk);
   float2* s_ss = reinterpret_cast<float2*>(smem + L.off_ss);     // {shift, scale} (TQ+)
-  double* s_cen = reinterpret_cast<double*>(smem + L.off_cen);
+  // Float centroids, widened to double where used (exact): a 16-float table is
+  // one conflict-free wavefront per lookup, a 16-double table two.
+  float* s_cen = reinterpret_cast<float*>(smem + L.off_cen);
   uint2* s_grid = reinterpret_cast<uint2*>(smem + L.off_grid);     // {base code, inner boundary bits}
   uint32_t* s_src = reinterpret_cast<uint32_t*>(smem + L.off_src);
   float* s_bnd = reinterpret_cast<float*>(smem + L.off_bnd);
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
     }
   }
   if (threadIdx.x < 16) {
-    s_cen[threadIdx.x] = static_cast<double>(a.centroids[threadIdx.x]);
+    s_cen[threadIdx.x] = a.centroids[threadIdx.x];
     s_bnd[threadIdx.x] = threadIdx.x < 15 ? a.boundaries[threadIdx.x] : 0.f;
   }
   for (int j = threadIdx.x; j < CodeGrid::kCells; j += blockDim.x) s_grid[j] = a.grid[j];
@@ -579,12 +581,13 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
             const float2 ss = s_ss[r * 32 + lane];
             const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
             code = grid_code(c, s_grid, g_lo, g_hi, g_a, g_k);
-            const double back = __dsub_rn(__dmul_rn(s_cen[code], static_cast<double>(s_bk[r * 32 + lane])),
+            const double back = __dsub_rn(__dmul_rn(static_cast<double>(s_cen[code]),
+                                                    static_cast<double>(s_bk[r * 32 + lane])),
                                           static_cast<double>(ss.x));
             term = __dmul_rn(static_cast<double>(y[r]), back);
           } else {
             code = grid_code(y[r], s_grid, g_lo, g_hi, g_a, g_k);
-            term = __dmul_rn(static_cast<double>(y[r]), s_cen[code]);
+            term = __dmul_rn(static_cast<double>(y[r]), static_cast<double>(s_cen[code]));
           }
           est = __dadd_rn(est, term);
           mag = __dadd_rn(mag, fabs(term));
@@ -625,10 +628,11 @@ __global__ void __launch_bounds__(MAXW * 32, 1) encode_pipe_kernel(EncodeArgs a)
                     const float2 ss = s_ss[r * 32 + lane];
                     const float c = __fmul_rn(__fadd_rn(y[r], ss.x), ss.y);
                     const unsigned code = pipe_code<BITS>(c, s_bnd);
-                    back = __dsub_rn(__dmul_rn(s_cen[code], static_cast<double>(s_bk[r * 32 + lane])),
+                    back = __dsub_rn(__dmul_rn(static_cast<double>(s_cen[code]),
+                                               static_cast<double>(s_bk[r * 32 + lane])),
                                      static_cast<double>(ss.x));
                   } else {
-                    back = s_cen[pipe_code<BITS>(y[r], s_bnd)];
+                    back = static_cast<double>(s_cen[pipe_code<BITS>(y[r], s_bnd)]);
                   }
                   ch[e & 3] = __fma_rn(static_cast<double>(y[r]), back, ch[e & 3]);
                 }
