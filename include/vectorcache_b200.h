@@ -185,6 +185,16 @@ int tq_index_replay_count(const tq_index* h, uint64_t* count);
 int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, int* n_ranges,
                        uint64_t* range_vectors, int* split_batches, int* stages);
 
+/* The same plan for an index of n vectors of dim coordinates at bits, on a device
+ * of `sms` SMs, computed on the host alone (no index, no device; the plan of a
+ * search through the index's own scratch). Outputs as above, plus the CTAs per SM
+ * of a one- or two-query batch-split scan (0 when it does not split). No
+ * counterpart in the reference: it lets tests check the planning rules and
+ * callers size a deployment without a GPU. Any out pointer may be null. */
+int tq_scan_plan_shape(uint64_t n, size_t nq, size_t dim, size_t bits, size_t k, int sms, int* q_per_cta,
+                       int* n_ranges, uint64_t* range_vectors, int* split_batches, int* stages,
+                       int* split_ctas_per_sm);
+
 /* ---- measurement (no counterpart in the reference, which times with
  *      std::chrono around whole calls: tools/gpu-bench.cpp:155-190) ---------- */
 

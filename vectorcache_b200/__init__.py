@@ -28,6 +28,7 @@ __all__ = [
     "TurboQuantError",
     "codebook",
     "rotation_tables",
+    "scan_plan_shape",
     "load_library",
     "LIB_PATH",
 ]
@@ -98,6 +99,9 @@ def _declare(lib):
         "tq_index_replay_count": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
         "tq_index_scan_plan": (C.c_int, [_P, _SZ, _SZ, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "tq_scan_plan_shape": (C.c_int, [C.c_uint64, _SZ, _SZ, _SZ, _SZ, C.c_int, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "tq_index_save": (C.c_int, [_P, C.c_char_p]),
         "tq_index_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_P)]),
         "tq_index_add_npy": (C.c_int, [_P, C.c_char_p]),
@@ -180,6 +184,20 @@ def rotation_tables(dim: int) -> tuple[np.ndarray, np.ndarray]:
     p = np.zeros(max(dim, 1), np.uint32)
     _check(load_library().tq_rotation_tables(dim, _ptr(s), _ptr(p)))
     return s, p
+
+
+def scan_plan_shape(n: int, nq: int, dim: int, bits: int, k: int, sms: int = 148) -> dict:
+    """The scan tiling a search of nq queries with this k would use on an index
+    of n vectors (dim, bits) and a device of `sms` SMs, planned on the host (no
+    GPU needed): TurboQuantIndex.scan_plan's fields plus the CTAs per SM of a
+    batch-split one- or two-query scan (0 when it does not split)."""
+    lib = load_library()
+    q, r, s, st, cps = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    rv = C.c_uint64()
+    _check(lib.tq_scan_plan_shape(n, nq, dim, bits, k, sms, C.byref(q), C.byref(r), C.byref(rv), C.byref(s),
+                                  C.byref(st), C.byref(cps)))
+    return {"q_per_cta": q.value, "n_ranges": r.value, "range_vectors": rv.value, "split_batches": s.value,
+            "stages": st.value, "split_ctas_per_sm": cps.value}
 
 
 def rescore(queries, corpus, results: "SearchResults", device: int = 0) -> "SearchResults":

@@ -474,6 +474,33 @@ int tq_index_scan_plan(const tq_index* h, size_t nq, size_t k, int* q_per_cta, i
   });
 }
 
+int tq_scan_plan_shape(uint64_t n, size_t nq, size_t dim, size_t bits, size_t k, int sms, int* q_per_cta,
+                       int* n_ranges, uint64_t* range_vectors, int* split_batches, int* stages,
+                       int* split_ctas_per_sm) {
+  return vcb::guarded([&] {
+    require(n >= 1 && nq >= 1, TQ_ERR_INVALID_ARGUMENT, "n and nq must be >= 1");
+    require(dim >= 8 && dim <= 16384 && dim % 8 == 0, TQ_ERR_INVALID_ARGUMENT,
+            "dim must be a positive multiple of 8, at most 16384");
+    require(bits >= 2 && bits <= 4, TQ_ERR_INVALID_ARGUMENT, "bits must be 2, 3 or 4");
+    require(k >= 1 && k <= static_cast<size_t>(vcb::kMaxK), TQ_ERR_UNSUPPORTED, "k must be in [1, 256]");
+    require(sms >= 1, TQ_ERR_INVALID_ARGUMENT, "sms must be >= 1");
+    const size_t nbg = dim / (8 / bits);  // byte groups: dim / 2 at 3 and 4 bits, dim / 4 at 2 bits
+    // search_device plans each pass of at most 65,536 queries.
+    const size_t m = std::min<size_t>(nq, size_t{1} << 16);
+    vcb::ScanPlan plan;
+    if (!vcb::plan_scan(static_cast<long long>(n), static_cast<long long>(m), static_cast<int>(nbg),
+                        static_cast<int>(std::min<uint64_t>(k, n)), sms, &plan, 0, static_cast<int>(bits))) {
+      vcb::fail(TQ_ERR_UNSUPPORTED, "no scan configuration fits shared memory for this dim / k");
+    }
+    if (q_per_cta) *q_per_cta = plan.q_per_cta;
+    if (n_ranges) *n_ranges = plan.n_ranges;
+    if (range_vectors) *range_vectors = static_cast<uint64_t>(plan.range_vectors);
+    if (split_batches) *split_batches = std::max(1, plan.split_batches);
+    if (stages) *stages = plan.stages;
+    if (split_ctas_per_sm) *split_ctas_per_sm = plan.split_batches > 1 ? plan.split_ctas_per_sm : 0;
+  });
+}
+
 }  // extern "C"
 
 extern "C" {
