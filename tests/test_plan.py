@@ -5,8 +5,10 @@ shapes run with, as tq_index_scan_plan reports them on a B200 (148 SMs).
 * One or two queries over at most two waves of 2048-vector blocks split by
   256-group batch; one query takes four CTAs per SM when that wastes less of
   the last wave (1M vectors), two otherwise (200k, 500k vectors).
-* Larger one-query scans run whole rows: a register ring for 2- and 4-bit
-  codes (stages 0), shared-memory slots for 3-bit codes and for two queries.
+* Larger one-query scans run whole rows: a register ring on four CTAs per SM
+  for 2- and 4-bit codes (stages 0) while four CTAs' LUTs fit an SM (rows up
+  to 3072 dims at 4 bits), shared-memory slots for wider rows, for 3-bit
+  codes and for two queries.
 """
 import pytest
 
@@ -49,6 +51,8 @@ def test_two_queries_split_on_two_ctas_per_sm():
     (4_000_000, 1, 1536, 2, 0),
     (10_000_000, 1, 768, 3, 6),   # shared-memory slots
     (4_000_000, 2, 1536, 4, 5),
+    (4_000_000, 1, 3072, 4, 0),   # the widest rows whose four LUTs fit an SM
+    (4_000_000, 1, 4096, 4, 6),   # wider: slots again
 ])
 def test_whole_row_code_stream(n, nq, dim, bits, stages):
     p = plan(n, nq, dim, bits)

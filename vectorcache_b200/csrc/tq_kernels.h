@@ -164,6 +164,9 @@ struct ScanPlan {
   // 64 registers) or 2 (16 groups in flight), whichever wastes less of its
   // last wave.
   int split_ctas_per_sm = 2;
+  // CTAs per SM of a one-query whole-row scan on the register ring: 4 (8
+  // groups in flight) for 2- and 4-bit codes when four CTAs' LUTs fit, else 2.
+  int ring_ctas_per_sm = 2;
   // > 0: the code stream goes through this many shared-memory slots per warp
   // (one or two queries per CTA, register top-k).
   int stages = 0;

@@ -846,8 +846,10 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
   // keeps an 8-group register ring on four CTAs per SM (one query, 4M x 1536
   // 4-bit: 0.612 ms staged, 0.562 ms ring); the lighter 3-bit lookups gain
   // more from the slots' bytes in flight (10M x 768: 0.568 ms staged, 0.583
-  // ms ring).
-  const bool staged = reg && q <= 2 && nbg % kStageGroups == 0 && !(q == 1 && bits != 3);
+  // ms ring). The ring needs four CTAs' resident LUTs on an SM (at most 48 KB
+  // each: nbg <= 1536, 3072 dims at 4 bits); wider rows keep the slots.
+  const bool ring4 = reg && q == 1 && bits != 3 && static_cast<size_t>(nbg) * 32 <= 48 * 1024;
+  const bool staged = reg && q <= 2 && nbg % kStageGroups == 0 && !ring4;
   const size_t stage_total = staged ? scan_stage_bytes(q) : 0;
   auto lut_area = [&](int c) {
     return staged ? scan_stage_offset(q, c) : static_cast<size_t>(q) * c * 32 + warp_total;
@@ -901,6 +903,7 @@ bool plan_scan(long long n, long long nq, int nbg, int k, int sms, ScanPlan* pla
     plan->smem_bytes = std::max(plan->smem_bytes, static_cast<size_t>(q) * kScanWarps * kWarp * 8);
   }
   plan->stages = staged ? stages_for(q) : 0;
+  plan->ring_ctas_per_sm = ring4 ? 4 : 2;
   if (staged) plan->smem_bytes = scan_stage_offset(q, chunk) + stage_total;
   plan->lists_per_range = reg ? 1 : kScanWarps;
   // One or two queries over at most two waves of blocks: whole blocks per CTA
@@ -966,7 +969,9 @@ cudaError_t launch_scan(const ScanArgs& a, const ScanPlan& plan, cudaStream_t st
               : launch_scan_t<4, 64, 1, false, prefetch_for(4), 0, true>(a, plan, stream);
   }
   // One query over 2- or 4-bit codes: the 8-group ring on four CTAs per SM.
-  if (q == 1 && km == 32 && !n8) return launch_scan_t<1, 32, 4, false, 8>(a, plan, stream);
+  if (q == 1 && km == 32 && !n8 && plan.ring_ctas_per_sm == 4) {
+    return launch_scan_t<1, 32, 4, false, 8>(a, plan, stream);
+  }
   VCB_SCAN(1, 32, 2) VCB_SCAN(2, 32, 2) VCB_SCAN(4, 32, 2)
   VCB_SCAN(1, 64, 1) VCB_SCAN(2, 64, 1) VCB_SCAN(4, 64, 1)
   VCB_SCAN(1, 256, 1) VCB_SCAN(2, 256, 1)
